@@ -1,0 +1,109 @@
+// Internal declarations shared by the C-ABI layer and the kernel files.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hh {
+
+constexpr int KMAX = 8;  // peaks tracked per window on the device (n_peaks <= 8)
+
+// Arguments of the fused correlation kernel (one pass, one image pair).
+struct CorrArgs {
+  const float* A;            // deformed (or raw) frame A, column-major nr x nc
+  const float* B;            // frame B
+  const uint8_t* mask;       // image mask (nonzero = excluded) or nullptr
+  int64_t ld;                // leading dimension (= nr)
+  const int32_t* jobs;       // 4 int32 per job: gi, gj, rs, cs (0-based)
+  int64_t njobs;
+  int32_t ny;                // grid rows; grid index id = gi + gj * ny
+  int64_t G;                 // grid size ny * nx
+  const float* apod;         // W x W apodization window (column-major)
+  const float* gain;         // N x N overlap gain (fftshifted layout) or nullptr
+  const float* phasew;       // N x N phase filter (natural FFT order) or nullptr
+  int32_t method, npeaks, finder, subpixel;
+  // grid-indexed outputs (residual displacement of this sweep)
+  float* du;
+  float* dv;
+  float* ratio;
+  float* moment;
+  float* alt_u;              // G x nalt or nullptr
+  float* alt_v;
+  int32_t nalt;
+  // optional per-job outputs
+  float* packed;             // (5 + 2(K-1)) x njobs
+  int32_t* locs;             // 2K x njobs (1-based row, col)
+  float* planes;             // N*N x njobs correlation planes
+};
+
+// Launch the correlation kernel for FFT size N (square) and window W.
+cudaError_t launch_correlate(const CorrArgs& a, int N, int W, cudaStream_t s, int num_sms);
+bool correlate_supported(int N, int W);
+size_t correlate_smem_bytes(int N, int W);
+
+// Device peak analysis of caller-supplied planes.
+struct AnalyzeArgs {
+  const float* planes;
+  int64_t nplanes;
+  int32_t nr, nc;
+  int32_t npeaks, finder, subpixel;
+  float* packed;
+  int32_t* locs;
+};
+cudaError_t launch_analyze_planes(const AnalyzeArgs& a, cudaStream_t s);
+
+// --- deformation -----------------------------------------------------------
+cudaError_t launch_prefilter(const float* img, int64_t nr, int64_t nc, float* coef, float* scratch,
+                             cudaStream_t s);
+struct PredGrid {
+  int32_t gny, gnx;
+  float y0, ysp, x0, xsp;
+};
+cudaError_t launch_deform(const float* CA, const float* CB, int64_t nr, int64_t nc, const float* pu,
+                          const float* pv, PredGrid g, float* wA, float* wB, cudaStream_t s);
+cudaError_t launch_node_values(const float* pu, const float* pv, PredGrid g, const float* y, int32_t ny,
+                               const float* x, int32_t nx, float* u, float* v, cudaStream_t s);
+
+// --- vector-grid kernels -----------------------------------------------------
+cudaError_t launch_combine(float* u, float* v, const float* resu, const float* resv, float* ratio, float* moment,
+                           float* alt_u, float* alt_v, int32_t nalt, const uint8_t* gmask, int64_t G,
+                           float* meas_u, float* meas_v, cudaStream_t s);
+cudaError_t launch_uod(const float* u, const float* v, int32_t ny, int32_t nx, double thr, int32_t nb, double eps,
+                       const uint8_t* exclude, uint8_t* flags, int32_t or_into, cudaStream_t s);
+cudaError_t launch_flag_ratio(const float* ratio, int64_t G, double thr, uint8_t* flags, cudaStream_t s);
+cudaError_t launch_flag_moment(const float* moment, int64_t G, double thr, uint8_t* flags, cudaStream_t s);
+cudaError_t launch_flag_velocity(const float* u, const float* v, int64_t G, double vmin, double vmax,
+                                 uint8_t* flags, cudaStream_t s);
+cudaError_t launch_mask_flags(uint8_t* flags, const uint8_t* gmask, int64_t G, cudaStream_t s);
+cudaError_t launch_substitute(float* u, float* v, const uint8_t* outl_in, uint8_t* outl_out, const uint8_t* gmask,
+                              const float* alt_u, const float* alt_v, int32_t nalt, int32_t ny, int32_t nx,
+                              int32_t er, double thr, cudaStream_t s);
+// replace_vectors!: invalid = flags | gmask (either may be nullptr); masked
+// cells are set to NaN afterwards when nan_mask is nonzero.
+cudaError_t launch_replace(float* u, float* v, const uint8_t* flags, const uint8_t* gmask, int32_t ny, int32_t nx,
+                           int32_t nan_mask, cudaStream_t s);
+cudaError_t launch_smooth(const float* f, int32_t ny, int32_t nx, float* out, cudaStream_t s);
+// field_change -> *out (device float); scratch: G floats + 2 KB
+cudaError_t launch_field_change(const float* u, const float* v, const float* pu, const float* pv,
+                                const uint8_t* gmask, int64_t G, float* scratch, float* out, cudaStream_t s);
+cudaError_t launch_restore_measured(float* u, float* v, const float* meas_u, const float* meas_v,
+                                    const uint8_t* outl, int64_t G, cudaStream_t s);
+cudaError_t launch_fill(float* p, float value, int64_t n, cudaStream_t s);
+
+// --- uncertainty -------------------------------------------------------------
+struct UQArgs {
+  const float* A;
+  const float* B;
+  const uint8_t* mask;
+  int64_t ld;
+  const int32_t* jobs;
+  int64_t njobs;
+  int32_t ny;
+  int32_t W;
+  const float* apod;
+  double* stats;     // 88 per job, or nullptr
+  float* unc_u;      // grid-indexed outputs, or nullptr
+  float* unc_v;
+};
+cudaError_t launch_uq(const UQArgs& a, cudaStream_t s, int num_sms);
+
+}  // namespace hh

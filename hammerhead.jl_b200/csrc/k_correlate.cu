@@ -1,0 +1,707 @@
+// Fused window correlation for the planar WIDIM pass (sm_100a).
+//
+// One CTA holds WPC interrogation windows in shared memory and runs, per
+// window, the whole of the reference's per-window chain
+//   load_windows!  (src/correlators.jl:188-263: column-major mean, apodize)
+//   FFT A, FFT B   (packed as one complex transform of A + iB)
+//   spectrum!      (src/correlators.jl:266-279: conj(FA) FB, or filtered phase)
+//   inverse FFT    (normalised by 1/N^2 like FFTW's inv(plan))
+//   fftshift_abs!, overlap gain (src/correlators.jl:282-289, 338-339)
+//   analyze_plane! (src/correlators.jl:459-468: regional-max or exclusion
+//                   peaks with the tie rules of src/localmax.jl:3-19,
+//                   gauss3/gauss9 in FP64, peak ratio, FP64 moment,
+//                   gauss3-refined alternatives)
+// writing the packed scalars of src/ka_backend.jl:497-506 straight into the
+// vector grid. Nothing but images in and scalars out touches HBM.
+//
+// Shared-memory plane layout: element (p, q) (row p, column q) of window w
+// lives at planes[w*N*LD + q*LD + p] with LD = N + 1, so a warp walking
+// either axis with one line per lane is bank-conflict free.
+//
+// The 2-D transform runs each axis as an in-register radix-N1 pass and, for
+// N > 32, a second radix-N2 pass (N = N1*N2). The forward transform leaves
+// frequency k at position N2*(k % N1) + k / N1 along each axis; the spectrum
+// step reads pairs (k, -k) from there and the inverse takes that order back
+// to natural order, so no bit-reversal pass exists anywhere.
+#include <math.h>
+#include <stdint.h>
+
+#include "hh_fft.cuh"
+#include "hh_internal.h"
+
+namespace hh {
+
+// ---------------------------------------------------------------------------
+// Peak keys: larger key = larger value, ties broken by smaller column-major
+// index (the reference's first-in-scan-order rule).
+__device__ __forceinline__ uint32_t fkey(float v) {
+  v = v + 0.0f;  // -0 -> +0 (they compare equal in the reference)
+  uint32_t b = __float_as_uint(v);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+struct TopK {
+  uint32_t hi[KMAX];
+  uint32_t lo[KMAX];
+  int cnt;
+  __device__ __forceinline__ void init() {
+    cnt = 0;
+#pragma unroll
+    for (int m = 0; m < KMAX; ++m) hi[m] = lo[m] = 0u;
+  }
+  // insert keeping (hi, lo) descending; K <= KMAX entries retained
+  __device__ __forceinline__ void insert(uint32_t h, uint32_t l, int K) {
+    if (cnt == K && !(h > hi[K - 1] || (h == hi[K - 1] && l > lo[K - 1]))) return;
+    uint32_t ch = h, cl = l;
+#pragma unroll
+    for (int m = 0; m < KMAX; ++m) {
+      if (m < K && m <= cnt) {
+        bool better = ch > hi[m] || (ch == hi[m] && cl > lo[m]) || m == cnt;
+        if (better) {
+          uint32_t th = hi[m], tl = lo[m];
+          hi[m] = ch;
+          lo[m] = cl;
+          ch = th;
+          cl = tl;
+        }
+      }
+    }
+    if (cnt < K) ++cnt;
+  }
+  __device__ __forceinline__ void pop() {
+#pragma unroll
+    for (int m = 0; m + 1 < KMAX; ++m) {
+      hi[m] = hi[m + 1];
+      lo[m] = lo[m + 1];
+    }
+    hi[KMAX - 1] = lo[KMAX - 1] = 0u;
+    if (cnt > 0) --cnt;
+  }
+};
+
+// is_local_maximum (src/localmax.jl:3-19) on a column-major plane with
+// leading dimension ldr: earlier neighbours (column-major) must be <=,
+// later ones must be <; NaN is never a maximum.
+__device__ __forceinline__ bool is_local_max(const float* R, int nr, int nc, int ldr, int r, int c, float I0) {
+  if (isnan(I0)) return false;
+  const int r0 = r > 0 ? r - 1 : 0, r1 = r < nr - 1 ? r + 1 : nr - 1;
+  const int c0 = c > 0 ? c - 1 : 0, c1 = c < nc - 1 ? c + 1 : nc - 1;
+  for (int jj = c0; jj <= c1; ++jj)
+    for (int ii = r0; ii <= r1; ++ii) {
+      if (ii == r && jj == c) continue;
+      float In = R[jj * ldr + ii];
+      bool earlier = (jj < c) || (jj == c && ii < r);
+      if (earlier ? (In > I0) : (In >= I0)) return false;
+    }
+  return true;
+}
+
+// Group-wide argmax of (hi, lo) keys. All threads of the CTA call it (it
+// contains __syncthreads); each window group gets its own reduction slots.
+__device__ __forceinline__ void group_argmax(uint32_t hi, uint32_t lo, uint32_t* red, int gwarp, int nwarps,
+                                             uint32_t& whi, uint32_t& wlo) {
+  const int lane = threadIdx.x & 31;
+  uint32_t mhi = __reduce_max_sync(0xffffffffu, hi);
+  uint32_t mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  if (lane == 0) {
+    red[2 * gwarp] = mhi;
+    red[2 * gwarp + 1] = mlo;
+  }
+  __syncthreads();
+  whi = 0u;
+  wlo = 0u;
+  for (int w = 0; w < nwarps; ++w) {
+    uint32_t h = red[2 * w], l = red[2 * w + 1];
+    if (h > whi || (h == whi && l > wlo)) {
+      whi = h;
+      wlo = l;
+    }
+  }
+  __syncthreads();
+}
+
+// subpixel_gauss3 (src/correlators.jl:499-520) with FP64 logarithms.
+// (i, j) 0-based; returns 1-based refined (row, col).
+__device__ __forceinline__ void gauss3_fp64(const float* R, int nr, int nc, int ldr, int i, int j, float* out) {
+  double di = 0.0, dj = 0.0;
+  const float I0 = R[j * ldr + i];
+  if (i > 0 && i < nr - 1) {
+    float Im = R[j * ldr + i - 1], Ip = R[j * ldr + i + 1];
+    if (Im > 0.f && I0 > 0.f && Ip > 0.f) {
+      double lm = log((double)Im), l0 = log((double)I0), lp = log((double)Ip);
+      double den = lm - 2.0 * l0 + lp;
+      di = den != 0.0 ? (lm - lp) / (2.0 * den) : 0.0;
+    }
+  }
+  if (j > 0 && j < nc - 1) {
+    float Im = R[(j - 1) * ldr + i], Ip = R[(j + 1) * ldr + i];
+    if (Im > 0.f && I0 > 0.f && Ip > 0.f) {
+      double lm = log((double)Im), l0 = log((double)I0), lp = log((double)Ip);
+      double den = lm - 2.0 * l0 + lp;
+      dj = den != 0.0 ? (lm - lp) / (2.0 * den) : 0.0;
+    }
+  }
+  out[0] = (float)((double)(i + 1) + di);
+  out[1] = (float)((double)(j + 1) + dj);
+}
+
+// subpixel_gauss9 (src/correlators.jl:534-564) with FP64 logarithms.
+__device__ __forceinline__ void gauss9_fp64(const float* R, int nr, int nc, int ldr, int pr, int pc, float* out) {
+  if (!(pr > 0 && pr < nr - 1 && pc > 0 && pc < nc - 1)) return gauss3_fp64(R, nr, nc, ldr, pr, pc, out);
+  double sL = 0, sxL = 0, syL = 0, sxxL = 0, syyL = 0, sxyL = 0;
+  for (int dj = -1; dj <= 1; ++dj)
+    for (int di = -1; di <= 1; ++di) {
+      float val = R[(pc + dj) * ldr + pr + di];
+      if (!(val > 0.f)) return gauss3_fp64(R, nr, nc, ldr, pr, pc, out);
+      double L = log((double)val);
+      sL += L;
+      sxL += dj * L;
+      syL += di * L;
+      sxxL += (dj * dj) * L;
+      syyL += (di * di) * L;
+      sxyL += (di * dj) * L;
+    }
+  double a1 = sxL / 6, a2 = syL / 6, a3 = sxxL / 2 - sL / 3, a4 = sxyL / 4, a5 = syyL / 2 - sL / 3;
+  double D = 4 * a3 * a5 - a4 * a4;
+  if (!(a3 < 0 && D > 0)) return gauss3_fp64(R, nr, nc, ldr, pr, pc, out);
+  double dx = (a4 * a2 - 2 * a5 * a1) / D;
+  double dy = (a4 * a1 - 2 * a3 * a2) / D;
+  if (!(fabs(dx) <= 1 && fabs(dy) <= 1)) return gauss3_fp64(R, nr, nc, ldr, pr, pc, out);
+  out[0] = (float)((double)(pr + 1) + dy);
+  out[1] = (float)((double)(pc + 1) + dx);
+}
+
+// calculate_correlation_moment (src/quality.jl:49-74, neighbourhood 3):
+// (c - pc)^2 in float like the Float32 reference, sums in FP64.
+__device__ __forceinline__ float moment_fp64(const float* R, int nr, int nc, int ldr, float pr, float pc) {
+  if (!(isfinite(pr) && isfinite(pc))) return __int_as_float(0x7fc00000);
+  int r0 = (int)rintf(pr), c0 = (int)rintf(pc);  // 1-based, ties to even
+  int rlo = max(1, r0 - 1), rhi = min(nr, r0 + 1), clo = max(1, c0 - 1), chi = min(nc, c0 + 1);
+  if (rlo > rhi || clo > chi) return __int_as_float(0x7fc00000);
+  double sumC = 0, sdx = 0, sdy = 0;
+  for (int c = clo; c <= chi; ++c)
+    for (int r = rlo; r <= rhi; ++r) {
+      double w = fmax((double)R[(c - 1) * ldr + (r - 1)], 0.0);
+      float dx = __fsub_rn((float)c, pc), dy = __fsub_rn((float)r, pr);
+      sumC += w;
+      sdx += (double)__fmul_rn(dx, dx) * w;
+      sdy += (double)__fmul_rn(dy, dy) * w;
+    }
+  if (sumC < 1e-9) return __int_as_float(0x7fc00000);
+  return (float)sqrt((sdx + sdy) / sumC);
+}
+
+struct PeakOut {
+  float* du;
+  float* dv;
+  float* ratio;
+  float* moment;
+  float* alt_u;
+  float* alt_v;
+  int32_t nalt;
+  int64_t G;
+  float* packed;
+  int32_t* locs;
+};
+
+// Peak analysis of one plane by a group of threads (tid in [0, gsize)).
+// Every thread of the CTA must call this (uniform K and finder), because
+// the merge rounds synchronise the whole CTA.
+__device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
+                              int subpixel, int gtid, int gsize, uint32_t* red, bool active, float* s_vals,
+                              int* s_locs, int64_t grid_id, int64_t job, const PeakOut& o) {
+  const int gwarp = gtid >> 5, nwarps = gsize >> 5;
+  const int P = nr * nc;
+  int nfound = 0;
+  if (finder == 0) {
+    // regional maxima: per-thread top-K over a strided scan, then K merges
+    TopK tk;
+    tk.init();
+    if (active) {
+      for (int lin = gtid; lin < P; lin += gsize) {
+        const int r = lin % nr, c = lin / nr;
+        const float v = R[c * ldr + r];
+        if (isnan(v)) continue;
+        const uint32_t h = fkey(v);
+        if (tk.cnt == K && h <= tk.hi[K - 1]) continue;  // later index cannot win a tie
+        if (!is_local_max(R, nr, nc, ldr, r, c, v)) continue;
+        tk.insert(h, ~(uint32_t)lin, K);
+      }
+    }
+    bool done = false;
+    for (int round = 0; round < K; ++round) {  // every round runs: group_argmax synchronises the CTA
+      uint32_t whi, wlo;
+      group_argmax(tk.cnt > 0 ? tk.hi[0] : 0u, tk.cnt > 0 ? tk.lo[0] : 0u, red, gwarp, nwarps, whi, wlo);
+      if (done || whi == 0u) { done = true; continue; }
+      if (tk.cnt > 0 && tk.hi[0] == whi && tk.lo[0] == wlo) tk.pop();
+      if (gtid == 0) {
+        const int lin = (int)(~wlo);
+        s_vals[round] = R[(lin / nr) * ldr + (lin % nr)];
+        s_locs[2 * round] = lin % nr;
+        s_locs[2 * round + 1] = lin / nr;
+      }
+      nfound = round + 1;
+    }
+  } else {
+    // exclusion finder (src/correlators.jl:390-421): K scans, box +-2
+    bool done = false;
+    for (int round = 0; round < K; ++round) {  // every round runs: group_argmax synchronises the CTA
+      uint32_t bh = 0u, bl = 0u;
+      if (active && !done) {
+        for (int lin = gtid; lin < P; lin += gsize) {
+          const int r = lin % nr, c = lin / nr;
+          bool ex = false;
+          for (int q = 0; q < nfound; ++q)
+            if (abs(r - s_locs[2 * q]) <= 2 && abs(c - s_locs[2 * q + 1]) <= 2) { ex = true; break; }
+          if (ex) continue;
+          const float v = R[c * ldr + r];
+          if (!(v > -INFINITY)) continue;  // NaN and -Inf never beat the initial -Inf
+          const uint32_t h = fkey(v), l = ~(uint32_t)lin;
+          if (h > bh || (h == bh && l > bl)) { bh = h; bl = l; }
+        }
+      }
+      uint32_t whi, wlo;
+      group_argmax(bh, bl, red, gwarp, nwarps, whi, wlo);
+      if (!done && whi != 0u) {
+        const int lin = (int)(~wlo);
+        const float best = R[(lin / nr) * ldr + (lin % nr)];
+        if (nfound > 0 && !(best > 0.f)) {
+          done = true;  // secondary peaks must be positive
+        } else {
+          if (gtid == 0) {
+            s_vals[nfound] = best;
+            s_locs[2 * nfound] = lin % nr;
+            s_locs[2 * nfound + 1] = lin / nr;
+          }
+          ++nfound;
+        }
+      } else {
+        done = true;
+      }
+      __syncthreads();  // s_locs visible to the next round's exclusion test
+    }
+  }
+  if (gtid != 0 || !active) return;
+  // found = leading peaks whose secondaries are positive
+  int found = 0;
+  if (nfound > 0) {
+    found = 1;
+    while (found < nfound && s_vals[found] > 0.f) ++found;
+  }
+  const float NaN = __int_as_float(0x7fc00000);
+  const int cr = nr / 2 + 1, cc = nc / 2 + 1;
+  float du = NaN, dv = NaN, ratio = NaN, mom = NaN;
+  float alt_du[KMAX], alt_dv[KMAX];
+#pragma unroll
+  for (int m = 0; m < KMAX; ++m) alt_du[m] = alt_dv[m] = NaN;
+  if (found > 0) {
+    float ref[2];
+    const int pr = s_locs[0], pc = s_locs[1];
+    if (subpixel == 1) gauss9_fp64(R, nr, nc, ldr, pr, pc, ref);
+    else if (subpixel == 3) { ref[0] = (float)(pr + 1); ref[1] = (float)(pc + 1); }
+    else gauss3_fp64(R, nr, nc, ldr, pr, pc, ref);
+    du = ref[1] - (float)cc;
+    dv = ref[0] - (float)cr;
+    const float v1 = s_vals[0];
+    ratio = found >= 2 ? v1 / s_vals[1] : (v1 > 0.f ? INFINITY : NaN);
+    mom = moment_fp64(R, nr, nc, ldr, ref[0], ref[1]);
+    const int mmax = found < npeaks ? found : npeaks;
+    for (int m = 2; m <= mmax; ++m) {
+      float a[2];
+      gauss3_fp64(R, nr, nc, ldr, s_locs[2 * (m - 1)], s_locs[2 * (m - 1) + 1], a);
+      alt_du[m - 2] = a[1] - (float)cc;
+      alt_dv[m - 2] = a[0] - (float)cr;
+    }
+  }
+  if (grid_id >= 0 && o.du) {
+    o.du[grid_id] = du;
+    o.dv[grid_id] = dv;
+    o.ratio[grid_id] = ratio;
+    o.moment[grid_id] = mom;
+    if (o.alt_u)
+      for (int m = 0; m < o.nalt; ++m) {
+        o.alt_u[grid_id + (int64_t)m * o.G] = alt_du[m];
+        o.alt_v[grid_id + (int64_t)m * o.G] = alt_dv[m];
+      }
+  }
+  if (o.packed) {
+    float* pk = o.packed + job * (int64_t)(5 + 2 * (K - 1));
+    pk[0] = du;
+    pk[1] = dv;
+    pk[2] = ratio;
+    pk[3] = mom;
+    pk[4] = (float)found;
+    for (int m = 0; m < K - 1; ++m) {
+      pk[5 + m] = alt_du[m];
+      pk[5 + (K - 1) + m] = alt_dv[m];
+    }
+  }
+  if (o.locs) {
+    int32_t* lc = o.locs + job * (int64_t)(2 * K);
+    for (int m = 0; m < K; ++m) {
+      lc[2 * m] = m < found ? s_locs[2 * m] + 1 : 0;
+      lc[2 * m + 1] = m < found ? s_locs[2 * m + 1] + 1 : 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <int N, int W> struct CorrCfg {
+  static constexpr int N1 = AxisSplit<N>::N1, N2 = AxisSplit<N>::N2;
+  static constexpr int WPC = N <= 32 ? 4 : (N <= 48 ? 2 : (N <= 64 ? 2 : 1));
+  static constexpr int NT = N <= 48 ? 128 : 256;
+  static constexpr int G = NT / WPC;  // threads per window in the analysis
+  static constexpr int LD = N + 1;    // complex plane leading dimension
+  static constexpr int LDR = N + 1;   // real plane leading dimension
+  static constexpr bool PADDED = (W * 2 == N);
+  static constexpr int NZ1 = PADDED ? (W / N2) : N1;  // nonzero inputs of a forward pass-A line
+  static constexpr size_t PLANE_B = (size_t)N * LD * sizeof(float2);
+  static constexpr size_t R_B = (size_t)N * LDR * sizeof(float);
+  static constexpr size_t smem() {
+    return WPC * PLANE_B + WPC * R_B + N * sizeof(float2) + WPC * (G / 32) * 2 * sizeof(uint32_t) +
+           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int) + 4 * sizeof(float)) + WPC * W * W + 64;
+  }
+  static_assert(W == N || 2 * W == N, "window must equal the FFT size or half of it");
+  static_assert(G >= 32 && G % 32 == 0, "analysis group must be whole warps");
+};
+
+template <int N, int W>
+__global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const CorrArgs a) {
+  using C = CorrCfg<N, W>;
+  constexpr int WPC = C::WPC, NT = C::NT, LD = C::LD, LDR = C::LDR, N1 = C::N1, N2 = C::N2;
+  constexpr int PS = N * LD;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* planes = reinterpret_cast<float2*>(smem_raw);
+  float* Rb = reinterpret_cast<float*>(smem_raw + WPC * C::PLANE_B);
+  float2* tw = reinterpret_cast<float2*>(smem_raw + WPC * C::PLANE_B + WPC * C::R_B);
+  uint32_t* red = reinterpret_cast<uint32_t*>(tw + N);
+  float* s_vals = reinterpret_cast<float*>(red + WPC * (C::G / 32) * 2);
+  int* s_locs = reinterpret_cast<int*>(s_vals + WPC * KMAX);
+  float* s_mean = reinterpret_cast<float*>(s_locs + WPC * 2 * KMAX);  // 4 per window
+  uint8_t* s_mflag = reinterpret_cast<uint8_t*>(s_mean + WPC * 4);
+
+  const int tid = threadIdx.x;
+  const int K = a.npeaks > 2 ? a.npeaks : 2;
+  if (N2 > 1) {
+    for (int m = tid; m < N; m += NT) {
+      double s, c;
+      sincospi(-2.0 * (double)m / (double)N, &s, &c);
+      tw[m] = make_float2((float)c, (float)s);  // W_N^m = exp(-2 pi i m / N)
+    }
+  }
+  const float scale = 1.0f / (float)(N * N);
+  PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
+
+  for (int64_t base = (int64_t)blockIdx.x * WPC; base < a.njobs; base += (int64_t)gridDim.x * WPC) {
+    // ---- stage 1: raw windows -> planes (A in .x, B in .y), mask flags
+    for (int it = tid; it < WPC * W * W; it += NT) {
+      const int p = it % W, q = (it / W) % W, w = it / (W * W);
+      const int64_t job = base + w;
+      float2 z = make_float2(0.f, 0.f);
+      uint8_t mf = 0;
+      if (job < a.njobs) {
+        const int rs = a.jobs[4 * job + 2], cs = a.jobs[4 * job + 3];
+        const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * a.ld;
+        z = make_float2(__ldg(a.A + off), __ldg(a.B + off));
+        if (a.mask) mf = __ldg(a.mask + off);
+      }
+      planes[w * PS + q * LD + p] = z;
+      if (a.mask) s_mflag[w * W * W + q * W + p] = mf;
+    }
+    __syncthreads();
+    // ---- stage 2: window means in the reference's column-major fold order
+    if (tid < 2 * WPC) {
+      const int w = tid >> 1, comp = tid & 1;
+      const float2* P = planes + w * PS;
+      float s = 0.f;
+      int n = 0;
+      if (!a.mask) {
+        s = comp ? P[0].y : P[0].x;
+        for (int k = 1; k < W * W; ++k) {
+          const float2 z = P[(k / W) * LD + (k % W)];
+          s += comp ? z.y : z.x;
+        }
+        n = W * W;
+      } else {
+        for (int k = 0; k < W * W; ++k) {
+          if (s_mflag[w * W * W + k]) continue;
+          const float2 z = P[(k / W) * LD + (k % W)];
+          s += comp ? z.y : z.x;
+          ++n;
+        }
+      }
+      s_mean[4 * w + comp] = n > 0 ? s / (float)n : 0.f;
+    }
+    __syncthreads();
+    // ---- stage 3: apod * (x - mean), masked pixels -> 0
+    for (int it = tid; it < WPC * W * W; it += NT) {
+      const int p = it % W, q = (it / W) % W, w = it / (W * W);
+      const float ap = __ldg(a.apod + q * W + p);
+      float2 z = planes[w * PS + q * LD + p];
+      if (a.mask && s_mflag[w * W * W + q * W + p]) z = make_float2(0.f, 0.f);
+      else z = make_float2(ap * (z.x - s_mean[4 * w]), ap * (z.y - s_mean[4 * w + 1]));
+      planes[w * PS + q * LD + p] = z;
+    }
+    __syncthreads();
+
+    // ---- stage 4: forward transform along p (columns q < W carry data)
+    {
+      const int nl = W;  // nonzero columns
+      for (int it = tid; it < WPC * nl * N2; it += NT) {
+        const int q = it % nl, n2 = (it / nl) % N2, w = it / (nl * N2);
+        float2* L = planes + w * PS + q * LD;
+        float2 x[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) x[n1] = n1 < C::NZ1 ? L[N2 * n1 + n2] : make_float2(0.f, 0.f);
+        RDFT<N1, false>::run(x, C::NZ1);
+        if (N2 > 1) {
+#pragma unroll
+          for (int k1 = 1; k1 < N1; ++k1) x[k1] = cmul(x[k1], tw[(n2 * k1) % N]);
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) L[N2 * k1 + n2] = x[k1];
+      }
+      if (N2 > 1) {
+        __syncthreads();
+        for (int it = tid; it < WPC * nl * N1; it += NT) {
+          const int q = it % nl, k1 = (it / nl) % N1, w = it / (nl * N1);
+          float2* L = planes + w * PS + q * LD + N2 * k1;
+          float2 x[N2];
+#pragma unroll
+          for (int n2 = 0; n2 < N2; ++n2) x[n2] = L[n2];
+          RDFT<N2, false>::run(x, N2);
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) L[k2] = x[k2];
+        }
+      }
+    }
+    __syncthreads();
+    // ---- stage 5: forward transform along q for every row p
+    {
+      for (int it = tid; it < WPC * N * N2; it += NT) {
+        const int p = it % N, n2 = (it / N) % N2, w = it / (N * N2);
+        float2* L = planes + w * PS + p;
+        float2 x[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1)
+          x[n1] = n1 < C::NZ1 ? L[(N2 * n1 + n2) * LD] : make_float2(0.f, 0.f);
+        RDFT<N1, false>::run(x, C::NZ1);
+        if (N2 > 1) {
+#pragma unroll
+          for (int k1 = 1; k1 < N1; ++k1) x[k1] = cmul(x[k1], tw[(n2 * k1) % N]);
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) L[(N2 * k1 + n2) * LD] = x[k1];
+      }
+      if (N2 > 1) {
+        __syncthreads();
+        for (int it = tid; it < WPC * N * N1; it += NT) {
+          const int p = it % N, k1 = (it / N) % N1, w = it / (N * N1);
+          float2* L = planes + w * PS + p + (N2 * k1) * LD;
+          float2 x[N2];
+#pragma unroll
+          for (int n2 = 0; n2 < N2; ++n2) x[n2] = L[n2 * LD];
+          RDFT<N2, false>::run(x, N2);
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) L[k2 * LD] = x[k2];
+        }
+      }
+    }
+    __syncthreads();
+    // ---- stage 6: cross-power (or filtered phase) spectrum, Hermitian pairs
+    for (int it = tid; it < WPC * N * N; it += NT) {
+      const int kp = it % N, kq = (it / N) % N, w = it / (N * N);
+      const int mp = (N - kp) % N, mq = (N - kq) % N;
+      if (kp + kq * N > mp + mq * N) continue;
+      const int ap = N2 * (kp % N1) + kp / N1, aq = N2 * (kq % N1) + kq / N1;
+      const int bp = N2 * (mp % N1) + mp / N1, bq = N2 * (mq % N1) + mq / N1;
+      float2* P = planes + w * PS;
+      const float2 X = P[aq * LD + ap];
+      const float2 Zm = P[bq * LD + bp];
+      const float2 Y = make_float2(Zm.x, -Zm.y);  // conj(Z[-k])
+      // FA = (X + Y)/2, FB = (X - Y)/(2i); S = conj(FA) * FB
+      const float Ar = 0.5f * (X.x + Y.x), Ai = 0.5f * (X.y + Y.y);
+      const float Br = 0.5f * (X.y - Y.y), Bi = -0.5f * (X.x - Y.x);
+      float2 S = cmul(make_float2(Ar, -Ai), make_float2(Br, Bi));
+      if (a.method == 1) {
+        const float den = hypotf(S.x, S.y) + 1.1920929e-7f;  // eps(Float32)
+        const float wk = __ldg(a.phasew + kq * N + kp);
+        S = make_float2((wk * S.x) / den, (wk * S.y) / den);
+      }
+      P[aq * LD + ap] = S;
+      P[bq * LD + bp] = make_float2(S.x, -S.y);
+    }
+    __syncthreads();
+    // ---- stage 7: inverse along q (every row p), back to natural order
+    {
+      if (N2 > 1) {
+        for (int it = tid; it < WPC * N * N1; it += NT) {
+          const int p = it % N, k1 = (it / N) % N1, w = it / (N * N1);
+          float2* L = planes + w * PS + p + (N2 * k1) * LD;
+          float2 x[N2];
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) x[k2] = L[k2 * LD];
+          RDFT<N2, true>::run(x, N2);
+#pragma unroll
+          for (int n2 = 1; n2 < N2; ++n2) {
+            const float2 t = tw[(n2 * k1) % N];
+            x[n2] = cmul(x[n2], make_float2(t.x, -t.y));
+          }
+#pragma unroll
+          for (int n2 = 0; n2 < N2; ++n2) L[n2 * LD] = x[n2];
+        }
+        __syncthreads();
+      }
+      for (int it = tid; it < WPC * N * N2; it += NT) {
+        const int p = it % N, n2 = (it / N) % N2, w = it / (N * N2);
+        float2* L = planes + w * PS + p;
+        float2 x[N1];
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) x[k1] = L[(N2 * k1 + n2) * LD];
+        RDFT<N1, true>::run(x, N1);
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) L[(N2 * n1 + n2) * LD] = x[n1];
+      }
+    }
+    __syncthreads();
+    // ---- stage 8: inverse along p (every column q); epilogue writes the
+    //      fftshifted, normalised, gain-weighted magnitude plane R
+    {
+      if (N2 > 1) {
+        for (int it = tid; it < WPC * N * N1; it += NT) {
+          const int q = it % N, k1 = (it / N) % N1, w = it / (N * N1);
+          float2* L = planes + w * PS + q * LD + N2 * k1;
+          float2 x[N2];
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) x[k2] = L[k2];
+          RDFT<N2, true>::run(x, N2);
+#pragma unroll
+          for (int n2 = 1; n2 < N2; ++n2) {
+            const float2 t = tw[(n2 * k1) % N];
+            x[n2] = cmul(x[n2], make_float2(t.x, -t.y));
+          }
+#pragma unroll
+          for (int n2 = 0; n2 < N2; ++n2) L[n2] = x[n2];
+        }
+        __syncthreads();
+      }
+      for (int it = tid; it < WPC * N * N2; it += NT) {
+        const int q = it % N, n2 = (it / N) % N2, w = it / (N * N2);
+        const float2* L = planes + w * PS + q * LD;
+        float2 x[N1];
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) x[k1] = L[N2 * k1 + n2];
+        RDFT<N1, true>::run(x, N1);
+        const int qs = (q + N / 2) % N;
+        float* Rw = Rb + w * N * LDR;
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) {
+          const int p = N2 * n1 + n2, ps = (p + N / 2) % N;
+          float r = fabsf(x[n1].x) * scale;
+          if (a.gain) r *= __ldg(a.gain + qs * N + ps);
+          Rw[qs * LDR + ps] = r;
+        }
+      }
+    }
+    __syncthreads();
+    if (a.planes) {
+      for (int it = tid; it < WPC * N * N; it += NT) {
+        const int p = it % N, q = (it / N) % N, w = it / (N * N);
+        const int64_t job = base + w;
+        if (job < a.njobs) a.planes[job * (int64_t)(N * N) + q * N + p] = Rb[w * N * LDR + q * LDR + p];
+      }
+    }
+    // ---- stage 9: peak analysis, one thread group per window
+    {
+      const int w = tid / C::G, gt = tid % C::G;
+      const int64_t job = base + w;
+      const bool active = job < a.njobs;
+      int64_t gid = -1;
+      if (active) gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
+      analyze_group(Rb + w * N * LDR, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, C::G,
+                    red + w * (C::G / 32) * 2, active, s_vals + w * KMAX, s_locs + w * 2 * KMAX, gid, job, po);
+    }
+    __syncthreads();
+  }
+}
+
+// Device analysis of caller-supplied planes (one CTA of 128 threads each).
+__global__ void __launch_bounds__(128) analyze_planes_kernel(const AnalyzeArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* R = reinterpret_cast<float*>(smem_raw);
+  const int P = a.nr * a.nc;
+  uint32_t* red = reinterpret_cast<uint32_t*>(R + P);
+  float* s_vals = reinterpret_cast<float*>(red + 8);
+  int* s_locs = reinterpret_cast<int*>(s_vals + KMAX);
+  const int K = a.npeaks > 2 ? a.npeaks : 2;
+  PeakOut po{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, a.packed, a.locs};
+  for (int64_t pl = blockIdx.x; pl < a.nplanes; pl += gridDim.x) {
+    for (int k = threadIdx.x; k < P; k += blockDim.x) R[k] = a.planes[pl * (int64_t)P + k];
+    __syncthreads();
+    analyze_group(R, a.nr, a.nc, a.nr, K, a.npeaks, a.finder, a.subpixel, threadIdx.x, 128, red, true, s_vals,
+                  s_locs, -1, pl, po);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <int N, int W> static cudaError_t launch_nw(const CorrArgs& a, cudaStream_t s, int num_sms) {
+  using C = CorrCfg<N, W>;
+  const size_t sm = C::smem();
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(correlate_kernel<N, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, correlate_kernel<N, W>, C::NT, sm);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  const int64_t units = (a.njobs + C::WPC - 1) / C::WPC;
+  int64_t grid = (int64_t)per_sm * num_sms;
+  if (grid > units) grid = units;
+  if (grid < 1) grid = 1;
+  correlate_kernel<N, W><<<(unsigned)grid, C::NT, sm, s>>>(a);
+  return cudaGetLastError();
+}
+
+#define HH_CORR_CASES(X) \
+  X(16, 8) X(16, 16) X(24, 12) X(24, 24) X(32, 16) X(32, 32) X(48, 24) X(48, 48) X(64, 32) X(64, 64) X(96, 48) \
+  X(96, 96) X(128, 64) X(128, 128)
+
+bool correlate_supported(int N, int W) {
+#define X(n, w) if (N == n && W == w) return true;
+  HH_CORR_CASES(X)
+#undef X
+  return false;
+}
+
+size_t correlate_smem_bytes(int N, int W) {
+#define X(n, w) if (N == n && W == w) return CorrCfg<n, w>::smem();
+  HH_CORR_CASES(X)
+#undef X
+  return 0;
+}
+
+cudaError_t launch_correlate(const CorrArgs& a, int N, int W, cudaStream_t s, int num_sms) {
+  if (a.njobs <= 0) return cudaSuccess;
+#define X(n, w) if (N == n && W == w) return launch_nw<n, w>(a, s, num_sms);
+  HH_CORR_CASES(X)
+#undef X
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_analyze_planes(const AnalyzeArgs& a, cudaStream_t s) {
+  if (a.nplanes <= 0) return cudaSuccess;
+  const size_t sm = (size_t)a.nr * a.nc * sizeof(float) + 8 * sizeof(uint32_t) + KMAX * sizeof(float) +
+                    2 * KMAX * sizeof(int) + 16;
+  if (sm > 200 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(analyze_planes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  int64_t grid = a.nplanes < 4096 ? a.nplanes : 4096;
+  analyze_planes_kernel<<<(unsigned)grid, 128, sm, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace hh

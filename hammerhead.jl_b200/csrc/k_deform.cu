@@ -1,0 +1,306 @@
+// Symmetric image deformation for WIDIM sweeps (sm_100a).
+//
+// prefilter: cubic B-spline coefficients of Interpolations.jl's
+//   BSpline(Cubic(Line(OnGrid()))) on the (nr+2) x (nc+2) padded index set
+//   (the coefficient array image_interpolant builds, src/pipeline.jl:75-85,
+//   909-915): per line, rows [1 4 1]/6 inside and the "Line" boundary rows
+//   c0 - 2c1 + c2 = 0. Eliminating the boundary rows leaves c1 = b1,
+//   c_{n-2} = b_{n-2} and a constant-coefficient tridiagonal system, solved
+//   by the Thomas algorithm with the line-independent elimination factors
+//   precomputed once. Separable: every column, then every row.
+// deform: one thread per output pixel evaluates the predictor by bilinear
+//   interpolation with flat extrapolation (Gridded(Linear()) + Flat(),
+//   src/pipeline.jl:561-600) and samples both coefficient arrays with the
+//   4x4 cubic B-spline at -+ half the displacement, zero outside the image
+//   (deform_columns!, src/pipeline.jl:957-965; _ka_deform!,
+//   src/ka_backend.jl:266-312).
+// All floating-point operations use explicit round-to-nearest intrinsics so
+// no multiply-add is fused: results equal the CPU restatement bit for bit.
+#include <math.h>
+#include <stdint.h>
+
+#include "hh_internal.h"
+
+namespace hh {
+
+#define FM(a, b) __fmul_rn((a), (b))
+#define FA(a, b) __fadd_rn((a), (b))
+#define FS(a, b) __fsub_rn((a), (b))
+#define FD(a, b) __fdiv_rn((a), (b))
+
+// Elimination factors for a line of padded length n: unknown rows
+// i = 3..n-2 (1-based). inv[k] = 1/den_k, cp[k] = (1/6)*inv[k], k = i - 3.
+__global__ void bspline_factors_kernel(int64_t n, float* cp, float* inv) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const float sixth = FD(1.0f, 6.0f), b = FD(4.0f, 6.0f);
+  const int64_t m = n - 4;  // number of unknowns
+  float cprev = 0.f;
+  for (int64_t k = 0; k < m; ++k) {
+    float den = k == 0 ? b : FS(b, FM(sixth, cprev));
+    float iv = FD(1.0f, den);
+    inv[k] = iv;
+    cprev = FM(sixth, iv);
+    cp[k] = cprev;
+  }
+}
+
+// Copy the image into the interior of the zeroed padded array.
+__global__ void pad_copy_kernel(const float* img, int64_t nr, int64_t nc, float* coef) {
+  const int64_t ld = nr + 2, total = ld * (nc + 2);
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = k % ld, j = k / ld;
+    coef[k] = (i >= 1 && i <= nr && j >= 1 && j <= nc) ? img[(i - 1) + (j - 1) * nr] : 0.f;
+  }
+}
+
+// Solve one line (padded length n, element stride es) in place.
+__device__ __forceinline__ void bspline_solve_line(float* x, int64_t n, int64_t es, const float* cp,
+                                                   const float* inv) {
+  if (n < 5) {
+    if (n == 4) {  // c1 = b1, c2 = b2, c0 = 2c1 - c2, c3 = 2c2 - c1
+      const float c1 = x[es], c2 = x[2 * es];
+      x[0] = FS(FM(2.0f, c1), c2);
+      x[3 * es] = FS(FM(2.0f, c2), c1);
+    }
+    return;
+  }
+  const float sixth = FD(1.0f, 6.0f);
+  const float c2 = x[1 * es], cn1 = x[(n - 2) * es];
+  const int64_t m = n - 4;
+  // forward sweep, dp stored in place (rows 3..n-2 -> 0-based 2..n-3)
+  float dprev = 0.f;
+  for (int64_t k = 0; k < m; ++k) {
+    float rhs = x[(k + 2) * es];
+    if (k == 0) rhs = FS(rhs, FM(sixth, c2));
+    if (k == m - 1) rhs = FS(rhs, FM(sixth, cn1));
+    float d = k == 0 ? FM(rhs, inv[0]) : FM(FS(rhs, FM(sixth, dprev)), inv[k]);
+    x[(k + 2) * es] = d;
+    dprev = d;
+  }
+  // backward sweep
+  float xn = x[(m - 1 + 2) * es];
+  for (int64_t k = m - 2; k >= 0; --k) {
+    float xi = FS(x[(k + 2) * es], FM(cp[k], xn));
+    x[(k + 2) * es] = xi;
+    xn = xi;
+  }
+  x[0] = FS(FM(2.0f, x[1 * es]), x[2 * es]);
+  x[(n - 1) * es] = FS(FM(2.0f, x[(n - 2) * es]), x[(n - 3) * es]);
+}
+
+// dim 1: lines are contiguous columns; stage tiles through shared memory so
+// global accesses coalesce while one lane walks each line.
+__global__ void __launch_bounds__(32) bspline_cols_kernel(float* coef, int64_t ld, int64_t ncols, const float* cp,
+                                                          const float* inv) {
+  __shared__ float tile[32][33];
+  const int lane = threadIdx.x;
+  const int64_t j0 = (int64_t)blockIdx.x * 32;
+  const int64_t n = ld;
+  const int64_t m = n - 4;
+  const float sixth = FD(1.0f, 6.0f);
+  const bool mine = (j0 + lane) < ncols;
+  float* myline = coef + (j0 + lane) * ld;
+  if (n < 5) {
+    if (mine) bspline_solve_line(myline, n, 1, cp, inv);
+    return;
+  }
+  float c2 = 0.f, cn1 = 0.f;
+  if (mine) {
+    c2 = myline[1];
+    cn1 = myline[n - 2];
+  }
+  // forward sweep over chunks of 32 rows
+  float dprev = 0.f;
+  for (int64_t i0 = 0; i0 < n; i0 += 32) {
+    for (int l = 0; l < 32; ++l) {
+      const int64_t j = j0 + l, i = i0 + lane;
+      tile[l][lane] = (j < ncols && i < n) ? coef[j * ld + i] : 0.f;
+    }
+    __syncwarp();
+    if (mine) {
+      for (int r = 0; r < 32; ++r) {
+        const int64_t i = i0 + r;
+        const int64_t k = i - 2;
+        if (k < 0 || k >= m) continue;
+        float rhs = tile[lane][r];
+        if (k == 0) rhs = FS(rhs, FM(sixth, c2));
+        if (k == m - 1) rhs = FS(rhs, FM(sixth, cn1));
+        float d = k == 0 ? FM(rhs, inv[0]) : FM(FS(rhs, FM(sixth, dprev)), inv[k]);
+        tile[lane][r] = d;
+        dprev = d;
+      }
+    }
+    __syncwarp();
+    for (int l = 0; l < 32; ++l) {
+      const int64_t j = j0 + l, i = i0 + lane;
+      if (j < ncols && i < n) coef[j * ld + i] = tile[l][lane];
+    }
+    __syncwarp();
+  }
+  // backward sweep over chunks, from the end
+  float xn = 0.f;
+  const int64_t last_chunk = ((n - 1) / 32) * 32;
+  for (int64_t i0 = last_chunk; i0 >= 0; i0 -= 32) {
+    for (int l = 0; l < 32; ++l) {
+      const int64_t j = j0 + l, i = i0 + lane;
+      tile[l][lane] = (j < ncols && i < n) ? coef[j * ld + i] : 0.f;
+    }
+    __syncwarp();
+    if (mine) {
+      for (int r = 31; r >= 0; --r) {
+        const int64_t i = i0 + r;
+        const int64_t k = i - 2;
+        if (k < 0 || k >= m) continue;
+        if (k == m - 1) {
+          xn = tile[lane][r];  // x_last = d_last
+          continue;
+        }
+        float xi = FS(tile[lane][r], FM(cp[k], xn));
+        tile[lane][r] = xi;
+        xn = xi;
+      }
+    }
+    __syncwarp();
+    for (int l = 0; l < 32; ++l) {
+      const int64_t j = j0 + l, i = i0 + lane;
+      if (j < ncols && i < n) coef[j * ld + i] = tile[l][lane];
+    }
+    __syncwarp();
+  }
+  __syncwarp();
+  if (mine) {
+    myline[0] = FS(FM(2.0f, myline[1]), myline[2]);
+    myline[n - 1] = FS(FM(2.0f, myline[n - 2]), myline[n - 3]);
+  }
+}
+
+// dim 2: lines are rows (stride ld); consecutive threads take consecutive
+// rows, so every step of the sweep is a coalesced access.
+__global__ void bspline_rows_kernel(float* coef, int64_t ld, int64_t ncols, const float* cp, const float* inv) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= ld) return;
+  bspline_solve_line(coef + i, ncols, ld, cp, inv);
+}
+
+cudaError_t launch_prefilter(const float* img, int64_t nr, int64_t nc, float* coef, float* scratch,
+                             cudaStream_t s) {
+  // scratch: 2 * (max(nr, nc) + 2) floats for the two factor tables, twice
+  const int64_t ld = nr + 2, ncols = nc + 2;
+  float* cpc = scratch;
+  float* ivc = scratch + ld;
+  float* cpr = scratch + 2 * ld;
+  float* ivr = scratch + 2 * ld + ncols;
+  bspline_factors_kernel<<<1, 1, 0, s>>>(ld, cpc, ivc);
+  bspline_factors_kernel<<<1, 1, 0, s>>>(ncols, cpr, ivr);
+  const int64_t total = ld * ncols;
+  int blocks = (int)((total + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  pad_copy_kernel<<<blocks, 256, 0, s>>>(img, nr, nc, coef);
+  // the two all-zero padding columns stay zero: solve columns 1..nc only
+  bspline_cols_kernel<<<(unsigned)((nc + 31) / 32), 32, 0, s>>>(coef + ld, ld, nc, cpc, ivc);
+  bspline_rows_kernel<<<(unsigned)((ld + 127) / 128), 128, 0, s>>>(coef, ld, ncols, cpr, ivr);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Gridded(Linear()) + Flat() along one axis of uniform knots q0 + k*step.
+__device__ __forceinline__ void lin_axis(float q, float q0, float step, int n, int& i, float& d) {
+  if (n == 1) { i = 0; d = 0.f; return; }
+  const float last = FA(q0, FM((float)(n - 1), step));
+  if (q <= q0) { i = 0; d = 0.f; return; }
+  if (q >= last) { i = n - 2; d = 1.f; return; }
+  i = (int)floorf(FD(FS(q, q0), step));
+  if (i > n - 2) i = n - 2;
+  const float k0 = FA(q0, FM((float)i, step)), k1 = FA(q0, FM((float)(i + 1), step));
+  d = FD(FS(q, k0), FS(k1, k0));
+}
+
+__device__ __forceinline__ float bilinear(const float* f, const PredGrid& g, float qy, float qx) {
+  int iy, ix;
+  float dy, dx;
+  lin_axis(qy, g.y0, g.ysp, g.gny, iy, dy);
+  lin_axis(qx, g.x0, g.xsp, g.gnx, ix, dx);
+  const int iy2 = g.gny == 1 ? iy : iy + 1, ix2 = g.gnx == 1 ? ix : ix + 1;
+  const float f00 = f[iy + ix * g.gny], f01 = f[iy + ix2 * g.gny], f10 = f[iy2 + ix * g.gny],
+              f11 = f[iy2 + ix2 * g.gny];
+  const float a = FA(FM(FS(1.f, dx), f00), FM(dx, f01));
+  const float b = FA(FM(FS(1.f, dx), f10), FM(dx, f11));
+  return FA(FM(FS(1.f, dy), a), FM(dy, b));
+}
+
+// Interpolations' cubic B-spline weights at fractional offset d.
+__device__ __forceinline__ void cubw(float d, float* w) {
+  const float x3 = FM(FM(d, d), d), c = FS(1.f, d), c3 = FM(FM(c, c), c);
+  const float two3 = FD(2.f, 3.f);
+  w[0] = FD(c3, 6.f);
+  w[1] = FA(FS(two3, FM(d, d)), FD(x3, 2.f));
+  w[2] = FA(FS(two3, FM(c, c)), FD(c3, 2.f));
+  w[3] = FD(x3, 6.f);
+}
+
+__device__ __forceinline__ float bspline_eval(const float* C, int64_t nr, int64_t nc, float yy, float xx) {
+  if (yy < 1.f || yy > (float)nr || xx < 1.f || xx > (float)nc) return 0.f;
+  int64_t iy = (int64_t)floorf(yy);
+  if (iy > nr - 1) iy = nr - 1;
+  int64_t ix = (int64_t)floorf(xx);
+  if (ix > nc - 1) ix = nc - 1;
+  float wy[4], wx[4];
+  cubw(FS(yy, (float)iy), wy);
+  cubw(FS(xx, (float)ix), wx);
+  const int64_t ld = nr + 2;
+  const float* base = C + (iy - 1) + (ix - 1) * ld;
+  float s = 0.f;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    float t = 0.f;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) t = FA(t, FM(wx[b], __ldg(base + a + b * ld)));
+    s = FA(s, FM(wy[a], t));
+  }
+  return s;
+}
+
+__global__ void __launch_bounds__(256) deform_kernel(const float* __restrict__ CA, const float* __restrict__ CB,
+                                                     int64_t nr, int64_t nc, const float* __restrict__ pu,
+                                                     const float* __restrict__ pv, PredGrid g, float* wA, float* wB) {
+  const int64_t total = nr * nc;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = k % nr, c = k / nr;
+    const float R = (float)(r + 1), Cc = (float)(c + 1);
+    const float du2 = FD(bilinear(pu, g, R, Cc), 2.f);
+    const float dv2 = FD(bilinear(pv, g, R, Cc), 2.f);
+    wA[k] = bspline_eval(CA, nr, nc, FS(R, dv2), FS(Cc, du2));
+    wB[k] = bspline_eval(CB, nr, nc, FA(R, dv2), FA(Cc, du2));
+  }
+}
+
+cudaError_t launch_deform(const float* CA, const float* CB, int64_t nr, int64_t nc, const float* pu,
+                          const float* pv, PredGrid g, float* wA, float* wB, cudaStream_t s) {
+  const int64_t total = nr * nc;
+  int64_t blocks = (total + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  deform_kernel<<<(unsigned)blocks, 256, 0, s>>>(CA, CB, nr, nc, pu, pv, g, wA, wB);
+  return cudaGetLastError();
+}
+
+__global__ void node_values_kernel(const float* pu, const float* pv, PredGrid g, const float* y, int32_t ny,
+                                   const float* x, int32_t nx, float* u, float* v) {
+  const int64_t total = (int64_t)ny * nx;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+    const int gi = (int)(k % ny), gj = (int)(k / ny);
+    u[k] = bilinear(pu, g, y[gi], x[gj]);
+    v[k] = bilinear(pv, g, y[gi], x[gj]);
+  }
+}
+
+cudaError_t launch_node_values(const float* pu, const float* pv, PredGrid g, const float* y, int32_t ny,
+                               const float* x, int32_t nx, float* u, float* v, cudaStream_t s) {
+  const int64_t total = (int64_t)ny * nx;
+  int64_t blocks = (total + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  if (blocks < 1) blocks = 1;
+  node_values_kernel<<<(unsigned)blocks, 256, 0, s>>>(pu, pv, g, y, ny, x, nx, u, v);
+  return cudaGetLastError();
+}
+
+}  // namespace hh

@@ -1,0 +1,240 @@
+/*
+ * hammerhead_b200.h — C ABI of the B200 (sm_100a) planar-WIDIM library.
+ *
+ * The library is the device half of a Hammerhead.jl backend: every entry
+ * point takes plain pointers and sizes (no Julia, Python or torch types), so
+ * the Julia package extension binds it with `ccall` and the Python host layer
+ * with ctypes. Images are Julia column-major matrices: element (i, j), 1-based,
+ * of an nr x nc image lives at offset (i-1) + (j-1)*nr. Vector grids are
+ * column-major (ny, nx) like `PIVResult{Float32}` fields.
+ *
+ * Each entry point names the reference interface it replaces
+ * (stillyslalom/Hammerhead.jl, path:line).
+ *
+ * Conventions
+ *   - Return value: hh_status (HH_OK == 0). On failure, hh_last_error(ctx)
+ *     (or hh_last_error(NULL) for context-free calls) gives the message.
+ *     Argument errors carry the same text as the reference's ArgumentError.
+ *   - Host pointers are borrowed for the duration of the call. Calls are
+ *     synchronous unless their name ends in _async (stream-ordered on the
+ *     context's stream).
+ *   - One context per PIVWorkspace; a context is not thread-safe
+ *     (src/pipeline.jl:16-19).
+ */
+#ifndef HAMMERHEAD_B200_H
+#define HAMMERHEAD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t hh_status;
+enum {
+  HH_OK = 0,
+  HH_ERR_ARG = 1,          /* invalid argument (ArgumentError / DimensionMismatch) */
+  HH_ERR_OOM = 2,          /* device allocation failed */
+  HH_ERR_CUDA = 3,         /* CUDA runtime error */
+  HH_ERR_TIMEOUT = 4,      /* a bounded device wait gave up */
+  HH_ERR_UNSUPPORTED = 5,  /* option outside the device scope (_ka_scope_check) */
+  HH_ERR_STATE = 6         /* call out of order (e.g. no staged pair) */
+};
+
+/* Correlation method, apodization, subpixel, peak finder: the Symbol
+ * arguments of PIVParameters (src/types.jl:212-291). */
+enum { HH_CROSS = 0, HH_PHASE = 1 };
+enum { HH_APOD_NONE = 0, HH_APOD_GAUSS = 1 };
+enum { HH_GAUSS3 = 0, HH_GAUSS9 = 1, HH_GAUSS2D = 2, HH_SUBPIXEL_NONE = 3 };
+enum { HH_REGIONALMAX = 0, HH_EXCLUSION = 1 };
+/* Extra validators (src/quality.jl:360-503, parse_validator). */
+enum { HH_VAL_PEAK_RATIO = 0, HH_VAL_MOMENT = 1, HH_VAL_VELOCITY = 2, HH_VAL_UOD = 3 };
+
+#define HH_MAX_VALIDATORS 8
+
+typedef struct hh_validator {
+  int32_t kind;          /* HH_VAL_* */
+  int32_t neighborhood;  /* UOD neighbourhood layers */
+  double threshold;      /* peak-ratio / moment / UOD threshold */
+  double vmin, vmax;     /* velocity magnitude bounds */
+  double epsilon;        /* UOD epsilon */
+} hh_validator;
+
+/* Mirror of PIVParameters (src/types.jl:212-291), one per pass. */
+typedef struct hh_pass_desc {
+  int32_t window[2];     /* (rows, cols) */
+  int32_t search[2];     /* search_area_size (rows, cols) */
+  int32_t overlap[2];
+  int32_t method;        /* HH_CROSS / HH_PHASE */
+  int32_t padding;       /* bool */
+  int32_t apodization;   /* HH_APOD_* */
+  int32_t subpixel;      /* HH_GAUSS3 / ... */
+  int32_t n_peaks;
+  int32_t peak_finder;   /* HH_REGIONALMAX / HH_EXCLUSION */
+  int32_t uncertainty;   /* bool */
+  int32_t uod_enable;    /* bool */
+  double uod_threshold;
+  int32_t uod_neighborhood;
+  int32_t replace_outliers; /* bool */
+  double min_peak_ratio;
+  int32_t max_iterations;
+  int32_t keep_correlation_planes; /* bool (rejected by the device scope check) */
+  double convergence_tol;
+  int32_t n_validators;
+  int32_t reserved0;
+  hh_validator validators[HH_MAX_VALIDATORS];
+} hh_pass_desc;
+
+/* Caller-owned host buffers for the final pass of run_piv: the fields of
+ * PIVResult{Float32} (src/types.jl:359-373). Grid dims come from
+ * hh_pass_grid on the final pass. Any pointer may be NULL (not returned). */
+typedef struct hh_result {
+  int32_t ny, nx;        /* filled by the library */
+  float *x, *y;          /* nx, ny */
+  float *u, *v, *peak_ratio, *correlation_moment, *uncertainty_u, *uncertainty_v; /* ny*nx */
+  uint8_t *outliers, *mask;                                                        /* ny*nx */
+} hh_result;
+
+typedef struct hh_ctx hh_ctx;
+
+/* Library identification. */
+const char* hh_version(void);
+/* Message of the last failure on ctx (ctx == NULL: last context-free failure). */
+const char* hh_last_error(const hh_ctx* ctx);
+
+/* Validate one pass descriptor with the checks and messages of the
+ * PIVParameters constructor (src/types.jl:254-285). Host-only. */
+hh_status hh_pass_validate(const hh_pass_desc* p);
+
+/* Reject options the device path does not implement, before any work:
+ * replaces _check_backend_params / _ka_scope_check (src/ka_backend.jl:13-29). */
+hh_status hh_check_backend_params(const hh_pass_desc* passes, int32_t npasses);
+
+/* Interrogation grid of one pass: replaces pass_grid (src/pipeline.jl:529-555).
+ * x (nx), y (ny): window centres; grid_mask (ny*nx) and jobs (4*njobs int32:
+ * gi, gj 1-based grid index, rs, cs 1-based window origin) may be NULL.
+ * Returns the number of jobs in *njobs. Host-only. */
+hh_status hh_pass_grid(int64_t nr, int64_t nc, const hh_pass_desc* p, const uint8_t* mask,
+                       double mask_threshold, int32_t* ny, int32_t* nx, float* x, float* y,
+                       uint8_t* grid_mask, int32_t* jobs, int64_t* njobs);
+
+/* Context: one device, one stream, a growable device arena.
+ * Replaces piv_workspace(; backend = :b200) (src/pipeline.jl:33-44). */
+hh_status hh_ctx_create(int32_t device, hh_ctx** out);
+void hh_ctx_destroy(hh_ctx* ctx);
+/* The context's cudaStream_t (as void*), for callers that time or order work. */
+void* hh_ctx_stream(hh_ctx* ctx);
+
+/* Whole planar-WIDIM schedule for one pair, all passes and sweeps on the
+ * device: replaces run_piv(imgA, imgB, passes; backend) with its pass loop
+ * piv_pass (src/pipeline.jl:361-449, 655-832). A, B host images (nr x nc,
+ * column-major float32), mask optional (uint8, nonzero = excluded). */
+hh_status hh_run_piv(hh_ctx* ctx, const float* A, const float* B, int64_t nr, int64_t nc,
+                     const hh_pass_desc* passes, int32_t npasses, const uint8_t* mask,
+                     double mask_threshold, int32_t predictor_smoothing, hh_result* out);
+
+/* Same, with A, B (and mask) already in device memory of the context's
+ * device; the result is still returned into the host buffers of *out. */
+hh_status hh_run_piv_device(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr, int64_t nc,
+                            const hh_pass_desc* passes, int32_t npasses, const uint8_t* dmask,
+                            double mask_threshold, int32_t predictor_smoothing, hh_result* out);
+
+/* Per-pass timing of the last hh_run_piv* call on ctx, measured with CUDA
+ * events on the context stream: ms[k] = device time of pass k (all sweeps,
+ * deformation, validation, uncertainty); sweeps[k] = sweeps run. */
+hh_status hh_last_pass_times(const hh_ctx* ctx, int32_t npasses, float* ms, int32_t* sweeps);
+
+/* ---- Backend-hook level entry points (the plugin seam of
+ *      docs/src/reference/backends.md:40-71) ---------------------------- */
+
+/* _deform_context: stage a pair (host, column-major) and build its cubic
+ * B-spline coefficients on the device (src/ka_backend.jl:335-351 +
+ * Interpolations prefilter, src/pipeline.jl:75-85). */
+hh_status hh_stage_pair(hh_ctx* ctx, const float* A, const float* B, int64_t nr, int64_t nc);
+
+/* apply_predictor: deform the staged pair by a coarse predictor field
+ * (gny x gnx, column-major, uniform knots y0 + k*ysp, x0 + k*xsp) on the
+ * device; optionally return the warped images (host, nr x nc) and the
+ * predictor at the nodes (ny x nx) of a target grid (y: ny, x: nx).
+ * Replaces apply_predictor / _ka_apply_predictor_ctx (src/pipeline.jl:575-600,
+ * src/ka_backend.jl:357-378). pu == NULL means no predictor (pass-through). */
+hh_status hh_apply_predictor(hh_ctx* ctx, const float* pu, const float* pv, int32_t gny, int32_t gnx,
+                             float y0, float ysp, float x0, float xsp, const float* y, int32_t ny,
+                             const float* x, int32_t nx, float* node_u, float* node_v, float* warpA,
+                             float* warpB);
+
+/* process_windows!: correlate the jobs of one pass on the current (warped
+ * or raw) staged pair and return the packed per-window scalars, layout of
+ * src/ka_backend.jl:497-506: out[(5 + 2*(K-1)) * njobs], K = max(n_peaks, 2),
+ * column j = [du, dv, peak_ratio, moment, found, alt du (K-1), alt dv (K-1)].
+ * jobs: 4*njobs int32 (gi, gj, rs, cs; 1-based). locs (2*K*njobs int32,
+ * 1-based (row, col) plane peaks) and uq (2*44*njobs float64 Wieneke
+ * statistics, src/uncertainty.jl:40-151) may be NULL. Replaces
+ * process_windows! (ext/HammerheadCUDAExt.jl:303-398). */
+hh_status hh_process_windows(hh_ctx* ctx, const hh_pass_desc* p, const int32_t* jobs, int64_t njobs,
+                             float* out, int32_t* locs, double* uq);
+
+/* Device plane analysis on caller-supplied correlation planes (nplanes
+ * column-major nr x nc float32 planes): peak search, subpixel fit, ratio,
+ * moment and alternatives, the same device code process_windows runs.
+ * Output layout as hh_process_windows. Replaces _ka_analyze!
+ * (src/ka_backend.jl:521-687); used for the crafted-plane golden vectors
+ * of test/test_ka.jl:28-71. */
+hh_status hh_analyze_planes(hh_ctx* ctx, const float* planes, int64_t nplanes, int32_t nr, int32_t nc,
+                            int32_t n_peaks, int32_t peak_finder, int32_t subpixel, float* out,
+                            int32_t* locs);
+
+/* Correlation planes (fftshifted, gain-normalised, the plane
+ * correlation_plane! returns, src/correlators.jl:326-341) of the jobs on the
+ * staged pair: planes[fft_rows * fft_cols * njobs]. */
+hh_status hh_correlation_planes(hh_ctx* ctx, const hh_pass_desc* p, const int32_t* jobs, int64_t njobs,
+                                float* planes);
+
+/* validate_and_replace! on a host vector grid, run on the device
+ * (src/pipeline.jl:617-645): UOD, peak ratio, extra validators, mask,
+ * peak substitution (alt_u/alt_v: (ny, nx, nalt) or NULL), replacement.
+ * u, v, outliers are updated in place. */
+hh_status hh_validate(hh_ctx* ctx, const hh_pass_desc* p, int32_t ny, int32_t nx, float* u, float* v,
+                      const float* peak_ratio, const float* moment, uint8_t* outliers, const uint8_t* mask,
+                      const float* alt_u, const float* alt_v, int32_t nalt, int32_t force_replace);
+
+/* universal_outlier_detection (src/quality.jl:244-293) on the device. */
+hh_status hh_uod(hh_ctx* ctx, const float* u, const float* v, int32_t ny, int32_t nx, double threshold,
+                 int32_t neighborhood, double epsilon, const uint8_t* exclude, uint8_t* flags);
+
+/* replace_vectors! (src/quality.jl:85-114) and smooth_field (:123-136). */
+hh_status hh_replace_vectors(hh_ctx* ctx, float* u, float* v, int32_t ny, int32_t nx, const uint8_t* invalid);
+hh_status hh_smooth_field(hh_ctx* ctx, const float* f, int32_t ny, int32_t nx, float* out);
+
+/* field_change (src/pipeline.jl:849-866): 95th-percentile change. */
+hh_status hh_field_change(hh_ctx* ctx, const float* u, const float* v, const float* pu, const float* pv,
+                          const uint8_t* mask, int64_t n, float* change);
+
+/* finalize_uncertainty (src/uncertainty.jl:162-179) of n windows' Wieneke
+ * statistics (2*44 float64 each) into sigma_u, sigma_v. Host-only. */
+hh_status hh_finalize_uncertainty(const double* stats, int64_t n, float* sigma_u, float* sigma_v);
+
+/* ---- Measurement (no counterpart in the reference) --------------------- */
+
+/* Per-kernel-class device time. When profiling is on, every launch of the
+ * correlation, deformation, prefilter, uncertainty and vector-grid kernels
+ * on ctx is bracketed by CUDA events on the context stream, and the
+ * algorithmic work of the launch (FLOPs, bytes) is accumulated with it. */
+enum { HH_K_CORRELATE = 0, HH_K_DEFORM = 1, HH_K_PREFILTER = 2, HH_K_UQ = 3, HH_K_VECTOR = 4, HH_K_CLASSES = 5 };
+typedef struct hh_kernel_profile {
+  int64_t launches;
+  double ms;       /* summed device time */
+  double flops;    /* algorithmic floating-point operations */
+  double bytes;    /* algorithmic DRAM bytes */
+  int64_t units;   /* windows (correlate, uq), pixels (deform, prefilter), vectors */
+} hh_kernel_profile;
+hh_status hh_set_profiling(hh_ctx* ctx, int32_t enable);
+hh_status hh_profile_read(hh_ctx* ctx, hh_kernel_profile* out /* HH_K_CLASSES entries */, int32_t reset);
+/* Kernels launched on ctx since creation (all classes, profiling or not). */
+int64_t hh_launch_count(const hh_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HAMMERHEAD_B200_H */

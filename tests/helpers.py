@@ -1,0 +1,54 @@
+"""Test-image helpers restating test/runtests.jl:11-34 of the reference.
+
+add_particle!: a Gaussian particle with diameter ~ 2 sigma, cut at 5 sigma.
+particle_pair: the same particles displaced by (dv, du) = (drow, dcol).
+Positions are (row, col), 1-based, like the Julia tests. The reference draws
+positions from Julia RNG streams that do not exist here; tests draw them
+from numpy generators with the same distributions.
+"""
+import numpy as np
+
+
+def add_particle(array, centroid, diameter):
+    sigma = diameter / 2
+    nr, nc = array.shape
+    i = np.arange(1, nr + 1)[:, None]
+    j = np.arange(1, nc + 1)[None, :]
+    d2 = (i - centroid[0]) ** 2 + (j - centroid[1]) ** 2
+    val = np.exp(-0.5 * d2 / sigma ** 2)
+    array += np.where(d2 > (5 * sigma) ** 2, 0.0, val)
+    return array
+
+
+def particle_pair(image_size, positions, dv, du, diameter=3.0):
+    A = np.zeros(image_size, np.float64)
+    B = np.zeros(image_size, np.float64)
+    for p in positions:
+        add_particle(A, p, diameter)
+        add_particle(B, (p[0] + dv, p[1] + du), diameter)
+    return np.asfortranarray(A), np.asfortranarray(B)
+
+
+def random_positions(rng, n, extent, margin=10):
+    return [(rng.uniform() * (extent + 2 * margin) - margin, rng.uniform() * (extent + 2 * margin) - margin)
+            for _ in range(n)]
+
+
+def shear_pair(seed, n=128, a=1 / 16, count=900):
+    """u(y) = a (y - 64), v = 0 (test/runtests.jl:338-352)."""
+    rng = np.random.default_rng(seed)
+    A = np.zeros((n, n))
+    B = np.zeros((n, n))
+    for _ in range(count):
+        p = (rng.uniform() * (n + 20) - 10, rng.uniform() * (n + 20) - 10)
+        add_particle(A, p, 3.0)
+        add_particle(B, (p[0], p[1] + a * (p[0] - 64)), 3.0)
+    return np.asfortranarray(A), np.asfortranarray(B)
+
+
+class Grid:
+    """Duck-typed result for error statistics over an oracle output dict."""
+
+    def __init__(self, d):
+        for k in ("x", "y", "u", "v", "mask", "outliers"):
+            setattr(self, k, d[k])
