@@ -48,6 +48,7 @@ struct hh_ctx {
   std::string err;
   std::map<std::string, DevBuf> bufs;
   std::map<TableKey, Tables> tables;
+  std::map<int64_t, std::pair<float*, float*>> bs_factors;  // line length -> (cp, inv)
   float* pinned = nullptr;  // small pinned scratch for scalar reads
   // staged pair for the hook-level entry points
   int64_t nr = 0, nc = 0;
@@ -260,6 +261,22 @@ hh_status set_device(hh_ctx* ctx) {
   return HH_OK;
 }
 
+// B-spline elimination factors of one line length, built once per context.
+hh_status bs_factors(hh_ctx* ctx, int64_t n, float** cp, float** inv) {
+  auto it = ctx->bs_factors.find(n);
+  if (it == ctx->bs_factors.end()) {
+    float *a = nullptr, *b = nullptr;
+    HH_CK(cudaMalloc(&a, std::max<int64_t>(n, 1) * sizeof(float)));
+    HH_CK(cudaMalloc(&b, std::max<int64_t>(n, 1) * sizeof(float)));
+    HH_CK(hh::launch_bspline_factors(n, a, b, ctx->stream));
+    ctx->launches += 1;
+    it = ctx->bs_factors.emplace(n, std::make_pair(a, b)).first;
+  }
+  *cp = it->second.first;
+  *inv = it->second.second;
+  return HH_OK;
+}
+
 cudaEvent_t pool_event(hh_ctx* ctx) {
   if (!ctx->evpool.empty()) {
     cudaEvent_t e = ctx->evpool.back();
@@ -322,6 +339,19 @@ double corr_flops(int N, int64_t njobs) {
 double corr_bytes(int W, int nalt, int64_t njobs) { return (double)njobs * (2.0 * W * W * 4 + 4.0 * (4 + 2 * nalt)); }
 double uq_flops(int W, int64_t njobs) { return (double)njobs * 2.0 * 2.0 * (3 + 41) * W * (W - 1); }
 
+// Cubic B-spline coefficients of both images of a pair.
+hh_status prefilter_pair(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr, int64_t nc, float* cA, float* cB) {
+  float *cpc, *ivc, *cpr, *ivr, *bsd;
+  HH_TRY(bs_factors(ctx, nr + 2, &cpc, &ivc));
+  HH_TRY(bs_factors(ctx, nc + 2, &cpr, &ivr));
+  HH_TRY(buf(ctx, "bs_dbuf", (size_t)(nr + 2) * (nc + 2), &bsd));
+  const double P = (double)nr * nc;
+  HH_K(HH_K_PREFILTER, 5, 12 * P, 8 * P, (int64_t)P, hh::launch_prefilter(dA, nr, nc, cA, bsd, cpc, ivc, cpr, ivr, ctx->stream));
+  HH_K(HH_K_PREFILTER, 5, 12 * P, 8 * P, (int64_t)P, hh::launch_prefilter(dB, nr, nc, cB, bsd, cpc, ivc, cpr, ivr, ctx->stream));
+  return HH_OK;
+}
+
+
 // validate_and_replace! (src/pipeline.jl:617-645) on device buffers.
 hh_status validate_device(hh_ctx* ctx, const hh_pass_desc& p, int ny, int nx, float* u, float* v, const float* ratio,
                           const float* moment, uint8_t* outl, uint8_t* outl2, const uint8_t* gmask, bool any_mask,
@@ -379,13 +409,12 @@ hh_status run_schedule(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr
   if (!(thr > 0 && thr <= 1)) return fail(ctx, HH_ERR_ARG, "mask_threshold must be in (0, 1], got " + num(thr));
   const bool deforms = np > 1 || std::any_of(passes, passes + np, [](const hh_pass_desc& p) { return p.max_iterations > 1; });
   const int64_t P = nr * nc;
-  float *coefA = nullptr, *coefB = nullptr, *warpA = nullptr, *warpB = nullptr, *pref = nullptr;
+  float *coefA = nullptr, *coefB = nullptr, *warpA = nullptr, *warpB = nullptr;
   if (deforms) {
     HH_TRY(buf(ctx, "coefA", (size_t)(nr + 2) * (nc + 2), &coefA));
     HH_TRY(buf(ctx, "coefB", (size_t)(nr + 2) * (nc + 2), &coefB));
     HH_TRY(buf(ctx, "warpA", (size_t)P, &warpA));
     HH_TRY(buf(ctx, "warpB", (size_t)P, &warpB));
-    HH_TRY(buf(ctx, "prefilter", (size_t)4 * (std::max(nr, nc) + 2), &pref));
   }
   // grids of every pass (host) and the largest grid
   std::vector<Grid> grids(np);
@@ -441,8 +470,7 @@ hh_status run_schedule(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr
 
   HH_CK(cudaEventRecord(ctx->events[0], s));
   if (deforms) {
-    HH_K(HH_K_PREFILTER, 5, 12 * P, 8 * P, P, hh::launch_prefilter(dA, nr, nc, coefA, pref, s));
-    HH_K(HH_K_PREFILTER, 5, 12 * P, 8 * P, P, hh::launch_prefilter(dB, nr, nc, coefB, pref, s));  // stream-ordered: the factors are rebuilt
+    HH_TRY(prefilter_pair(ctx, dA, dB, nr, nc, coefA, coefB));
   }
   bool have_pred = false;
   hh::PredGrid pg{};
@@ -775,6 +803,10 @@ void hh_ctx_destroy(hh_ctx* ctx) {
     if (kv.second.gain) cudaFree(kv.second.gain);
     if (kv.second.phasew) cudaFree(kv.second.phasew);
   }
+  for (auto& kv : ctx->bs_factors) {
+    cudaFree(kv.second.first);
+    cudaFree(kv.second.second);
+  }
   for (auto e : ctx->events) cudaEventDestroy(e);
   for (auto e : ctx->evpool) cudaEventDestroy(e);
   for (auto& q : ctx->pending) {
@@ -841,16 +873,14 @@ hh_status hh_stage_pair(hh_ctx* ctx, const float* A, const float* B, int64_t nr,
   HH_TRY(set_device(ctx));
   if (!A || !B || nr < 1 || nc < 1) return fail(ctx, HH_ERR_ARG, "invalid image arguments");
   const int64_t P = nr * nc;
-  float *dA, *dB, *cA, *cB, *pref;
+  float *dA, *dB, *cA, *cB;
   HH_TRY(buf(ctx, "imgA", (size_t)P, &dA));
   HH_TRY(buf(ctx, "imgB", (size_t)P, &dB));
   HH_TRY(buf(ctx, "coefA", (size_t)(nr + 2) * (nc + 2), &cA));
   HH_TRY(buf(ctx, "coefB", (size_t)(nr + 2) * (nc + 2), &cB));
-  HH_TRY(buf(ctx, "prefilter", (size_t)4 * (std::max(nr, nc) + 2), &pref));
   HH_CK(cudaMemcpyAsync(dA, A, P * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
   HH_CK(cudaMemcpyAsync(dB, B, P * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-  HH_K(HH_K_PREFILTER, 5, 0, 0, 0, hh::launch_prefilter(dA, nr, nc, cA, pref, ctx->stream));
-  HH_K(HH_K_PREFILTER, 5, 0, 0, 0, hh::launch_prefilter(dB, nr, nc, cB, pref, ctx->stream));
+  HH_TRY(prefilter_pair(ctx, dA, dB, nr, nc, cA, cB));
   HH_CK(cudaStreamSynchronize(ctx->stream));
   ctx->nr = nr;
   ctx->nc = nc;

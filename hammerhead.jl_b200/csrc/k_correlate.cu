@@ -214,18 +214,52 @@ __device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, in
   const int P = nr * nc;
   int nfound = 0;
   if (finder == 0) {
-    // regional maxima: per-thread top-K over a strided scan, then K merges
+    // regional maxima (src/localmax.jl:3-19): each thread walks column strips
+    // top to bottom keeping the 3x3 neighbourhood in registers (3 loads per
+    // pixel). Earlier neighbours in column-major order (the left column and
+    // the pixel above) must not exceed the value, later ones (the right
+    // column and the pixel below) must stay below it; fmaxf drops NaN
+    // neighbours, which never block in the reference either.
     TopK tk;
     tk.init();
     if (active) {
-      for (int lin = gtid; lin < P; lin += gsize) {
-        const int r = lin % nr, c = lin / nr;
-        const float v = R[c * ldr + r];
-        if (isnan(v)) continue;
-        const uint32_t h = fkey(v);
-        if (tk.cnt == K && h <= tk.hi[K - 1]) continue;  // later index cannot win a tie
-        if (!is_local_max(R, nr, nc, ldr, r, c, v)) continue;
-        tk.insert(h, ~(uint32_t)lin, K);
+      const int S = gsize / nc > 0 ? gsize / nc : 1;  // row segments per column
+      const int rps = (nr + S - 1) / S;
+      const float NaNf = __int_as_float(0x7fc00000);
+      for (int strip = gtid; strip < nc * S; strip += gsize) {
+        const int c = strip % nc, seg = strip / nc;
+        const int r0 = seg * rps, r1 = min(nr, r0 + rps);
+        if (r0 >= r1) continue;
+        const float* Cl = c > 0 ? R + (c - 1) * ldr : nullptr;
+        const float* Cc = R + c * ldr;
+        const float* Cr = c < nc - 1 ? R + (c + 1) * ldr : nullptr;
+        float lt = NaNf, ct = NaNf, rt = NaNf;  // row r - 1
+        if (r0 > 0) {
+          lt = Cl ? Cl[r0 - 1] : NaNf;
+          ct = Cc[r0 - 1];
+          rt = Cr ? Cr[r0 - 1] : NaNf;
+        }
+        float lm = Cl ? Cl[r0] : NaNf, cm = Cc[r0], rm = Cr ? Cr[r0] : NaNf;  // row r
+        for (int r = r0; r < r1; ++r) {
+          float lb = NaNf, cb = NaNf, rb = NaNf;  // row r + 1
+          if (r + 1 < nr) {
+            lb = Cl ? Cl[r + 1] : NaNf;
+            cb = Cc[r + 1];
+            rb = Cr ? Cr[r + 1] : NaNf;
+          }
+          const float v = cm;
+          if (!isnan(v)) {
+            const uint32_t h = fkey(v);
+            // a later index cannot win a tie, so a full list rejects h <= last
+            if (tk.cnt < K || h > tk.hi[K - 1]) {
+              const float e = fmaxf(fmaxf(lt, lm), fmaxf(lb, ct));
+              const float l = fmaxf(fmaxf(rt, rm), fmaxf(rb, cb));
+              if (!(e > v) && !(l >= v)) tk.insert(h, ~(uint32_t)(r + c * nr), K);
+            }
+          }
+          lt = lm; ct = cm; rt = rm;
+          lm = lb; cm = cb; rm = rb;
+        }
       }
     }
     bool done = false;
@@ -281,8 +315,11 @@ __device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, in
       __syncthreads();  // s_locs visible to the next round's exclusion test
     }
   }
-  if (gtid != 0 || !active) return;
-  // found = leading peaks whose secondaries are positive
+  // Epilogue on the group's first warp: lane 0 refines the primary and forms
+  // ratio and moment, lanes 1..K-1 refine the alternatives in parallel.
+  if (gtid >= 32 || !active) return;
+  __syncwarp();  // s_vals / s_locs written by lane 0 after the last merge round
+  const int lane = gtid;
   int found = 0;
   if (nfound > 0) {
     found = 1;
@@ -290,95 +327,94 @@ __device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, in
   }
   const float NaN = __int_as_float(0x7fc00000);
   const int cr = nr / 2 + 1, cc = nc / 2 + 1;
-  float du = NaN, dv = NaN, ratio = NaN, mom = NaN;
-  float alt_du[KMAX], alt_dv[KMAX];
-#pragma unroll
-  for (int m = 0; m < KMAX; ++m) alt_du[m] = alt_dv[m] = NaN;
-  if (found > 0) {
-    float ref[2];
-    const int pr = s_locs[0], pc = s_locs[1];
-    if (subpixel == 1) gauss9_fp64(R, nr, nc, ldr, pr, pc, ref);
-    else if (subpixel == 3) { ref[0] = (float)(pr + 1); ref[1] = (float)(pc + 1); }
+  if (lane >= K) return;
+  float ref[2] = {NaN, NaN};
+  const int mmax = found < npeaks ? found : npeaks;  // peaks 1..mmax carry results
+  if (lane < found && (lane == 0 || lane < mmax)) {
+    const int pr = s_locs[2 * lane], pc = s_locs[2 * lane + 1];
+    if (lane == 0 && subpixel == 1) gauss9_fp64(R, nr, nc, ldr, pr, pc, ref);
+    else if (lane == 0 && subpixel == 3) { ref[0] = (float)(pr + 1); ref[1] = (float)(pc + 1); }
     else gauss3_fp64(R, nr, nc, ldr, pr, pc, ref);
-    du = ref[1] - (float)cc;
-    dv = ref[0] - (float)cr;
-    const float v1 = s_vals[0];
-    ratio = found >= 2 ? v1 / s_vals[1] : (v1 > 0.f ? INFINITY : NaN);
-    mom = moment_fp64(R, nr, nc, ldr, ref[0], ref[1]);
-    const int mmax = found < npeaks ? found : npeaks;
-    for (int m = 2; m <= mmax; ++m) {
-      float a[2];
-      gauss3_fp64(R, nr, nc, ldr, s_locs[2 * (m - 1)], s_locs[2 * (m - 1) + 1], a);
-      alt_du[m - 2] = a[1] - (float)cc;
-      alt_dv[m - 2] = a[0] - (float)cr;
+  }
+  const float d_col = ref[1] - (float)cc, d_row = ref[0] - (float)cr;
+  if (lane == 0) {
+    float ratio = NaN, mom = NaN;
+    if (found > 0) {
+      const float v1 = s_vals[0];
+      ratio = found >= 2 ? v1 / s_vals[1] : (v1 > 0.f ? INFINITY : NaN);
+      mom = moment_fp64(R, nr, nc, ldr, ref[0], ref[1]);
     }
-  }
-  if (grid_id >= 0 && o.du) {
-    o.du[grid_id] = du;
-    o.dv[grid_id] = dv;
-    o.ratio[grid_id] = ratio;
-    o.moment[grid_id] = mom;
-    if (o.alt_u)
-      for (int m = 0; m < o.nalt; ++m) {
-        o.alt_u[grid_id + (int64_t)m * o.G] = alt_du[m];
-        o.alt_v[grid_id + (int64_t)m * o.G] = alt_dv[m];
-      }
-  }
-  if (o.packed) {
-    float* pk = o.packed + job * (int64_t)(5 + 2 * (K - 1));
-    pk[0] = du;
-    pk[1] = dv;
-    pk[2] = ratio;
-    pk[3] = mom;
-    pk[4] = (float)found;
-    for (int m = 0; m < K - 1; ++m) {
-      pk[5 + m] = alt_du[m];
-      pk[5 + (K - 1) + m] = alt_dv[m];
+    if (grid_id >= 0 && o.du) {
+      o.du[grid_id] = d_col;
+      o.dv[grid_id] = d_row;
+      o.ratio[grid_id] = ratio;
+      o.moment[grid_id] = mom;
+    }
+    if (o.packed) {
+      float* pk = o.packed + job * (int64_t)(5 + 2 * (K - 1));
+      pk[0] = d_col;
+      pk[1] = d_row;
+      pk[2] = ratio;
+      pk[3] = mom;
+      pk[4] = (float)found;
+    }
+  } else {
+    // alternative peak `lane` (0-based): result only while lane < min(found, npeaks)
+    const bool has = lane < mmax;
+    const float au = has ? d_col : NaN, av = has ? d_row : NaN;
+    if (grid_id >= 0 && o.alt_u && lane - 1 < o.nalt) {
+      o.alt_u[grid_id + (int64_t)(lane - 1) * o.G] = au;
+      o.alt_v[grid_id + (int64_t)(lane - 1) * o.G] = av;
+    }
+    if (o.packed) {
+      float* pk = o.packed + job * (int64_t)(5 + 2 * (K - 1));
+      pk[5 + (lane - 1)] = au;
+      pk[5 + (K - 1) + (lane - 1)] = av;
     }
   }
   if (o.locs) {
     int32_t* lc = o.locs + job * (int64_t)(2 * K);
-    for (int m = 0; m < K; ++m) {
-      lc[2 * m] = m < found ? s_locs[2 * m] + 1 : 0;
-      lc[2 * m + 1] = m < found ? s_locs[2 * m + 1] + 1 : 0;
-    }
+    lc[2 * lane] = lane < found ? s_locs[2 * lane] + 1 : 0;
+    lc[2 * lane + 1] = lane < found ? s_locs[2 * lane + 1] + 1 : 0;
   }
 }
 
 // ---------------------------------------------------------------------------
 template <int N, int W> struct CorrCfg {
   static constexpr int N1 = AxisSplit<N>::N1, N2 = AxisSplit<N>::N2;
-  static constexpr int WPC = N <= 32 ? 4 : (N <= 48 ? 2 : (N <= 64 ? 2 : 1));
-  static constexpr int NT = N <= 48 ? 128 : 256;
+  static constexpr int WPC = N <= 32 ? 4 : (N <= 64 ? 2 : 1);    // windows per CTA
+  static constexpr int NT = N <= 48 ? 128 : (N <= 64 ? 256 : 512);
   static constexpr int G = NT / WPC;  // threads per window in the analysis
-  static constexpr int LD = N + 1;    // complex plane leading dimension
-  static constexpr int LDR = N + 1;   // real plane leading dimension
+  static constexpr int LD = N + 1;    // complex plane leading dimension (float2)
+  static constexpr int LDR = N + 1;   // real plane leading dimension (float), overlays the complex plane
   static constexpr bool PADDED = (W * 2 == N);
   static constexpr int NZ1 = PADDED ? (W / N2) : N1;  // nonzero inputs of a forward pass-A line
+  static constexpr int IPT = (WPC * N * N2 + NT - 1) / NT;  // final inverse items per thread
   static constexpr size_t PLANE_B = (size_t)N * LD * sizeof(float2);
-  static constexpr size_t R_B = (size_t)N * LDR * sizeof(float);
   static constexpr size_t smem() {
-    return WPC * PLANE_B + WPC * R_B + N * sizeof(float2) + WPC * (G / 32) * 2 * sizeof(uint32_t) +
-           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int) + 4 * sizeof(float)) + WPC * W * W + 64;
+    return WPC * PLANE_B + N * sizeof(float2) + WPC * (G / 32) * 2 * sizeof(uint32_t) +
+           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int) + 4 * sizeof(float) + 2 * sizeof(int)) +
+           WPC * W * W + 64;
   }
   static_assert(W == N || 2 * W == N, "window must equal the FFT size or half of it");
   static_assert(G >= 32 && G % 32 == 0, "analysis group must be whole warps");
+  static_assert(N * LDR <= 2 * N * LD, "real plane must fit in the complex plane");
 };
 
 template <int N, int W>
 __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const CorrArgs a) {
   using C = CorrCfg<N, W>;
-  constexpr int WPC = C::WPC, NT = C::NT, LD = C::LD, LDR = C::LDR, N1 = C::N1, N2 = C::N2;
+  constexpr int WPC = C::WPC, NT = C::NT, LD = C::LD, LDR = C::LDR, N1 = C::N1, N2 = C::N2, IPT = C::IPT;
   constexpr int PS = N * LD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* planes = reinterpret_cast<float2*>(smem_raw);
-  float* Rb = reinterpret_cast<float*>(smem_raw + WPC * C::PLANE_B);
-  float2* tw = reinterpret_cast<float2*>(smem_raw + WPC * C::PLANE_B + WPC * C::R_B);
+  float2* tw = reinterpret_cast<float2*>(smem_raw + WPC * C::PLANE_B);
   uint32_t* red = reinterpret_cast<uint32_t*>(tw + N);
   float* s_vals = reinterpret_cast<float*>(red + WPC * (C::G / 32) * 2);
   int* s_locs = reinterpret_cast<int*>(s_vals + WPC * KMAX);
   float* s_mean = reinterpret_cast<float*>(s_locs + WPC * 2 * KMAX);  // 4 per window
-  uint8_t* s_mflag = reinterpret_cast<uint8_t*>(s_mean + WPC * 4);
+  int* s_job = reinterpret_cast<int*>(s_mean + WPC * 4);              // rs, cs per window
+  uint8_t* s_mflag = reinterpret_cast<uint8_t*>(s_job + WPC * 2);
 
   const int tid = threadIdx.x;
   const int K = a.npeaks > 2 ? a.npeaks : 2;
@@ -393,14 +429,19 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
   PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
 
   for (int64_t base = (int64_t)blockIdx.x * WPC; base < a.njobs; base += (int64_t)gridDim.x * WPC) {
+    if (tid < WPC) {
+      const int64_t job = base + tid;
+      s_job[2 * tid] = job < a.njobs ? a.jobs[4 * job + 2] : -1;
+      s_job[2 * tid + 1] = job < a.njobs ? a.jobs[4 * job + 3] : -1;
+    }
+    __syncthreads();
     // ---- stage 1: raw windows -> planes (A in .x, B in .y), mask flags
     for (int it = tid; it < WPC * W * W; it += NT) {
       const int p = it % W, q = (it / W) % W, w = it / (W * W);
-      const int64_t job = base + w;
+      const int rs = s_job[2 * w], cs = s_job[2 * w + 1];
       float2 z = make_float2(0.f, 0.f);
       uint8_t mf = 0;
-      if (job < a.njobs) {
-        const int rs = a.jobs[4 * job + 2], cs = a.jobs[4 * job + 3];
+      if (rs >= 0) {
         const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * a.ld;
         z = make_float2(__ldg(a.A + off), __ldg(a.B + off));
         if (a.mask) mf = __ldg(a.mask + off);
@@ -410,27 +451,33 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
     }
     __syncthreads();
     // ---- stage 2: window means in the reference's column-major fold order
-    if (tid < 2 * WPC) {
-      const int w = tid >> 1, comp = tid & 1;
-      const float2* P = planes + w * PS;
-      float s = 0.f;
+    //      (one lane per window folds both frames; loads are independent of
+    //      the running sums, so the unrolled loop is bound by the add chain)
+    if (tid < WPC) {
+      const float2* P = planes + tid * PS;
+      float sa = 0.f, sb = 0.f;
       int n = 0;
       if (!a.mask) {
-        s = comp ? P[0].y : P[0].x;
+        sa = P[0].x;
+        sb = P[0].y;
+#pragma unroll 8
         for (int k = 1; k < W * W; ++k) {
           const float2 z = P[(k / W) * LD + (k % W)];
-          s += comp ? z.y : z.x;
+          sa += z.x;
+          sb += z.y;
         }
         n = W * W;
       } else {
         for (int k = 0; k < W * W; ++k) {
-          if (s_mflag[w * W * W + k]) continue;
+          if (s_mflag[tid * W * W + k]) continue;
           const float2 z = P[(k / W) * LD + (k % W)];
-          s += comp ? z.y : z.x;
+          sa += z.x;
+          sb += z.y;
           ++n;
         }
       }
-      s_mean[4 * w + comp] = n > 0 ? s / (float)n : 0.f;
+      s_mean[4 * tid] = n > 0 ? sa / (float)n : 0.f;
+      s_mean[4 * tid + 1] = n > 0 ? sb / (float)n : 0.f;
     }
     __syncthreads();
     // ---- stage 3: apod * (x - mean), masked pixels -> 0
@@ -444,77 +491,72 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
     }
     __syncthreads();
 
-    // ---- stage 4: forward transform along p (columns q < W carry data)
-    {
-      const int nl = W;  // nonzero columns
-      for (int it = tid; it < WPC * nl * N2; it += NT) {
-        const int q = it % nl, n2 = (it / nl) % N2, w = it / (nl * N2);
-        float2* L = planes + w * PS + q * LD;
-        float2 x[N1];
+    // ---- stage 4: forward transform along p (only the W data columns)
+    for (int it = tid; it < WPC * W * N2; it += NT) {
+      const int q = it % W, n2 = (it / W) % N2, w = it / (W * N2);
+      float2* L = planes + w * PS + q * LD;
+      float2 x[N1];
 #pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1) x[n1] = n1 < C::NZ1 ? L[N2 * n1 + n2] : make_float2(0.f, 0.f);
-        RDFT<N1, false>::run(x, C::NZ1);
-        if (N2 > 1) {
-#pragma unroll
-          for (int k1 = 1; k1 < N1; ++k1) x[k1] = cmul(x[k1], tw[(n2 * k1) % N]);
-        }
-#pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) L[N2 * k1 + n2] = x[k1];
-      }
+      for (int n1 = 0; n1 < N1; ++n1) x[n1] = n1 < C::NZ1 ? L[N2 * n1 + n2] : make_float2(0.f, 0.f);
+      RDFT<N1, false>::run(x, C::NZ1);
       if (N2 > 1) {
-        __syncthreads();
-        for (int it = tid; it < WPC * nl * N1; it += NT) {
-          const int q = it % nl, k1 = (it / nl) % N1, w = it / (nl * N1);
-          float2* L = planes + w * PS + q * LD + N2 * k1;
-          float2 x[N2];
 #pragma unroll
-          for (int n2 = 0; n2 < N2; ++n2) x[n2] = L[n2];
-          RDFT<N2, false>::run(x, N2);
+        for (int k1 = 1; k1 < N1; ++k1) x[k1] = cmul(x[k1], tw[(n2 * k1) % N]);
+      }
 #pragma unroll
-          for (int k2 = 0; k2 < N2; ++k2) L[k2] = x[k2];
-        }
+      for (int k1 = 0; k1 < N1; ++k1) L[N2 * k1 + n2] = x[k1];
+    }
+    if (N2 > 1) {
+      __syncthreads();
+      for (int it = tid; it < WPC * W * N1; it += NT) {
+        const int q = it % W, k1 = (it / W) % N1, w = it / (W * N1);
+        float2* L = planes + w * PS + q * LD + N2 * k1;
+        float2 x[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) x[n2] = L[n2];
+        RDFT<N2, false>::run(x, N2);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) L[k2] = x[k2];
       }
     }
     __syncthreads();
     // ---- stage 5: forward transform along q for every row p
-    {
-      for (int it = tid; it < WPC * N * N2; it += NT) {
-        const int p = it % N, n2 = (it / N) % N2, w = it / (N * N2);
-        float2* L = planes + w * PS + p;
-        float2 x[N1];
+    for (int it = tid; it < WPC * N * N2; it += NT) {
+      const int p = it % N, n2 = (it / N) % N2, w = it / (N * N2);
+      float2* L = planes + w * PS + p;
+      float2 x[N1];
 #pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1)
-          x[n1] = n1 < C::NZ1 ? L[(N2 * n1 + n2) * LD] : make_float2(0.f, 0.f);
-        RDFT<N1, false>::run(x, C::NZ1);
-        if (N2 > 1) {
-#pragma unroll
-          for (int k1 = 1; k1 < N1; ++k1) x[k1] = cmul(x[k1], tw[(n2 * k1) % N]);
-        }
-#pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) L[(N2 * k1 + n2) * LD] = x[k1];
-      }
+      for (int n1 = 0; n1 < N1; ++n1) x[n1] = n1 < C::NZ1 ? L[(N2 * n1 + n2) * LD] : make_float2(0.f, 0.f);
+      RDFT<N1, false>::run(x, C::NZ1);
       if (N2 > 1) {
-        __syncthreads();
-        for (int it = tid; it < WPC * N * N1; it += NT) {
-          const int p = it % N, k1 = (it / N) % N1, w = it / (N * N1);
-          float2* L = planes + w * PS + p + (N2 * k1) * LD;
-          float2 x[N2];
 #pragma unroll
-          for (int n2 = 0; n2 < N2; ++n2) x[n2] = L[n2 * LD];
-          RDFT<N2, false>::run(x, N2);
+        for (int k1 = 1; k1 < N1; ++k1) x[k1] = cmul(x[k1], tw[(n2 * k1) % N]);
+      }
 #pragma unroll
-          for (int k2 = 0; k2 < N2; ++k2) L[k2 * LD] = x[k2];
-        }
+      for (int k1 = 0; k1 < N1; ++k1) L[(N2 * k1 + n2) * LD] = x[k1];
+    }
+    if (N2 > 1) {
+      __syncthreads();
+      for (int it = tid; it < WPC * N * N1; it += NT) {
+        const int p = it % N, k1 = (it / N) % N1, w = it / (N * N1);
+        float2* L = planes + w * PS + p + (N2 * k1) * LD;
+        float2 x[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) x[n2] = L[n2 * LD];
+        RDFT<N2, false>::run(x, N2);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) L[k2 * LD] = x[k2];
       }
     }
     __syncthreads();
-    // ---- stage 6: cross-power (or filtered phase) spectrum, Hermitian pairs
+    // ---- stage 6: cross-power (or filtered phase) spectrum over Hermitian
+    //      pairs; walked by storage position so a warp reads consecutive words
     for (int it = tid; it < WPC * N * N; it += NT) {
-      const int kp = it % N, kq = (it / N) % N, w = it / (N * N);
+      const int ap = it % N, aq = (it / N) % N, w = it / (N * N);
+      const int kp = ap / N2 + N1 * (ap % N2), kq = aq / N2 + N1 * (aq % N2);  // frequencies stored here
       const int mp = (N - kp) % N, mq = (N - kq) % N;
-      if (kp + kq * N > mp + mq * N) continue;
-      const int ap = N2 * (kp % N1) + kp / N1, aq = N2 * (kq % N1) + kq / N1;
       const int bp = N2 * (mp % N1) + mp / N1, bq = N2 * (mq % N1) + mq / N1;
+      if (ap + aq * N > bp + bq * N) continue;  // the partner position does this pair
       float2* P = planes + w * PS;
       const float2 X = P[aq * LD + ap];
       const float2 Zm = P[bq * LD + bp];
@@ -533,73 +575,88 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
     }
     __syncthreads();
     // ---- stage 7: inverse along q (every row p), back to natural order
-    {
-      if (N2 > 1) {
-        for (int it = tid; it < WPC * N * N1; it += NT) {
-          const int p = it % N, k1 = (it / N) % N1, w = it / (N * N1);
-          float2* L = planes + w * PS + p + (N2 * k1) * LD;
-          float2 x[N2];
+    if (N2 > 1) {
+      for (int it = tid; it < WPC * N * N1; it += NT) {
+        const int p = it % N, k1 = (it / N) % N1, w = it / (N * N1);
+        float2* L = planes + w * PS + p + (N2 * k1) * LD;
+        float2 x[N2];
 #pragma unroll
-          for (int k2 = 0; k2 < N2; ++k2) x[k2] = L[k2 * LD];
-          RDFT<N2, true>::run(x, N2);
+        for (int k2 = 0; k2 < N2; ++k2) x[k2] = L[k2 * LD];
+        RDFT<N2, true>::run(x, N2);
 #pragma unroll
-          for (int n2 = 1; n2 < N2; ++n2) {
-            const float2 t = tw[(n2 * k1) % N];
-            x[n2] = cmul(x[n2], make_float2(t.x, -t.y));
-          }
-#pragma unroll
-          for (int n2 = 0; n2 < N2; ++n2) L[n2 * LD] = x[n2];
+        for (int n2 = 1; n2 < N2; ++n2) {
+          const float2 t = tw[(n2 * k1) % N];
+          x[n2] = cmul(x[n2], make_float2(t.x, -t.y));
         }
-        __syncthreads();
-      }
-      for (int it = tid; it < WPC * N * N2; it += NT) {
-        const int p = it % N, n2 = (it / N) % N2, w = it / (N * N2);
-        float2* L = planes + w * PS + p;
-        float2 x[N1];
 #pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) x[k1] = L[(N2 * k1 + n2) * LD];
-        RDFT<N1, true>::run(x, N1);
-#pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1) L[(N2 * n1 + n2) * LD] = x[n1];
+        for (int n2 = 0; n2 < N2; ++n2) L[n2 * LD] = x[n2];
       }
+      __syncthreads();
+    }
+    for (int it = tid; it < WPC * N * N2; it += NT) {
+      const int p = it % N, n2 = (it / N) % N2, w = it / (N * N2);
+      float2* L = planes + w * PS + p;
+      float2 x[N1];
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) x[k1] = L[(N2 * k1 + n2) * LD];
+      RDFT<N1, true>::run(x, N1);
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) L[(N2 * n1 + n2) * LD] = x[n1];
     }
     __syncthreads();
-    // ---- stage 8: inverse along p (every column q); epilogue writes the
-    //      fftshifted, normalised, gain-weighted magnitude plane R
-    {
-      if (N2 > 1) {
-        for (int it = tid; it < WPC * N * N1; it += NT) {
-          const int q = it % N, k1 = (it / N) % N1, w = it / (N * N1);
-          float2* L = planes + w * PS + q * LD + N2 * k1;
-          float2 x[N2];
+    // ---- stage 8: inverse along p (every column q). The fftshifted,
+    //      normalised, gain-weighted magnitudes are held in registers across
+    //      a barrier, then written as the real plane R over the complex one.
+    if (N2 > 1) {
+      for (int it = tid; it < WPC * N * N1; it += NT) {
+        const int q = it % N, k1 = (it / N) % N1, w = it / (N * N1);
+        float2* L = planes + w * PS + q * LD + N2 * k1;
+        float2 x[N2];
 #pragma unroll
-          for (int k2 = 0; k2 < N2; ++k2) x[k2] = L[k2];
-          RDFT<N2, true>::run(x, N2);
+        for (int k2 = 0; k2 < N2; ++k2) x[k2] = L[k2];
+        RDFT<N2, true>::run(x, N2);
 #pragma unroll
-          for (int n2 = 1; n2 < N2; ++n2) {
-            const float2 t = tw[(n2 * k1) % N];
-            x[n2] = cmul(x[n2], make_float2(t.x, -t.y));
-          }
-#pragma unroll
-          for (int n2 = 0; n2 < N2; ++n2) L[n2] = x[n2];
+        for (int n2 = 1; n2 < N2; ++n2) {
+          const float2 t = tw[(n2 * k1) % N];
+          x[n2] = cmul(x[n2], make_float2(t.x, -t.y));
         }
-        __syncthreads();
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) L[n2] = x[n2];
       }
-      for (int it = tid; it < WPC * N * N2; it += NT) {
-        const int q = it % N, n2 = (it / N) % N2, w = it / (N * N2);
-        const float2* L = planes + w * PS + q * LD;
-        float2 x[N1];
+      __syncthreads();
+    }
+    {
+      float rv[IPT][N1];
 #pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) x[k1] = L[N2 * k1 + n2];
-        RDFT<N1, true>::run(x, N1);
-        const int qs = (q + N / 2) % N;
-        float* Rw = Rb + w * N * LDR;
+      for (int i = 0; i < IPT; ++i) {
+        const int it = tid + i * NT;
+        if (it < WPC * N * N2) {
+          const int q = it % N, n2 = (it / N) % N2, w = it / (N * N2);
+          const float2* L = planes + w * PS + q * LD;
+          float2 x[N1];
 #pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1) {
-          const int p = N2 * n1 + n2, ps = (p + N / 2) % N;
-          float r = fabsf(x[n1].x) * scale;
-          if (a.gain) r *= __ldg(a.gain + qs * N + ps);
-          Rw[qs * LDR + ps] = r;
+          for (int k1 = 0; k1 < N1; ++k1) x[k1] = L[N2 * k1 + n2];
+          RDFT<N1, true>::run(x, N1);
+          const int qs = (q + N / 2) % N;
+#pragma unroll
+          for (int n1 = 0; n1 < N1; ++n1) {
+            const int ps = (N2 * n1 + n2 + N / 2) % N;
+            float r = fabsf(x[n1].x) * scale;
+            if (a.gain) r *= __ldg(a.gain + qs * N + ps);
+            rv[i][n1] = r;
+          }
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < IPT; ++i) {
+        const int it = tid + i * NT;
+        if (it < WPC * N * N2) {
+          const int q = it % N, n2 = (it / N) % N2, w = it / (N * N2);
+          const int qs = (q + N / 2) % N;
+          float* Rw = reinterpret_cast<float*>(planes + w * PS);
+#pragma unroll
+          for (int n1 = 0; n1 < N1; ++n1) Rw[qs * LDR + (N2 * n1 + n2 + N / 2) % N] = rv[i][n1];
         }
       }
     }
@@ -608,7 +665,8 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
       for (int it = tid; it < WPC * N * N; it += NT) {
         const int p = it % N, q = (it / N) % N, w = it / (N * N);
         const int64_t job = base + w;
-        if (job < a.njobs) a.planes[job * (int64_t)(N * N) + q * N + p] = Rb[w * N * LDR + q * LDR + p];
+        if (job < a.njobs)
+          a.planes[job * (int64_t)(N * N) + q * N + p] = reinterpret_cast<const float*>(planes + w * PS)[q * LDR + p];
       }
     }
     // ---- stage 9: peak analysis, one thread group per window
@@ -618,8 +676,9 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
       const bool active = job < a.njobs;
       int64_t gid = -1;
       if (active) gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
-      analyze_group(Rb + w * N * LDR, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, C::G,
-                    red + w * (C::G / 32) * 2, active, s_vals + w * KMAX, s_locs + w * 2 * KMAX, gid, job, po);
+      analyze_group(reinterpret_cast<const float*>(planes + w * PS), N, N, LDR, K, a.npeaks, a.finder, a.subpixel,
+                    gt, C::G, red + w * (C::G / 32) * 2, active, s_vals + w * KMAX, s_locs + w * 2 * KMAX, gid, job,
+                    po);
     }
     __syncthreads();
   }

@@ -72,7 +72,10 @@ def test_analyze_random_planes(ws, orc, hooks, finder, subpixel, npeaks):
         np.testing.assert_allclose(out[k, :2], ref[:2], atol=1e-5)
         assert out[k, 2] == ref[2] or (math.isnan(out[k, 2]) and math.isnan(ref[2]))
         np.testing.assert_allclose(out[k, 3], ref[3], rtol=1e-5, equal_nan=True)
-        np.testing.assert_allclose(out[k, 5:5 + 2 * (K - 1)], ref[5:5 + 2 * (K - 1)], atol=1e-5, equal_nan=True)
+        # alternative peaks on noise can be ill-conditioned fits (offsets of
+        # hundreds of px); FP64 vs Float32 logarithms then differ relatively
+        np.testing.assert_allclose(out[k, 5:5 + 2 * (K - 1)], ref[5:5 + 2 * (K - 1)], rtol=2e-4, atol=1e-5,
+                                   equal_nan=True)
 
 
 # --- correlation planes and per-window outputs ------------------------------------
