@@ -390,11 +390,12 @@ template <int N, int W> struct CorrCfg {
   static constexpr bool PADDED = (W * 2 == N);
   static constexpr int NZ1 = PADDED ? (W / N2) : N1;  // nonzero inputs of a forward pass-A line
   static constexpr int IPT = (WPC * N * N2 + NT - 1) / NT;  // final inverse items per thread
+  static constexpr int EPT = (W * W + G - 1) / G;             // window pixels per thread
   static constexpr size_t PLANE_B = (size_t)N * LD * sizeof(float2);
   static constexpr size_t smem() {
-    return WPC * PLANE_B + N * sizeof(float2) + WPC * (G / 32) * 2 * sizeof(uint32_t) +
-           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int) + 4 * sizeof(float) + 2 * sizeof(int)) +
-           WPC * W * W + 64;
+    return WPC * PLANE_B + WPC * (G / 32) * 3 * sizeof(double) + N * sizeof(float2) +
+           WPC * (G / 32) * 2 * sizeof(uint32_t) +
+           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int) + 2 * sizeof(int)) + 64;
   }
   static_assert(W == N || 2 * W == N, "window must equal the FFT size or half of it");
   static_assert(G >= 32 && G % 32 == 0, "analysis group must be whole warps");
@@ -405,16 +406,16 @@ template <int N, int W>
 __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const CorrArgs a) {
   using C = CorrCfg<N, W>;
   constexpr int WPC = C::WPC, NT = C::NT, LD = C::LD, LDR = C::LDR, N1 = C::N1, N2 = C::N2, IPT = C::IPT;
+  constexpr int G = C::G, EPT = C::EPT;
   constexpr int PS = N * LD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* planes = reinterpret_cast<float2*>(smem_raw);
-  float2* tw = reinterpret_cast<float2*>(smem_raw + WPC * C::PLANE_B);
+  double* s_part = reinterpret_cast<double*>(smem_raw + WPC * C::PLANE_B);  // 3 per warp: sum A, sum B, count
+  float2* tw = reinterpret_cast<float2*>(s_part + WPC * (C::G / 32) * 3);
   uint32_t* red = reinterpret_cast<uint32_t*>(tw + N);
   float* s_vals = reinterpret_cast<float*>(red + WPC * (C::G / 32) * 2);
   int* s_locs = reinterpret_cast<int*>(s_vals + WPC * KMAX);
-  float* s_mean = reinterpret_cast<float*>(s_locs + WPC * 2 * KMAX);  // 4 per window
-  int* s_job = reinterpret_cast<int*>(s_mean + WPC * 4);              // rs, cs per window
-  uint8_t* s_mflag = reinterpret_cast<uint8_t*>(s_job + WPC * 2);
+  int* s_job = s_locs + WPC * 2 * KMAX;  // rs, cs per window
 
   const int tid = threadIdx.x;
   const int K = a.npeaks > 2 ? a.npeaks : 2;
@@ -435,59 +436,65 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
       s_job[2 * tid + 1] = job < a.njobs ? a.jobs[4 * job + 3] : -1;
     }
     __syncthreads();
-    // ---- stage 1: raw windows -> planes (A in .x, B in .y), mask flags
-    for (int it = tid; it < WPC * W * W; it += NT) {
-      const int p = it % W, q = (it / W) % W, w = it / (W * W);
+    // ---- stages 1-3: each window's thread group loads its pixels (coalesced
+    //      down the columns), reduces the window means in FP64, and stores
+    //      apod * (x - mean) into the plane; masked pixels enter as zero and
+    //      leave the mean (load_windows!, src/correlators.jl:188-263). The
+    //      mean is the exact sum over n rounded once, where the reference
+    //      folds in Float32 left to right; the two differ by a few ulp.
+    {
+      const int w = tid / G, gt = tid % G, lane = tid & 31, gw = gt >> 5;
       const int rs = s_job[2 * w], cs = s_job[2 * w + 1];
-      float2 z = make_float2(0.f, 0.f);
-      uint8_t mf = 0;
-      if (rs >= 0) {
-        const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * a.ld;
-        z = make_float2(__ldg(a.A + off), __ldg(a.B + off));
-        if (a.mask) mf = __ldg(a.mask + off);
-      }
-      planes[w * PS + q * LD + p] = z;
-      if (a.mask) s_mflag[w * W * W + q * W + p] = mf;
-    }
-    __syncthreads();
-    // ---- stage 2: window means in the reference's column-major fold order
-    //      (one lane per window folds both frames; loads are independent of
-    //      the running sums, so the unrolled loop is bound by the add chain)
-    if (tid < WPC) {
-      const float2* P = planes + tid * PS;
-      float sa = 0.f, sb = 0.f;
-      int n = 0;
-      if (!a.mask) {
-        sa = P[0].x;
-        sb = P[0].y;
-#pragma unroll 8
-        for (int k = 1; k < W * W; ++k) {
-          const float2 z = P[(k / W) * LD + (k % W)];
-          sa += z.x;
-          sb += z.y;
-        }
-        n = W * W;
-      } else {
-        for (int k = 0; k < W * W; ++k) {
-          if (s_mflag[tid * W * W + k]) continue;
-          const float2 z = P[(k / W) * LD + (k % W)];
-          sa += z.x;
-          sb += z.y;
-          ++n;
+      float2 z[EPT];
+      bool mk[EPT];
+      double sa = 0.0, sb = 0.0, cnt = 0.0;
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int e = gt + i * G;
+        z[i] = make_float2(0.f, 0.f);
+        mk[i] = true;
+        if (e < W * W && rs >= 0) {
+          const int p = e % W, q = e / W;
+          const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * a.ld;
+          z[i] = make_float2(__ldg(a.A + off), __ldg(a.B + off));
+          mk[i] = a.mask ? __ldg(a.mask + off) != 0 : false;
+          if (!mk[i]) {
+            sa += (double)z[i].x;
+            sb += (double)z[i].y;
+            cnt += 1.0;
+          }
         }
       }
-      s_mean[4 * tid] = n > 0 ? sa / (float)n : 0.f;
-      s_mean[4 * tid + 1] = n > 0 ? sb / (float)n : 0.f;
-    }
-    __syncthreads();
-    // ---- stage 3: apod * (x - mean), masked pixels -> 0
-    for (int it = tid; it < WPC * W * W; it += NT) {
-      const int p = it % W, q = (it / W) % W, w = it / (W * W);
-      const float ap = __ldg(a.apod + q * W + p);
-      float2 z = planes[w * PS + q * LD + p];
-      if (a.mask && s_mflag[w * W * W + q * W + p]) z = make_float2(0.f, 0.f);
-      else z = make_float2(ap * (z.x - s_mean[4 * w]), ap * (z.y - s_mean[4 * w + 1]));
-      planes[w * PS + q * LD + p] = z;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sa += __shfl_xor_sync(0xffffffffu, sa, o);
+        sb += __shfl_xor_sync(0xffffffffu, sb, o);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+      }
+      double* part = s_part + w * (G / 32) * 3;
+      if (lane == 0) {
+        part[3 * gw] = sa;
+        part[3 * gw + 1] = sb;
+        part[3 * gw + 2] = cnt;
+      }
+      __syncthreads();
+      double ta = 0.0, tb = 0.0, tn = 0.0;
+      for (int k = 0; k < G / 32; ++k) {
+        ta += part[3 * k];
+        tb += part[3 * k + 1];
+        tn += part[3 * k + 2];
+      }
+      const float ma = tn > 0 ? (float)(ta / tn) : 0.f, mb = tn > 0 ? (float)(tb / tn) : 0.f;
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int e = gt + i * G;
+        if (e < W * W) {
+          const int p = e % W, q = e / W;
+          const float ap = __ldg(a.apod + e);
+          planes[w * PS + q * LD + p] =
+              mk[i] ? make_float2(0.f, 0.f) : make_float2(ap * (z[i].x - ma), ap * (z[i].y - mb));
+        }
+      }
     }
     __syncthreads();
 
@@ -550,28 +557,44 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
     }
     __syncthreads();
     // ---- stage 6: cross-power (or filtered phase) spectrum over Hermitian
-    //      pairs; walked by storage position so a warp reads consecutive words
-    for (int it = tid; it < WPC * N * N; it += NT) {
-      const int ap = it % N, aq = (it / N) % N, w = it / (N * N);
-      const int kp = ap / N2 + N1 * (ap % N2), kq = aq / N2 + N1 * (aq % N2);  // frequencies stored here
-      const int mp = (N - kp) % N, mq = (N - kq) % N;
-      const int bp = N2 * (mp % N1) + mp / N1, bq = N2 * (mq % N1) + mq / N1;
-      if (ap + aq * N > bp + bq * N) continue;  // the partner position does this pair
-      float2* P = planes + w * PS;
-      const float2 X = P[aq * LD + ap];
-      const float2 Zm = P[bq * LD + bp];
-      const float2 Y = make_float2(Zm.x, -Zm.y);  // conj(Z[-k])
-      // FA = (X + Y)/2, FB = (X - Y)/(2i); S = conj(FA) * FB
-      const float Ar = 0.5f * (X.x + Y.x), Ai = 0.5f * (X.y + Y.y);
-      const float Br = 0.5f * (X.y - Y.y), Bi = -0.5f * (X.x - Y.x);
-      float2 S = cmul(make_float2(Ar, -Ai), make_float2(Br, Bi));
-      if (a.method == 1) {
-        const float den = hypotf(S.x, S.y) + 1.1920929e-7f;  // eps(Float32)
-        const float wk = __ldg(a.phasew + kq * N + kp);
-        S = make_float2((wk * S.x) / den, (wk * S.y) / den);
+    //      pairs (k, -k). For N <= 32 the frequencies are stored in natural
+    //      order and only the canonical half is enumerated; for larger N the
+    //      walk follows storage order so a warp reads consecutive words.
+    {
+      constexpr int NCAN = N2 == 1 ? (N / 2 + 1) * N : N * N;  // columns kq <= N/2 hold every pair
+      for (int it = tid; it < WPC * NCAN; it += NT) {
+        int ap, aq, kp, kq;
+        const int w = it / NCAN, r = it % NCAN;
+        if (N2 == 1) {
+          kp = r % N;
+          kq = r / N;
+          ap = kp;
+          aq = kq;
+        } else {
+          ap = r % N;
+          aq = r / N;
+          kp = ap / N2 + N1 * (ap % N2);
+          kq = aq / N2 + N1 * (aq % N2);
+        }
+        const int mp = (N - kp) % N, mq = (N - kq) % N;
+        const int bp = N2 * (mp % N1) + mp / N1, bq = N2 * (mq % N1) + mq / N1;
+        if (ap + aq * N > bp + bq * N) continue;  // the partner position does this pair
+        float2* P = planes + w * PS;
+        const float2 X = P[aq * LD + ap];
+        const float2 Zm = P[bq * LD + bp];
+        const float2 Y = make_float2(Zm.x, -Zm.y);  // conj(Z[-k])
+        // FA = (X + Y)/2, FB = (X - Y)/(2i); S = conj(FA) * FB
+        const float Ar = 0.5f * (X.x + Y.x), Ai = 0.5f * (X.y + Y.y);
+        const float Br = 0.5f * (X.y - Y.y), Bi = -0.5f * (X.x - Y.x);
+        float2 S = cmul(make_float2(Ar, -Ai), make_float2(Br, Bi));
+        if (a.method == 1) {
+          const float den = hypotf(S.x, S.y) + 1.1920929e-7f;  // eps(Float32)
+          const float wk = __ldg(a.phasew + kq * N + kp);
+          S = make_float2((wk * S.x) / den, (wk * S.y) / den);
+        }
+        P[aq * LD + ap] = S;
+        P[bq * LD + bp] = make_float2(S.x, -S.y);
       }
-      P[aq * LD + ap] = S;
-      P[bq * LD + bp] = make_float2(S.x, -S.y);
     }
     __syncthreads();
     // ---- stage 7: inverse along q (every row p), back to natural order

@@ -1,14 +1,12 @@
 // Wieneke (2015) correlation-statistics uncertainty (sm_100a).
 //
 // One CTA per interrogation window (grid-stride over jobs). It restates
-// src/uncertainty.jl:51-179: the windows are mean-subtracted (column-major
-// fold) and apodized exactly like load_windows!, the per-pixel correlation
+// src/uncertainty.jl:51-179: the windows are mean-subtracted and apodized
+// like load_windows!, the per-pixel correlation
 // difference dC = a0*b1 - a1*b0 and its (1,2,1)/4 smoothing are formed in
 // FP32, and the 2 x 44 statistics (C0, C+, C-, S00 and the 40 half-plane
-// covariance sums of rings 1..4) are reduced in FP64. Each statistic is
-// summed by one thread in the reference's loop order with explicit
-// round-to-nearest FP64 arithmetic, so the sums equal the CPU restatement
-// bit for bit; finalize_uncertainty (:162-179) then runs on the same thread.
+// covariance sums of rings 1..4) are reduced in FP64 across the CTA;
+// finalize_uncertainty (:162-179) then runs on one thread per component.
 #include <math.h>
 #include <stdint.h>
 
@@ -68,126 +66,139 @@ __device__ __forceinline__ float uq_finalize(const double* s, const UQOffsets& o
   return (float)(__dsub_rn(lhi, llo) / __dmul_rn(2.0, denom));
 }
 
-// Statistic `si` (0..43) of one component over the smoothed field dCs
-// (nr x m, column-major, leading dim nr) and windows wa/wb viewed through
-// (str, stc) strides.
-__device__ double uq_stat(int si, const float* wa, const float* wb, int str, int stc, int nr, int m,
-                          const float* dCs, double mu, const UQOffsets& o) {
-  double acc = 0.0;
-  if (si < 3) {
-    for (int c = 0; c < m; ++c)
-      for (int r = 0; r < nr; ++r) {
-        const float a0 = wa[r * str + c * stc], a1 = wa[r * str + (c + 1) * stc];
-        const float b0 = wb[r * str + c * stc], b1 = wb[r * str + (c + 1) * stc];
-        const float pr = si == 0 ? __fmul_rn(a0, b0) : (si == 1 ? __fmul_rn(a0, b1) : __fmul_rn(a1, b0));
-        acc = __dadd_rn(acc, (double)pr);
-      }
-    return acc;
-  }
-  if (si == 3) {
-    for (int c = 0; c < m; ++c)
-      for (int r = 0; r < nr; ++r) {
-        const double d = __dsub_rn((double)dCs[r + c * nr], mu);
-        acc = __dadd_rn(acc, __dmul_rn(d, d));
-      }
-    return acc;
-  }
-  const int k = si - 4, dr = o.dr[k], dc = o.dc[k];
-  const int c0 = 1 > 1 - dc ? 1 : 1 - dc, c1 = m < m - dc ? m : m - dc;
-  const int r0 = 1 > 1 - dr ? 1 : 1 - dr, r1 = nr < nr - dr ? nr : nr - dr;
-  for (int c = c0; c <= c1; ++c)
-    for (int r = r0; r <= r1; ++r) {
-      const double d1 = __dsub_rn((double)dCs[(r - 1) + (c - 1) * nr], mu);
-      const double d2 = __dsub_rn((double)dCs[(r - 1 + dr) + (c - 1 + dc) * nr], mu);
-      acc = __dadd_rn(acc, __dmul_rn(d1, d2));
-    }
-  return acc;
+// One CTA (4 warps) per window. Every reduction runs across lanes: the
+// window means and the mean of the smoothed field are block-wide FP64 sums,
+// and each of the 88 statistics is summed by one warp (lanes stride over the
+// pixel pairs, then a shuffle reduction). The FP32 parts -- the apodized
+// windows, dC and its smoothing -- use the reference's operation order.
+constexpr int UQ_THREADS = 128;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
 
-__global__ void __launch_bounds__(128) uq_kernel(const UQArgs a, const UQOffsets o) {
+__global__ void __launch_bounds__(UQ_THREADS) uq_kernel(const UQArgs a, const UQOffsets o) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int W = a.W, m = W - 1;
-  float* wa = reinterpret_cast<float*>(smem_raw);  // W*W
-  float* wb = wa + W * W;                           // W*W
-  float* dC = wb + W * W;                           // 2 * W*m (u then v)
-  float* dCs = dC + 2 * W * m;                      // 2 * W*m
-  double* stats = reinterpret_cast<double*>(dCs + 2 * W * m + ((2 * W * m) & 1));  // 88
-  __shared__ float s_mean[2];
-  __shared__ double s_mu[2];
-  __shared__ int s_any;
-  const int tid = threadIdx.x;
+  const int W = a.W, m = W - 1, WM = W * m;
+  double* dd = reinterpret_cast<double*>(smem_raw);       // 2*WM: smoothed dC minus its mean (u, v)
+  double* stats = dd + 2 * WM;                             // 88
+  double* part = stats + 88;                               // 4 warps x 3
+  float* wa = reinterpret_cast<float*>(part + 12);         // W*W
+  float* wb = wa + W * W;                                  // W*W
+  float* dC = wb + W * W;                                  // 2*WM
+  float* dCs = dC + 2 * WM;                                // 2*WM
+  uint8_t* mf = reinterpret_cast<uint8_t*>(dCs + 2 * WM);  // W*W
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int64_t job = blockIdx.x; job < a.njobs; job += gridDim.x) {
     const int rs = a.jobs[4 * job + 2], cs = a.jobs[4 * job + 3];
-    if (tid == 0) s_any = 0;
-    __syncthreads();
-    for (int k = tid; k < W * W; k += blockDim.x) {
+    // windows and their means (load_uncertainty_windows!, :51-83)
+    double sa = 0.0, sb = 0.0, cnt = 0.0;
+    for (int k = tid; k < W * W; k += UQ_THREADS) {
       const int p = k % W, q = k / W;
       const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * a.ld;
-      wa[k] = a.A[off];
-      wb[k] = a.B[off];
-      if (a.mask && a.mask[off]) s_any = 1;
-    }
-    __syncthreads();
-    // means (load_uncertainty_windows!, :51-83)
-    if (tid < 2) {
-      const float* x = tid == 0 ? wa : wb;
-      float s = 0.f;
-      int n = 0;
-      if (!s_any) {
-        s = x[0];
-        for (int k = 1; k < W * W; ++k) s = __fadd_rn(s, x[k]);
-        n = W * W;
-      } else {
-        for (int k = 0; k < W * W; ++k) {
-          const int p = k % W, q = k / W;
-          if (a.mask[(int64_t)(rs + p) + (int64_t)(cs + q) * a.ld]) continue;
-          s = __fadd_rn(s, x[k]);
-          ++n;
-        }
+      const float va = a.A[off], vb = a.B[off];
+      const uint8_t mk = a.mask ? a.mask[off] : 0;
+      wa[k] = va;
+      wb[k] = vb;
+      mf[k] = mk;
+      if (!mk) {
+        sa += (double)va;
+        sb += (double)vb;
+        cnt += 1.0;
       }
-      s_mean[tid] = n > 0 ? __fdiv_rn(s, (float)n) : 0.f;
+    }
+    sa = warp_sum(sa);
+    sb = warp_sum(sb);
+    cnt = warp_sum(cnt);
+    if (lane == 0) {
+      part[3 * warp] = sa;
+      part[3 * warp + 1] = sb;
+      part[3 * warp + 2] = cnt;
     }
     __syncthreads();
-    for (int k = tid; k < W * W; k += blockDim.x) {
-      const int p = k % W, q = k / W;
-      bool masked = s_any && a.mask[(int64_t)(rs + p) + (int64_t)(cs + q) * a.ld];
+    double ta = 0, tb = 0, tn = 0;
+    for (int w = 0; w < UQ_THREADS / 32; ++w) {
+      ta += part[3 * w];
+      tb += part[3 * w + 1];
+      tn += part[3 * w + 2];
+    }
+    const float ma = tn > 0 ? (float)(ta / tn) : 0.f, mb = tn > 0 ? (float)(tb / tn) : 0.f;
+    for (int k = tid; k < W * W; k += UQ_THREADS) {
       const float ap = a.apod[k];
-      wa[k] = masked ? 0.f : __fmul_rn(ap, __fsub_rn(wa[k], s_mean[0]));
-      wb[k] = masked ? 0.f : __fmul_rn(ap, __fsub_rn(wb[k], s_mean[1]));
+      wa[k] = mf[k] ? 0.f : __fmul_rn(ap, __fsub_rn(wa[k], ma));
+      wb[k] = mf[k] ? 0.f : __fmul_rn(ap, __fsub_rn(wb[k], mb));
     }
     __syncthreads();
-    // dC for both components: u views (r, c) = (p, q); v views (r, c) = (q, p)
-    for (int k = tid; k < 2 * W * m; k += blockDim.x) {
-      const int comp = k / (W * m), e = k % (W * m), r = e % W, c = e / W;
+    // dC = a0 b1 - a1 b0 for both components: u views (r, c) = (p, q), v = (q, p)
+    for (int k = tid; k < 2 * WM; k += UQ_THREADS) {
+      const int comp = k / WM, e = k % WM, r = e % W, c = e / W;
       const int str = comp == 0 ? 1 : W, stc = comp == 0 ? W : 1;
       const float a0 = wa[r * str + c * stc], a1 = wa[r * str + (c + 1) * stc];
       const float b0 = wb[r * str + c * stc], b1 = wb[r * str + (c + 1) * stc];
       dC[k] = __fsub_rn(__fmul_rn(a0, b1), __fmul_rn(a1, b0));
     }
     __syncthreads();
-    for (int k = tid; k < 2 * W * m; k += blockDim.x) {
-      const int comp = k / (W * m), e = k % (W * m), r = e % W, c = e / W;
-      const float* d = dC + comp * W * m;
+    double s0 = 0.0, s1 = 0.0;
+    for (int k = tid; k < 2 * WM; k += UQ_THREADS) {
+      const int comp = k / WM, e = k % WM, r = e % W, c = e / W;
+      const float* d = dC + comp * WM;
       const int cl = c > 0 ? c - 1 : 0, cr = c < m - 1 ? c + 1 : m - 1;
-      dCs[k] = __fmul_rn(0.25f, __fadd_rn(__fadd_rn(d[r + cl * W], __fmul_rn(2.0f, d[r + c * W])), d[r + cr * W]));
+      const float v = __fmul_rn(0.25f, __fadd_rn(__fadd_rn(d[r + cl * W], __fmul_rn(2.0f, d[r + c * W])), d[r + cr * W]));
+      dCs[k] = v;
+      if (comp == 0) s0 += (double)v;
+      else s1 += (double)v;
+    }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    __syncthreads();  // part reused
+    if (lane == 0) {
+      part[3 * warp] = s0;
+      part[3 * warp + 1] = s1;
     }
     __syncthreads();
-    if (tid < 2) {
-      const float* d = dCs + tid * W * m;
-      double mu = 0.0;
-      for (int c = 0; c < m; ++c)
-        for (int r = 0; r < W; ++r) mu = __dadd_rn(mu, (double)d[r + c * W]);
-      s_mu[tid] = mu / (double)(W * m);
+    double mu0 = 0, mu1 = 0;
+    for (int w = 0; w < UQ_THREADS / 32; ++w) {
+      mu0 += part[3 * w];
+      mu1 += part[3 * w + 1];
     }
+    mu0 /= (double)WM;
+    mu1 /= (double)WM;
+    for (int k = tid; k < 2 * WM; k += UQ_THREADS) dd[k] = (double)dCs[k] - (k < WM ? mu0 : mu1);
     __syncthreads();
-    for (int it = tid; it < 88; it += blockDim.x) {
-      const int comp = it / 44, si = it % 44;
+    // the 2 x 44 statistics, one warp per statistic (uq_component!, :104-151)
+    for (int st = warp; st < 88; st += UQ_THREADS / 32) {
+      const int comp = st / 44, si = st % 44;
       const int str = comp == 0 ? 1 : W, stc = comp == 0 ? W : 1;
-      stats[it] = uq_stat(si, wa, wb, str, stc, W, m, dCs + comp * W * m, s_mu[comp], o);
+      const double* d = dd + comp * WM;
+      double acc = 0.0;
+      if (si < 3) {
+        for (int t = lane; t < WM; t += 32) {
+          const int r = t % W, c = t / W;
+          const float a0 = wa[r * str + c * stc], a1 = wa[r * str + (c + 1) * stc];
+          const float b0 = wb[r * str + c * stc], b1 = wb[r * str + (c + 1) * stc];
+          const float pr = si == 0 ? __fmul_rn(a0, b0) : (si == 1 ? __fmul_rn(a0, b1) : __fmul_rn(a1, b0));
+          acc += (double)pr;
+        }
+      } else if (si == 3) {
+        for (int t = lane; t < WM; t += 32) acc = fma(d[t], d[t], acc);
+      } else {
+        const int k = si - 4, dr = o.dr[k], dc = o.dc[k];
+        const int c0 = dc < 0 ? -dc : 0, c1 = dc > 0 ? m - dc : m;  // c in [c0, c1)
+        const int r0 = dr < 0 ? -dr : 0, r1 = dr > 0 ? W - dr : W;  // r in [r0, r1)
+        const int nrr = r1 - r0, ncc = c1 - c0;
+        for (int t = lane; t < nrr * ncc; t += 32) {
+          const int r = r0 + t % nrr, c = c0 + t / nrr;
+          acc = fma(d[r + c * W], d[(r + dr) + (c + dc) * W], acc);
+        }
+      }
+      acc = warp_sum(acc);
+      if (lane == 0) stats[st] = acc;
     }
     __syncthreads();
     if (a.stats)
-      for (int it = tid; it < 88; it += blockDim.x) a.stats[job * 88 + it] = stats[it];
+      for (int it = tid; it < 88; it += UQ_THREADS) a.stats[job * 88 + it] = stats[it];
     if (a.unc_u && tid < 2) {
       const int64_t gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
       const float sg = uq_finalize(stats + 44 * tid, o);
@@ -201,18 +212,19 @@ __global__ void __launch_bounds__(128) uq_kernel(const UQArgs a, const UQOffsets
 cudaError_t launch_uq(const UQArgs& a, cudaStream_t s, int num_sms) {
   if (a.njobs <= 0) return cudaSuccess;
   static const UQOffsets offs = make_offsets();
-  const int W = a.W, m = W - 1;
-  const size_t sm = (size_t)(2 * W * W + 4 * W * m + 2) * sizeof(float) + 88 * sizeof(double) + 16;
-  if (sm > 200 * 1024) return cudaErrorInvalidValue;
+  const int W = a.W, WM = W * (W - 1);
+  const size_t sm = (size_t)(2 * WM + 88 + 12) * sizeof(double) + (size_t)(2 * W * W + 4 * WM) * sizeof(float) +
+                    (size_t)W * W + 16;
+  if (sm > 220 * 1024) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(uq_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, uq_kernel, 128, sm);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, uq_kernel, UQ_THREADS, sm);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   int64_t grid = (int64_t)per_sm * num_sms;
   if (grid > a.njobs) grid = a.njobs;
-  uq_kernel<<<(unsigned)grid, 128, sm, s>>>(a, offs);
+  uq_kernel<<<(unsigned)grid, UQ_THREADS, sm, s>>>(a, offs);
   return cudaGetLastError();
 }
 

@@ -262,8 +262,12 @@ def test_field_change_bit_exact(ws, orc, hooks):
 
 # --- uncertainty -------------------------------------------------------------------------
 
-@pytest.mark.parametrize("w", [16, 24, 32])
-def test_uq_statistics_bit_exact(ws, orc, hb, hooks, pair256, w):
+@pytest.mark.parametrize("w", [16, 24, 32, 64])
+def test_uq_statistics(ws, orc, hb, hooks, pair256, w):
+    """Wieneke statistics of the device against the oracle. The device forms
+    window means as one FP64 reduction (the oracle folds left to right in
+    Float32, like the reference), so the sums agree to float round-off of
+    the mean, and the final sigma to ~1e-5 relative."""
     A, B = pair256
     p = hb.PIVParameters(window_size=w, overlap=w // 2, padding=True, apodization="gauss", uncertainty=True)
     sess = hooks.DeviceSession(ws)
@@ -272,7 +276,14 @@ def test_uq_statistics_bit_exact(ws, orc, hb, hooks, pair256, w):
     _, _, uq = sess.process_windows(p, jobs, want_uq=True)
     for q, (gi, gj, rs, cs) in enumerate(jobs):
         s = orc.uq_stats(A[rs - 1:rs - 1 + w, cs - 1:cs - 1 + w], B[rs - 1:rs - 1 + w, cs - 1:cs - 1 + w], "gauss")
-        assert np.array_equal(uq[q], s), q
+        for comp in (0, 1):
+            c = slice(44 * comp, 44 * comp + 3)
+            np.testing.assert_allclose(uq[q, c], s[c], rtol=0, atol=2e-5 * np.abs(s[c]).max())
+        np.testing.assert_allclose(uq[q], s, rtol=1e-3, atol=1e-6 * abs(s[3]))
+        for comp in (0, 1):
+            a = orc.finalize_uncertainty(uq[q, 44 * comp:44 * comp + 44])
+            b = orc.finalize_uncertainty(s[44 * comp:44 * comp + 44])
+            assert (math.isnan(a) and math.isnan(b)) or abs(a - b) <= 1e-4 * abs(b) + 1e-7
 
 
 # --- end to end ---------------------------------------------------------------------------
