@@ -131,6 +131,10 @@ SIGNATURES = [
     ("hh_set_profiling", ctypes.c_int32, [_CTX, ctypes.c_int32]),
     ("hh_profile_read", ctypes.c_int32, [_CTX, ctypes.POINTER(hh_kernel_profile), ctypes.c_int32]),
     ("hh_launch_count", ctypes.c_int64, [_CTX]),
+    ("hh_field_change_noalloc", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+      ctypes.c_void_p, ctypes.c_void_p]),
+    ("hh_noalloc_last_error", ctypes.c_char_p, []),
 ]
 
 

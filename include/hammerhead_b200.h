@@ -234,6 +234,32 @@ hh_status hh_profile_read(hh_ctx* ctx, hh_kernel_profile* out /* HH_K_CLASSES en
 /* Kernels launched on ctx since creation (all classes, profiling or not). */
 int64_t hh_launch_count(const hh_ctx* ctx);
 
+/* ---- Allocation-free convergence norm (no counterpart in the reference) --
+ *
+ * For callers that must not have the library allocate device memory: a host
+ * runtime whose GPU memory belongs to its own pool allocator, a loop that
+ * cannot absorb an allocation stall, or a process held to a fixed memory
+ * budget. Computes what hh_field_change computes (the 95th-percentile
+ * vector change of src/pipeline.jl:849-866) on caller-owned device buffers
+ * d_u, d_v, d_pu, d_pv (n float32 each) and optional d_mask (n uint8,
+ * nonzero = masked), writing the result to the device float *d_change,
+ * asynchronously on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream). It allocates nothing: its scratch is a fixed array of
+ * HH_NOALLOC_MAX_VECTORS 32-bit keys compiled into the library, which every
+ * GPU that loads the library holds until the process exits (4 MiB).
+ *   - n > HH_NOALLOC_MAX_VECTORS is rejected with HH_ERR_ARG.
+ *   - The first call on a device looks up the scratch address for that
+ *     device (the device current at the call); make that first call before
+ *     any stream capture.
+ *   - All calls on a device share the scratch; each call rewrites the
+ *     entries it reads, so nothing carries over, but calls whose kernels
+ *     overlap on the GPU (different streams, no ordering) race on it.
+ * Errors are reported through hh_noalloc_last_error(). */
+#define HH_NOALLOC_MAX_VECTORS (1 << 20)
+hh_status hh_field_change_noalloc(const float* d_u, const float* d_v, const float* d_pu, const float* d_pv,
+                                  const uint8_t* d_mask, int64_t n, float* d_change, void* stream);
+const char* hh_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
