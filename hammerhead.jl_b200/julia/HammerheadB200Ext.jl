@@ -1,0 +1,156 @@
+# Package extension that registers `backend = :b200` in Hammerhead.jl and
+# forwards the planar WIDIM path to libhammerhead_b200.so through ccall.
+#
+# Not runnable in this repository's environment (no Julia toolchain); it is
+# written against the backend-hook contract of docs/src/reference/backends.md
+# and src/types.jl:61-111 of the reference, and mirrors what the Python host
+# layer (hammerhead.jl_b200/hammerhead_b200) does with the same C ABI.
+module HammerheadB200Ext
+
+using Hammerhead
+import Hammerhead: _AbstractHammerheadBackend, _resolve_backend, _check_backend_params, _engine_nchunks,
+    _supports_fft, _supports_batched_fft, _supports_fp64, PIVParameters, PIVResult, run_piv
+
+const LIB = get(ENV, "HAMMERHEAD_B200_LIB", "libhammerhead_b200.so")
+
+struct _B200Backend <: _AbstractHammerheadBackend end
+_resolve_backend(::Val{:b200}) = _B200Backend()
+_engine_nchunks(::_B200Backend, ::Int) = 1
+_supports_fft(::_B200Backend) = true
+_supports_batched_fft(::_B200Backend) = true
+_supports_fp64(::_B200Backend) = true   # FP64 uncertainty reductions on the device
+
+# hh_validator / hh_pass_desc (include/hammerhead_b200.h), field for field.
+struct Validator
+    kind::Int32
+    neighborhood::Int32
+    threshold::Float64
+    vmin::Float64
+    vmax::Float64
+    epsilon::Float64
+end
+const NOVAL = Validator(0, 0, 0.0, 0.0, 0.0, 0.0)
+
+struct PassDesc
+    window::NTuple{2,Int32}
+    search::NTuple{2,Int32}
+    overlap::NTuple{2,Int32}
+    method::Int32
+    padding::Int32
+    apodization::Int32
+    subpixel::Int32
+    n_peaks::Int32
+    peak_finder::Int32
+    uncertainty::Int32
+    uod_enable::Int32
+    uod_threshold::Float64
+    uod_neighborhood::Int32
+    replace_outliers::Int32
+    min_peak_ratio::Float64
+    max_iterations::Int32
+    keep_correlation_planes::Int32
+    convergence_tol::Float64
+    n_validators::Int32
+    reserved0::Int32
+    validators::NTuple{8,Validator}
+end
+
+const SUBPIXEL = Dict(:gauss3 => 0, :gauss9 => 1, :gauss2d => 2, :none => 3)
+
+validator(v::Hammerhead.PeakRatioValidator) = Validator(0, 0, v.threshold, 0.0, 0.0, 0.0)
+validator(v::Hammerhead.CorrelationMomentValidator) = Validator(1, 0, v.threshold, 0.0, 0.0, 0.0)
+validator(v::Hammerhead.VelocityMagnitudeValidator) = Validator(2, 0, 0.0, v.min, v.max, 0.0)
+validator(v::Hammerhead.UniversalOutlierValidator) =
+    Validator(3, v.neighborhood_size, v.threshold, 0.0, 0.0, v.epsilon)
+
+function pass_desc(p::PIVParameters)
+    vals = map(validator, p.validation)
+    length(vals) <= 8 || throw(ArgumentError("backend :b200 supports at most 8 extra validators"))
+    vt = ntuple(i -> i <= length(vals) ? vals[i] : NOVAL, 8)
+    PassDesc(Int32.(p.window_size), Int32.(p.search_area_size), Int32.(p.overlap),
+             p.correlation_method === :phase ? 1 : 0, p.padding, p.apodization === :gauss ? 1 : 0,
+             SUBPIXEL[p.subpixel_method], p.n_peaks, p.peak_finder === :exclusion ? 1 : 0,
+             p.uncertainty, p.uod_enable, p.uod_threshold, p.uod_neighborhood, p.replace_outliers,
+             p.min_peak_ratio, p.max_iterations, p.keep_correlation_planes, p.convergence_tol,
+             length(vals), 0, vt)
+end
+
+struct Result
+    ny::Int32
+    nx::Int32
+    x::Ptr{Float32}
+    y::Ptr{Float32}
+    u::Ptr{Float32}
+    v::Ptr{Float32}
+    peak_ratio::Ptr{Float32}
+    correlation_moment::Ptr{Float32}
+    uncertainty_u::Ptr{Float32}
+    uncertainty_v::Ptr{Float32}
+    outliers::Ptr{UInt8}
+    mask::Ptr{UInt8}
+end
+
+last_error(ctx) = unsafe_string(ccall((:hh_last_error, LIB), Cstring, (Ptr{Cvoid},), ctx))
+
+function check(st, ctx = C_NULL)
+    st == 0 && return nothing
+    (st == 1 || st == 5) && throw(ArgumentError(last_error(ctx)))
+    error("hammerhead_b200: " * last_error(ctx))
+end
+
+function _check_backend_params(::_B200Backend, passes)
+    d = [pass_desc(p) for p in passes]
+    check(ccall((:hh_check_backend_params, LIB), Int32, (Ptr{PassDesc}, Int32), d, length(d)))
+end
+
+# Context per workspace: created lazily, destroyed by a finalizer.
+mutable struct Context
+    ptr::Ptr{Cvoid}
+    function Context(device::Integer = 0)
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:hh_ctx_create, LIB), Int32, (Int32, Ref{Ptr{Cvoid}}), device, r))
+        c = new(r[])
+        finalizer(c -> ccall((:hh_ctx_destroy, LIB), Cvoid, (Ptr{Cvoid},), c.ptr), c)
+        return c
+    end
+end
+
+# The whole schedule on the device: run_piv(...; backend = :b200) with
+# Float32 images (the device path computes in Float32; FP64 only for the
+# subpixel logarithms and the uncertainty sums).
+function run_piv_b200(imgA::AbstractMatrix{<:Real}, imgB::AbstractMatrix{<:Real},
+                      passes::AbstractVector{PIVParameters};
+                      predictor_smoothing::Bool = true,
+                      mask::Union{Nothing,AbstractMatrix{Bool}} = nothing, mask_threshold::Real = 0.5,
+                      ctx::Context = Context())
+    _check_backend_params(_B200Backend(), passes)
+    size(imgA) == size(imgB) ||
+        throw(DimensionMismatch("images must have the same size, got $(size(imgA)) and $(size(imgB))"))
+    A = Matrix{Float32}(imgA)
+    B = Matrix{Float32}(imgB)
+    M = mask === nothing ? C_NULL : Matrix{UInt8}(mask)
+    nr, nc = size(A)
+    final = last(passes)
+    d = [pass_desc(p) for p in passes]
+    ny, nx, nj = Ref{Int32}(0), Ref{Int32}(0), Ref{Int64}(0)
+    check(ccall((:hh_pass_grid, LIB), Int32,
+                (Int64, Int64, Ref{PassDesc}, Ptr{UInt8}, Float64, Ref{Int32}, Ref{Int32}, Ptr{Float32},
+                 Ptr{Float32}, Ptr{UInt8}, Ptr{Int32}, Ref{Int64}),
+                nr, nc, pass_desc(final), C_NULL, mask_threshold, ny, nx, C_NULL, C_NULL, C_NULL, C_NULL, nj))
+    gy, gx = Int(ny[]), Int(nx[])
+    x = Vector{Float32}(undef, gx); y = Vector{Float32}(undef, gy)
+    f() = Matrix{Float32}(undef, gy, gx)
+    u, v, ratio, moment, su, sv = f(), f(), f(), f(), f(), f()
+    outl = Matrix{UInt8}(undef, gy, gx); gm = Matrix{UInt8}(undef, gy, gx)
+    GC.@preserve A B M x y u v ratio moment su sv outl gm begin
+        res = Ref(Result(0, 0, pointer(x), pointer(y), pointer(u), pointer(v), pointer(ratio), pointer(moment),
+                         pointer(su), pointer(sv), pointer(outl), pointer(gm)))
+        check(ccall((:hh_run_piv, LIB), Int32,
+                    (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Int64, Int64, Ptr{PassDesc}, Int32, Ptr{UInt8},
+                     Float64, Int32, Ref{Result}),
+                    ctx.ptr, A, B, nr, nc, d, length(d), M, mask_threshold, predictor_smoothing, res), ctx.ptr)
+    end
+    return PIVResult(x, y, u, v, ratio, moment, su, sv, BitMatrix(outl .!= 0), BitMatrix(gm .!= 0), final)
+end
+
+end # module
