@@ -10,9 +10,14 @@ is one complete WIDIM run of every pair. Inputs (704 MB per rank) exceed the
 
 value  = final-pass vectors of all pairs (all ranks) / max-over-ranks device
          time of the whole step (every pass, sweep, deformation, validation
-         and uncertainty), images resident in HBM.
-e2e    = the same through run_piv with pinned host images: host->device
-         copies and the result read-back inside the timed region.
+         and uncertainty), images resident in HBM, in the batched form: every
+         pass slot of all 64 pairs as one launch per kernel, convergence
+         decided on the device, the launch sequence replayed as a CUDA graph.
+         The plain per-pair form (run_piv per pair) is timed beside it
+         ("plain_form") with --plain timing it as the headline instead.
+e2e    = the same through the public batched API (BatchRunner) with pinned
+         host images: host->device copies and the result read-back inside
+         the timed region.
 
 --impl reference times the CPU restatement of the reference algorithm
 (oracle/, all host threads) on a bounded sample of the same workload; the
@@ -62,10 +67,12 @@ def make_workload(hb, name, rank=0, limit=None):
         raise ValueError(name)
     if limit:
         specs = specs[:limit]
-    pairs = []
+    pairs, scheds = [], {}
     for sp in specs:
         A, B = syn.particle_pair(sp["shape"], sp["flow"], seed=sp["seed"])
-        pairs.append(dict(sp, A=A, B=B, passes=schedule(hb, sp["schedule"])))
+        if sp["schedule"] not in scheds:
+            scheds[sp["schedule"]] = schedule(hb, sp["schedule"])
+        pairs.append(dict(sp, A=A, B=B, passes=scheds[sp["schedule"]]))
     return pairs
 
 
@@ -201,6 +208,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="batch64", choices=["batch64", "vortex"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain", action="store_true", help="time the plain per-pair form instead of the batched one")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison step")
     ap.add_argument("--limit", type=int, default=None, help="use only the first N pairs (debugging)")
     args = ap.parse_args()
 
@@ -230,80 +239,92 @@ def main():
     ws = hb.piv_workspace(device=local)
     L = hb._lib.lib()
     stream = torch.cuda.ExternalStream(ws.stream())
-    dev = []
-    for p in pairs:
-        dev.append((torch.from_numpy(np.ascontiguousarray(p["A"].T)).cuda().T,
-                    torch.from_numpy(np.ascontiguousarray(p["B"].T)).cuda().T))
+    dev = [(torch.from_numpy(np.ascontiguousarray(p["A"].T)).cuda().T,
+            torch.from_numpy(np.ascontiguousarray(p["B"].T)).cuda().T) for p in pairs]
+    scheds = [p["passes"] for p in pairs]
     nvec_rank = sum(final_vectors(hb, p) for p in pairs)
 
-    def step(timing=None):
-        fin = 0.0
-        out = []
-        for p, (dA, dB) in zip(pairs, dev):
-            r = hb.run_piv(dA, dB, p["passes"], workspace=ws)
-            fin += float(r.pass_times_ms[-1])
-            out.append(r)
-        return out, fin
-
-    for _ in range(args.warmup):
-        results, _ = step()
-    # accuracy of the last warm-up step against the known displacement
-    rms = [hb.rms_error(r, p["flow"]) for r, p in zip(results, pairs)]
-    rms_all = float(np.sqrt(np.mean(np.square(rms))))
-
-    # ---- timed region: device-resident inputs
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    L.hh_set_profiling(ws.ctx, 1)
-    hb._lib.profile_read(ws.ctx, reset=True)
-    launches0 = L.hh_launch_count(ws.ctx)
-    with ClockSampler(local) as clk:
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        fin_ms = 0.0
-        for _ in range(args.steps):
-            _, f = step()
-            fin_ms += f
-        ev1.record(stream)
+    def dev_time(fn, steps):
+        """Device time of `steps` calls of fn on the context stream (ms per call)."""
+        if world > 1:
+            dist.barrier()
         torch.cuda.synchronize()
-    launches = L.hh_launch_count(ws.ctx) - launches0
-    prof = hb._lib.profile_read(ws.ctx, reset=True)
-    L.hh_set_profiling(ws.ctx, 0)
-    ms = ev0.elapsed_time(ev1) / args.steps
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     nv = torch.tensor([nvec_rank], dtype=torch.float64, device="cuda")
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.all_reduce(nv, op=dist.ReduceOp.SUM)
-    ms_max = float(t.item())
     nvec_total = float(nv.item())
+
+    # ---- batched form, images resident in HBM, results left on the device
+    runner = hb.BatchRunner(dev, scheds, workspace=ws, graph=not args.plain)
+    if args.plain:
+        def step():
+            for p, (dA, dB) in zip(pairs, dev):
+                hb.run_piv(dA, dB, p["passes"], workspace=ws)
+    else:
+        def step():
+            runner.run(read=False)
+    for _ in range(args.warmup):
+        step()
+    runner.run()
+    results = runner.results(copy=False)
+    rms = [hb.rms_error(r, p["flow"]) for r, p in zip(results, pairs)]
+    rms_all = float(np.sqrt(np.mean(np.square(rms))))
+    launches0 = L.hh_launch_count(ws.ctx)
+    with ClockSampler(local) as clk:
+        ms = dev_time(step, args.steps)
+    launches = (L.hh_launch_count(ws.ctx) - launches0) // args.steps
+    ms_max = max_over_ranks(ms)
     value = nvec_total / (ms_max / 1e3)
 
-    # ---- end to end: pinned host images through the public API
-    pinned = [(torch.from_numpy(p["A"].T.copy()).pin_memory().numpy().T,
-               torch.from_numpy(p["B"].T.copy()).pin_memory().numpy().T) for p in pairs]
+    # ---- the plain per-pair form on the same pairs (one step), for the ratio
+    plain_ms = None
+    if not args.plain and not args.no_plain:
+        def plain_step():
+            for p, (dA, dB) in zip(pairs, dev):
+                hb.run_piv(dA, dB, p["passes"], workspace=ws)
+        plain_step()
+        plain_ms = max_over_ranks(dev_time(plain_step, 1))
+
+    # ---- kernel classes: one profiled run (events around every launch, no graph)
+    L.hh_set_profiling(ws.ctx, 1)
+    hb._lib.profile_read(ws.ctx, reset=True)
+    step()
+    torch.cuda.synchronize()
+    prof = hb._lib.profile_read(ws.ctx, reset=True)
+    L.hh_set_profiling(ws.ctx, 0)
+
+    # ---- end to end: pinned host images through the public API, results read back
+    pinned = [(torch.from_numpy(np.ascontiguousarray(p["A"].T)).pin_memory().numpy().T,
+               torch.from_numpy(np.ascontiguousarray(p["B"].T)).pin_memory().numpy().T) for p in pairs]
     h2d = sum(2 * p["A"].size * 4 for p in pairs)
-    d2h = 0
-    for p in pairs:
-        x, y, gm, _ = hb.pass_grid(p["A"].shape, p["passes"][-1])
-        d2h += gm.size * (6 * 4 + 1)
-    hb.run_piv(pinned[0][0], pinned[0][1], pairs[0]["passes"], workspace=ws)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for p, (hA, hB) in zip(pairs, pinned):
-        hb.run_piv(hA, hB, p["passes"], workspace=ws)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-    e2e_value = nvec_total / (float(e2e_ms.item()) / 1e3)
+    d2h = int(runner.offsets[-1]) * (6 * 4 + 1)
+    if args.plain:
+        def e2e_step():
+            for p, (hA, hB) in zip(pairs, pinned):
+                hb.run_piv(hA, hB, p["passes"], workspace=ws)
+    else:
+        host_runner = hb.BatchRunner(pinned, scheds, workspace=ws)
+
+        def e2e_step():
+            host_runner.run()
+    e2e_step()
+    e2e_ms = max_over_ranks(dev_time(e2e_step, max(1, min(args.steps, 3))))
+    e2e_value = nvec_total / (e2e_ms / 1e3)
 
     # ---- roofline of the dominant kernel (the fused correlation)
     c = prof["correlate"]
@@ -325,15 +346,19 @@ def main():
         base = cpu_baseline(hb, pairs)
 
     if rank == 0:
+        form = "plain (per-pair device schedule)" if args.plain else \
+            "batched (one launch per kernel per pass slot for all pairs, CUDA graph replay)"
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload_name(args.workload), "pairs_per_rank": len(pairs),
-                       "final_pass_vectors_per_rank": nvec_rank, "form": "plain (per-pair device schedule)",
+                       "final_pass_vectors_per_rank": nvec_rank, "form": form,
                        "l2": "inputs larger than L2 (704 MB per rank)", "parallelism": f"replicas x{world}"},
             "pairs_per_s": len(pairs) * world / (ms_max / 1e3),
-            "final_pass_only_vectors_per_s": nvec_total / (fin_ms / args.steps / 1e3) if fin_ms > 0 else None,
+            "plain_form": None if plain_ms is None else {
+                "value": nvec_total / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
+                "batched_speedup": plain_ms / ms_max},
             "rms_px": rms_all,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
@@ -352,6 +377,7 @@ def main():
         if line["roofline"]["frac"] is not None:
             line["roofline"]["frac"] = round(line["roofline"]["frac"], 4)
         print(json.dumps(line))
+    runner.close()
     ws.close()
     if world > 1:
         dist.destroy_process_group()

@@ -133,7 +133,7 @@ __device__ __forceinline__ bool repl_invalid(const uint8_t* flags, const uint8_t
 
 // k-th smallest (0-based) of the valid values in a square, by counting;
 // used only when a square holds more than REPL_LOCAL valid values.
-__device__ double select_square(const float* f, const uint8_t* flags, const uint8_t* gmask, int ny, int r0, int r1,
+static __device__ double select_square(const float* f, const uint8_t* flags, const uint8_t* gmask, int ny, int r0, int r1,
                                 int c0, int c1, int kth) {
   for (int cc = c0; cc <= c1; ++cc)
     for (int rr = r0; rr <= r1; ++rr) {
@@ -154,7 +154,7 @@ __device__ double select_square(const float* f, const uint8_t* flags, const uint
   return __longlong_as_double(0x7ff8000000000000LL);
 }
 
-__device__ double median_square(const float* f, const uint8_t* flags, const uint8_t* gmask, int ny, int r0, int r1,
+static __device__ double median_square(const float* f, const uint8_t* flags, const uint8_t* gmask, int ny, int r0, int r1,
                                 int c0, int c1, int n) {
   if (n <= REPL_LOCAL) {
     double buf[REPL_LOCAL];

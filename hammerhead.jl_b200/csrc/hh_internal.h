@@ -5,6 +5,8 @@
 
 namespace hh {
 
+struct BPair;
+
 constexpr int KMAX = 8;  // peaks tracked per window on the device (n_peaks <= 8)
 
 // Arguments of the fused correlation kernel (one pass, one image pair).
@@ -33,6 +35,12 @@ struct CorrArgs {
   float* packed;             // (5 + 2(K-1)) x njobs
   int32_t* locs;             // 2K x njobs (1-based row, col)
   float* planes;             // N*N x njobs correlation planes
+  // batched mode (bp != nullptr): jobs are (pair, gi | gj << 16, rs, cs);
+  // images, grid offsets and sizes come from bp[pair]; windows of pairs not
+  // live in sweep `it` are skipped
+  const BPair* bp;
+  const int32_t* done;
+  int32_t it;
 };
 
 // Launch the correlation kernel for FFT size N (square) and window W.
@@ -104,6 +112,11 @@ struct UQArgs {
   double* stats;     // 88 per job, or nullptr
   float* unc_u;      // grid-indexed outputs, or nullptr
   float* unc_v;
+  // batched mode (bp != nullptr): jobs as in CorrArgs; mode 0 = the fused
+  // estimate of a single-sweep pass (sweep 1), 1 = the post-loop estimate
+  const BPair* bp;
+  const int32_t* done;
+  int32_t mode;
 };
 cudaError_t launch_uq(const UQArgs& a, cudaStream_t s, int num_sms);
 

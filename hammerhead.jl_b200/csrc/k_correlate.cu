@@ -26,6 +26,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "hh_batch.h"
 #include "hh_fft.cuh"
 #include "hh_internal.h"
 
@@ -395,7 +396,8 @@ template <int N, int W> struct CorrCfg {
   static constexpr size_t smem() {
     return WPC * PLANE_B + WPC * (G / 32) * 3 * sizeof(double) + N * sizeof(float2) +
            WPC * (G / 32) * 2 * sizeof(uint32_t) +
-           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int) + 2 * sizeof(int)) + 64;
+           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int) + 4 * sizeof(int)) +
+           WPC * (3 * sizeof(void*) + sizeof(int64_t)) + 64;
   }
   static_assert(W == N || 2 * W == N, "window must equal the FFT size or half of it");
   static_assert(G >= 32 && G % 32 == 0, "analysis group must be whole warps");
@@ -415,7 +417,10 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
   uint32_t* red = reinterpret_cast<uint32_t*>(tw + N);
   float* s_vals = reinterpret_cast<float*>(red + WPC * (C::G / 32) * 2);
   int* s_locs = reinterpret_cast<int*>(s_vals + WPC * KMAX);
-  int* s_job = s_locs + WPC * 2 * KMAX;  // rs, cs per window
+  int* s_job = s_locs + WPC * 2 * KMAX;  // rs, cs, pair, unused per window
+  uintptr_t* s_src = reinterpret_cast<uintptr_t*>(
+      (reinterpret_cast<uintptr_t>(s_job + WPC * 4) + 7) & ~(uintptr_t)7);  // A, B, mask per window
+  int64_t* s_ld = reinterpret_cast<int64_t*>(s_src + 3 * WPC);
 
   const int tid = threadIdx.x;
   const int K = a.npeaks > 2 ? a.npeaks : 2;
@@ -432,8 +437,39 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
   for (int64_t base = (int64_t)blockIdx.x * WPC; base < a.njobs; base += (int64_t)gridDim.x * WPC) {
     if (tid < WPC) {
       const int64_t job = base + tid;
-      s_job[2 * tid] = job < a.njobs ? a.jobs[4 * job + 2] : -1;
-      s_job[2 * tid + 1] = job < a.njobs ? a.jobs[4 * job + 3] : -1;
+      int rs = -1, cs = -1, pr = -1;
+      const float* A = a.A;
+      const float* B = a.B;
+      const uint8_t* M = a.mask;
+      int64_t ld = a.ld;
+      if (job < a.njobs) {
+        if (a.bp) {
+          const int p = a.jobs[4 * job];
+          const BPair& b = a.bp[p];
+          const int gij = a.jobs[4 * job + 1];
+          const int64_t cell = (int64_t)(gij & 0xFFFF) + (int64_t)(gij >> 16) * b.ny;
+          if (bp_live(b, a.it, a.done, p) && !(b.gmask && b.gmask[cell])) {
+            pr = p;
+            rs = a.jobs[4 * job + 2];
+            cs = a.jobs[4 * job + 3];
+            const bool warped = a.it > 1 || b.has_pred0;
+            A = warped ? b.warpA : b.A;
+            B = warped ? b.warpB : b.B;
+            M = b.mask;
+            ld = b.nr;
+          }
+        } else {
+          rs = a.jobs[4 * job + 2];
+          cs = a.jobs[4 * job + 3];
+        }
+      }
+      s_job[4 * tid] = rs;
+      s_job[4 * tid + 1] = cs;
+      s_job[4 * tid + 2] = pr;
+      s_src[3 * tid] = reinterpret_cast<uintptr_t>(A);
+      s_src[3 * tid + 1] = reinterpret_cast<uintptr_t>(B);
+      s_src[3 * tid + 2] = reinterpret_cast<uintptr_t>(M);
+      s_ld[tid] = ld;
     }
     __syncthreads();
     // ---- stages 1-3: each window's thread group loads its pixels (coalesced
@@ -444,7 +480,11 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
     //      folds in Float32 left to right; the two differ by a few ulp.
     {
       const int w = tid / G, gt = tid % G, lane = tid & 31, gw = gt >> 5;
-      const int rs = s_job[2 * w], cs = s_job[2 * w + 1];
+      const int rs = s_job[4 * w], cs = s_job[4 * w + 1];
+      const float* wA = reinterpret_cast<const float*>(s_src[3 * w]);
+      const float* wB = reinterpret_cast<const float*>(s_src[3 * w + 1]);
+      const uint8_t* wM = reinterpret_cast<const uint8_t*>(s_src[3 * w + 2]);
+      const int64_t wld = s_ld[w];
       float2 z[EPT];
       bool mk[EPT];
       double sa = 0.0, sb = 0.0, cnt = 0.0;
@@ -455,9 +495,9 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
         mk[i] = true;
         if (e < W * W && rs >= 0) {
           const int p = e % W, q = e / W;
-          const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * a.ld;
-          z[i] = make_float2(__ldg(a.A + off), __ldg(a.B + off));
-          mk[i] = a.mask ? __ldg(a.mask + off) != 0 : false;
+          const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * wld;
+          z[i] = make_float2(__ldg(wA + off), __ldg(wB + off));
+          mk[i] = wM ? __ldg(wM + off) != 0 : false;
           if (!mk[i]) {
             sa += (double)z[i].x;
             sb += (double)z[i].y;
@@ -696,12 +736,29 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
     {
       const int w = tid / C::G, gt = tid % C::G;
       const int64_t job = base + w;
-      const bool active = job < a.njobs;
+      bool active = job < a.njobs;
       int64_t gid = -1;
-      if (active) gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
+      PeakOut pw = po;
+      if (active) {
+        if (a.bp) {
+          const int p = s_job[4 * w + 2];
+          active = p >= 0;
+          if (active) {
+            const BPair& b = a.bp[p];
+            const int gij = a.jobs[4 * job + 1];
+            gid = b.goff + (int64_t)(gij & 0xFFFF) + (int64_t)(gij >> 16) * b.ny;
+            pw.G = (int64_t)b.ny * b.nx;
+            pw.nalt = b.nalt;
+            pw.alt_u = a.alt_u ? a.alt_u + b.aoff - b.goff : nullptr;  // indexed by gid + m*G
+            pw.alt_v = a.alt_v ? a.alt_v + b.aoff - b.goff : nullptr;
+          }
+        } else {
+          gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
+        }
+      }
       analyze_group(reinterpret_cast<const float*>(planes + w * PS), N, N, LDR, K, a.npeaks, a.finder, a.subpixel,
                     gt, C::G, red + w * (C::G / 32) * 2, active, s_vals + w * KMAX, s_locs + w * 2 * KMAX, gid, job,
-                    po);
+                    pw);
     }
     __syncthreads();
   }

@@ -19,6 +19,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "hh_batch.h"
 #include "hh_internal.h"
 
 namespace hh {
@@ -63,59 +64,71 @@ constexpr int BS_SEG = 64, BS_WARM = 32;
 
 // forward sweep: d_k = (rhs_k - d_{k-1}/6) * inv_k into dbuf. Unknown k lives
 // at line element k + 2; rhs_0 and rhs_{m-1} carry the known c1, c_{n-2}.
+__device__ __forceinline__ void bs_fwd_item(const float* __restrict__ in, float* __restrict__ dbuf, int64_t n,
+                                            int64_t es, int64_t ls, int64_t nlines, const float* __restrict__ inv,
+                                            int64_t t) {
+  const int64_t m = n - 4;
+  const float sixth = FD(1.0f, 6.0f);
+  const int64_t line = t % nlines, seg = t / nlines;
+  const float* x = in + line * ls;
+  float* d = dbuf + line * ls;
+  const float c2 = x[es], cn1 = x[(n - 2) * es];
+  const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG), ks = max((int64_t)0, k0 - BS_WARM);
+  float dv = 0.f;
+  for (int64_t k = ks; k < k1; ++k) {
+    float rhs = x[(k + 2) * es];
+    if (k == 0) rhs = FS(rhs, FM(sixth, c2));
+    if (k == m - 1) rhs = FS(rhs, FM(sixth, cn1));
+    dv = k == 0 ? FM(rhs, inv[0]) : FM(FS(rhs, FM(sixth, dv)), inv[k]);
+    if (k >= k0) d[(k + 2) * es] = dv;
+  }
+}
+
 __global__ void bspline_fwd_kernel(const float* __restrict__ in, float* __restrict__ dbuf, int64_t n, int64_t es,
                                    int64_t ls, int64_t nlines, const float* __restrict__ inv) {
   const int64_t m = n - 4;
   if (m < 1) return;
   const int64_t nseg = (m + BS_SEG - 1) / BS_SEG;
-  const float sixth = FD(1.0f, 6.0f);
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nlines * nseg;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t line = t % nlines, seg = t / nlines;
-    const float* x = in + line * ls;
-    float* d = dbuf + line * ls;
-    const float c2 = x[es], cn1 = x[(n - 2) * es];
-    const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG), ks = max((int64_t)0, k0 - BS_WARM);
-    float dv = 0.f;
-    for (int64_t k = ks; k < k1; ++k) {
-      float rhs = x[(k + 2) * es];
-      if (k == 0) rhs = FS(rhs, FM(sixth, c2));
-      if (k == m - 1) rhs = FS(rhs, FM(sixth, cn1));
-      dv = k == 0 ? FM(rhs, inv[0]) : FM(FS(rhs, FM(sixth, dv)), inv[k]);
-      if (k >= k0) d[(k + 2) * es] = dv;
-    }
-  }
+       t += (int64_t)gridDim.x * blockDim.x)
+    bs_fwd_item(in, dbuf, n, es, ls, nlines, inv, t);
 }
 
 // backward sweep x_k = d_k - cp_k x_{k+1} into coef, plus the "Line"
 // boundary coefficients c0 = 2c1 - c2 and c_{n-1} = 2c_{n-2} - c_{n-3}.
+__device__ __forceinline__ void bs_bwd_item(float* __restrict__ coef, const float* __restrict__ dbuf, int64_t n,
+                                            int64_t es, int64_t ls, int64_t nlines, const float* __restrict__ cp,
+                                            int64_t t) {
+  const int64_t m = n - 4;
+  const int64_t line = t % nlines, seg = t / nlines;
+  float* x = coef + line * ls;
+  if (m < 1) {  // n == 4: c1 = b1, c2 = b2 only
+    const float c1 = x[es], c2 = x[2 * es];
+    x[0] = FS(FM(2.0f, c1), c2);
+    x[3 * es] = FS(FM(2.0f, c2), c1);
+    return;
+  }
+  const float* d = dbuf + line * ls;
+  const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG), ke = min(m - 1, k1 - 1 + BS_WARM);
+  float xv = 0.f, xlast = 0.f;
+  for (int64_t k = ke; k >= k0; --k) {
+    const float dk = d[(k + 2) * es];
+    xv = k == ke ? dk : FS(dk, FM(cp[k], xv));
+    if (k < k1) x[(k + 2) * es] = xv;
+    if (k == m - 1) xlast = xv;
+  }
+  if (k0 == 0) x[0] = FS(FM(2.0f, x[es]), xv);  // xv == x_0 here
+  if (k1 == m) x[(n - 1) * es] = FS(FM(2.0f, x[(n - 2) * es]), xlast);
+}
+
 __global__ void bspline_bwd_kernel(float* __restrict__ coef, const float* __restrict__ dbuf, int64_t n, int64_t es,
                                    int64_t ls, int64_t nlines, const float* __restrict__ cp) {
   const int64_t m = n - 4;
   if (n < 4) return;
   const int64_t nseg = m < 1 ? 1 : (m + BS_SEG - 1) / BS_SEG;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nlines * nseg;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t line = t % nlines, seg = t / nlines;
-    float* x = coef + line * ls;
-    if (m < 1) {  // n == 4: c1 = b1, c2 = b2 only
-      const float c1 = x[es], c2 = x[2 * es];
-      x[0] = FS(FM(2.0f, c1), c2);
-      x[3 * es] = FS(FM(2.0f, c2), c1);
-      continue;
-    }
-    const float* d = dbuf + line * ls;
-    const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG), ke = min(m - 1, k1 - 1 + BS_WARM);
-    float xv = 0.f, xlast = 0.f;
-    for (int64_t k = ke; k >= k0; --k) {
-      const float dk = d[(k + 2) * es];
-      xv = k == ke ? dk : FS(dk, FM(cp[k], xv));
-      if (k < k1) x[(k + 2) * es] = xv;
-      if (k == m - 1) xlast = xv;
-    }
-    if (k0 == 0) x[0] = FS(FM(2.0f, x[es]), xv);  // xv == x_0 here
-    if (k1 == m) x[(n - 1) * es] = FS(FM(2.0f, x[(n - 2) * es]), xlast);
-  }
+       t += (int64_t)gridDim.x * blockDim.x)
+    bs_bwd_item(coef, dbuf, n, es, ls, nlines, cp, t);
 }
 
 static unsigned seg_blocks(int64_t work) {
@@ -247,6 +260,146 @@ cudaError_t launch_node_values(const float* pu, const float* pv, PredGrid g, con
   if (blocks > 148 * 8) blocks = 148 * 8;
   if (blocks < 1) blocks = 1;
   node_values_kernel<<<(unsigned)blocks, 256, 0, s>>>(pu, pv, g, y, ny, x, nx, u, v);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Batched forms: every pair of a pass slot in one launch (see hh_batch.h).
+
+#define B_STRIDE(k, n) for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (n); k += (int64_t)gridDim.x * blockDim.x)
+
+static unsigned b_blocks(int64_t n, int cap_per_sm = 16) {
+  int64_t b = (n + 255) / 256;
+  if (b > 148 * (int64_t)cap_per_sm) b = 148 * (int64_t)cap_per_sm;
+  return (unsigned)(b < 1 ? 1 : b);
+}
+
+// prefilter of both frames (blockIdx.y: 0 = A, 1 = B) of every deforming pair
+__global__ void b_pad_copy_kernel(const BPair* __restrict__ bp, int npairs, int64_t qtot) {
+  const int img = blockIdx.y;
+  B_STRIDE(k, qtot) {
+    const BPair& b = bp[bp_find<&BPair::qoff>(bp, npairs, k)];
+    const int64_t ld = b.nr + 2, l = k - b.qoff;
+    if (!b.deforms || l >= ld * (b.nc + 2)) continue;
+    const int64_t i = l % ld, j = l / ld;
+    const float* src = img ? b.B : b.A;
+    float* coef = img ? b.coefB : b.coefA;
+    coef[l] = (i >= 1 && i <= b.nr && j >= 1 && j <= b.nc) ? src[(i - 1) + (j - 1) * b.nr] : 0.f;
+  }
+}
+
+__device__ __forceinline__ int64_t b_nseg(int64_t n) { return n >= 5 ? (n - 4 + BS_SEG - 1) / BS_SEG : 1; }
+
+// dim 1 (image columns, pass 0 = forward, 1 = backward) or dim 2 (padded rows)
+template <int DIM, int PASS>
+__global__ void b_bspline_kernel(const BPair* __restrict__ bp, int npairs, int64_t wtot, float* dbuf, int64_t qtot) {
+  const int img = blockIdx.y;
+  B_STRIDE(t, wtot) {
+    const BPair& b = bp[bp_find<DIM == 1 ? &BPair::wcol : &BPair::wrow>(bp, npairs, t)];
+    if (!b.deforms) continue;
+    const int64_t ld = b.nr + 2, ncols = b.nc + 2;
+    const int64_t n = DIM == 1 ? ld : ncols;
+    const int64_t nlines = DIM == 1 ? b.nc : ld;
+    const int64_t l = t - (DIM == 1 ? b.wcol : b.wrow);
+    if (l >= nlines * b_nseg(n)) continue;
+    float* coef = img ? b.coefB : b.coefA;
+    float* d = dbuf + (int64_t)img * qtot + b.qoff;
+    const int64_t off = DIM == 1 ? ld : 0, es = DIM == 1 ? 1 : ld, ls = DIM == 1 ? ld : 1;
+    if (PASS == 0) {
+      if (n - 4 >= 1) bs_fwd_item(coef + off, d + off, n, es, ls, nlines, DIM == 1 ? b.ivc : b.ivr, l);
+    } else {
+      if (n >= 4) bs_bwd_item(coef + off, d + off, n, es, ls, nlines, DIM == 1 ? b.cpc : b.cpr, l);
+    }
+  }
+}
+
+cudaError_t launch_b_prefilter(const BPair* bp, int npairs, int64_t qtot, int64_t wcol_tot, int64_t wrow_tot,
+                               float* dbuf, cudaStream_t s) {
+  if (qtot <= 0) return cudaSuccess;
+  b_pad_copy_kernel<<<dim3(b_blocks(qtot), 2), 256, 0, s>>>(bp, npairs, qtot);
+  if (wcol_tot > 0) {
+    b_bspline_kernel<1, 0><<<dim3(b_blocks(wcol_tot, 32), 2), 256, 0, s>>>(bp, npairs, wcol_tot, dbuf, qtot);
+    b_bspline_kernel<1, 1><<<dim3(b_blocks(wcol_tot, 32), 2), 256, 0, s>>>(bp, npairs, wcol_tot, dbuf, qtot);
+  }
+  if (wrow_tot > 0) {
+    b_bspline_kernel<2, 0><<<dim3(b_blocks(wrow_tot, 32), 2), 256, 0, s>>>(bp, npairs, wrow_tot, dbuf, qtot);
+    b_bspline_kernel<2, 1><<<dim3(b_blocks(wrow_tot, 32), 2), 256, 0, s>>>(bp, npairs, wrow_tot, dbuf, qtot);
+  }
+  return cudaGetLastError();
+}
+
+// the predictor grid of sweep `it`: the previous slot's grid in sweep 1,
+// this slot's grid afterwards
+__device__ __forceinline__ PredGrid b_pred_grid(const BPair& b, int it) {
+  PredGrid g;
+  if (it == 1) {
+    g.gny = b.pgny; g.gnx = b.pgnx; g.y0 = b.py0; g.ysp = b.pysp; g.x0 = b.px0; g.xsp = b.pxsp;
+  } else {
+    g.gny = b.ny; g.gnx = b.nx; g.y0 = b.gy0; g.ysp = b.gysp; g.x0 = b.gx0; g.xsp = b.gxsp;
+  }
+  return g;
+}
+
+// Start of sweep `it`: the node values of the predictor (zero without one),
+// NaN uncertainties at the start of the slot, and the sweep count of pairs
+// in their final pass.
+__global__ void b_sweep_begin_kernel(const BPair* __restrict__ bp, int npairs, const int32_t* __restrict__ done, int it,
+                                     int64_t gtot, const float* __restrict__ pu, const float* __restrict__ pv, float* u,
+                                     float* v, float* uncu, float* uncv, int32_t* sweeps) {
+  B_STRIDE(k, gtot) {
+    const int p = bp_find<&BPair::coff>(bp, npairs, k);
+    const BPair& b = bp[p];
+    const int64_t l = k - b.coff;
+    if (!bp_live(b, it, done, p) || l >= (int64_t)b.ny * b.nx) continue;
+    const int64_t id = b.goff + l;
+    if (l == 0 && b.is_final) sweeps[p] = it;
+    if (it == 1) {
+      uncu[id] = __int_as_float(0x7fc00000);
+      uncv[id] = __int_as_float(0x7fc00000);
+    }
+    if (it > 1 || b.has_pred0) {
+      const PredGrid g = b_pred_grid(b, it);
+      const int gi = (int)(l % b.ny), gj = (int)(l / b.ny);
+      const float y = FA(b.gy0, FM((float)gi, b.gysp)), x = FA(b.gx0, FM((float)gj, b.gxsp));
+      u[id] = bilinear(pu + b.goff, g, y, x);
+      v[id] = bilinear(pv + b.goff, g, y, x);
+    } else {
+      u[id] = 0.f;
+      v[id] = 0.f;
+    }
+  }
+}
+
+cudaError_t launch_b_sweep_begin(const BPair* bp, int npairs, const int32_t* done, int it, int64_t gtot,
+                                 const float* pu, const float* pv, float* u, float* v, float* uncu, float* uncv,
+                                 int32_t* sweeps, cudaStream_t s) {
+  if (gtot <= 0) return cudaSuccess;
+  b_sweep_begin_kernel<<<b_blocks(gtot), 256, 0, s>>>(bp, npairs, done, it, gtot, pu, pv, u, v, uncu, uncv, sweeps);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(256) b_deform_kernel(const BPair* __restrict__ bp, int npairs,
+                                                       const int32_t* __restrict__ done, int it, int64_t ptot,
+                                                       const float* __restrict__ pu, const float* __restrict__ pv) {
+  B_STRIDE(k, ptot) {
+    const int p = bp_find<&BPair::pcoff>(bp, npairs, k);
+    const BPair& b = bp[p];
+    const int64_t l = k - b.pcoff;
+    if (!bp_live(b, it, done, p) || !(it > 1 || b.has_pred0) || !b.deforms || l >= b.nr * b.nc) continue;
+    const PredGrid g = b_pred_grid(b, it);
+    const int64_t r = l % b.nr, c = l / b.nr;
+    const float R = (float)(r + 1), Cc = (float)(c + 1);
+    const float du2 = FD(bilinear(pu + b.goff, g, R, Cc), 2.f);
+    const float dv2 = FD(bilinear(pv + b.goff, g, R, Cc), 2.f);
+    b.warpA[l] = bspline_eval(b.coefA, b.nr, b.nc, FS(R, dv2), FS(Cc, du2));
+    b.warpB[l] = bspline_eval(b.coefB, b.nr, b.nc, FA(R, dv2), FA(Cc, du2));
+  }
+}
+
+cudaError_t launch_b_deform(const BPair* bp, int npairs, const int32_t* done, int it, int64_t ptot, const float* pu,
+                            const float* pv, cudaStream_t s) {
+  if (ptot <= 0) return cudaSuccess;
+  b_deform_kernel<<<b_blocks(ptot, 32), 256, 0, s>>>(bp, npairs, done, it, ptot, pu, pv);
   return cudaGetLastError();
 }
 

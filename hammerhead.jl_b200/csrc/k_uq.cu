@@ -10,6 +10,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "hh_batch.h"
 #include "hh_internal.h"
 
 namespace hh {
@@ -93,13 +94,33 @@ __global__ void __launch_bounds__(UQ_THREADS) uq_kernel(const UQArgs a, const UQ
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int64_t job = blockIdx.x; job < a.njobs; job += gridDim.x) {
     const int rs = a.jobs[4 * job + 2], cs = a.jobs[4 * job + 3];
+    const float* A = a.A;
+    const float* B = a.B;
+    const uint8_t* M = a.mask;
+    int64_t ld = a.ld, gid;
+    if (a.bp) {  // batched: the pair's images and grid region; skip windows it does not need
+      const int p = a.jobs[4 * job];
+      const BPair& b = a.bp[p];
+      const int gij = a.jobs[4 * job + 1];
+      const int64_t cell = (int64_t)(gij & 0xFFFF) + (int64_t)(gij >> 16) * b.ny;
+      const bool on = a.mode == 0 ? (b.unc_fused && bp_live(b, 1, a.done, p)) : (b.unc_post && b.live);
+      if (!on || (b.gmask && b.gmask[cell])) continue;  // uniform across the CTA
+      const bool warped = a.mode == 1 || b.has_pred0;
+      A = warped ? b.warpA : b.A;
+      B = warped ? b.warpB : b.B;
+      M = b.mask;
+      ld = b.nr;
+      gid = b.goff + cell;
+    } else {
+      gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
+    }
     // windows and their means (load_uncertainty_windows!, :51-83)
     double sa = 0.0, sb = 0.0, cnt = 0.0;
     for (int k = tid; k < W * W; k += UQ_THREADS) {
       const int p = k % W, q = k / W;
-      const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * a.ld;
-      const float va = a.A[off], vb = a.B[off];
-      const uint8_t mk = a.mask ? a.mask[off] : 0;
+      const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * ld;
+      const float va = A[off], vb = B[off];
+      const uint8_t mk = M ? M[off] : 0;
       wa[k] = va;
       wb[k] = vb;
       mf[k] = mk;
@@ -200,7 +221,6 @@ __global__ void __launch_bounds__(UQ_THREADS) uq_kernel(const UQArgs a, const UQ
     if (a.stats)
       for (int it = tid; it < 88; it += UQ_THREADS) a.stats[job * 88 + it] = stats[it];
     if (a.unc_u && tid < 2) {
-      const int64_t gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
       const float sg = uq_finalize(stats + 44 * tid, o);
       if (tid == 0) a.unc_u[gid] = sg;
       else a.unc_v[gid] = sg;

@@ -84,6 +84,39 @@ class hh_result(ctypes.Structure):
     ]
 
 
+class hh_batch_pair(ctypes.Structure):
+    _fields_ = [
+        ("A", ctypes.c_void_p),
+        ("B", ctypes.c_void_p),
+        ("mask", ctypes.c_void_p),
+        ("nr", ctypes.c_int64),
+        ("nc", ctypes.c_int64),
+        ("schedule", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+class hh_batch_result(ctypes.Structure):
+    _fields_ = [
+        ("ny", _I32),
+        ("nx", _I32),
+        ("offsets", _I64),
+        ("u", _F),
+        ("v", _F),
+        ("peak_ratio", _F),
+        ("correlation_moment", _F),
+        ("uncertainty_u", _F),
+        ("uncertainty_v", _F),
+        ("outliers", _U8),
+        ("mask", _U8),
+        ("sweeps", _I32),
+    ]
+
+
+HH_BATCH_DEVICE_INPUTS = 1
+HH_BATCH_NO_GRAPH = 2
+
+
 class hh_kernel_profile(ctypes.Structure):
     _fields_ = [("launches", ctypes.c_int64), ("ms", ctypes.c_double), ("flops", ctypes.c_double),
                 ("bytes", ctypes.c_double), ("units", ctypes.c_int64)]
@@ -111,6 +144,11 @@ SIGNATURES = [
      [_CTX, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, _PASS, ctypes.c_int32, ctypes.c_void_p,
       ctypes.c_double, ctypes.c_int32, ctypes.POINTER(hh_result)]),
     ("hh_last_pass_times", ctypes.c_int32, [_CTX, ctypes.c_int32, _F, _I32]),
+    ("hh_batch_grid", ctypes.c_int32,
+     [ctypes.POINTER(hh_batch_pair), ctypes.c_int32, _PASS, _I32, ctypes.c_int32, _I32, _I32, _I64]),
+    ("hh_run_batched", ctypes.c_int32,
+     [_CTX, ctypes.POINTER(hh_batch_pair), ctypes.c_int32, _PASS, _I32, ctypes.c_int32, ctypes.c_double,
+      ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(hh_batch_result)]),
     ("hh_stage_pair", ctypes.c_int32, [_CTX, _F, _F, ctypes.c_int64, ctypes.c_int64]),
     ("hh_apply_predictor", ctypes.c_int32,
      [_CTX, _F, _F, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,

@@ -1,0 +1,226 @@
+"""Batched planar WIDIM: many image pairs of uneven size and schedule at once.
+
+The reference analyses a stream of pairs with run_piv_sequence
+(src/io.jl:229-361), one run_piv per pair, results identical to separate
+calls. Here the whole batch runs as one device schedule (hh_run_batched):
+every pass slot is one launch per kernel for all pairs, convergence is
+decided on the device, and the launch sequence of a batch shape is captured
+in a CUDA graph once and replayed. Results equal run_piv on each pair.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import ArgumentError, DimensionMismatch
+from .params import PIVParameters
+from .pipeline import PIVResult, PIVWorkspace, _is_device_tensor, check_backend_params, pass_grid
+
+_FIELDS = ("u", "v", "peak_ratio", "correlation_moment", "uncertainty_u", "uncertainty_v")
+
+
+def _schedules(passes, npairs):
+    """One pass list per pair, deduplicated: (unique schedules, index per pair)."""
+    if isinstance(passes, PIVParameters):
+        per_pair = [[passes]] * npairs
+    elif passes and all(isinstance(p, PIVParameters) for p in passes):
+        per_pair = [list(passes)] * npairs
+    else:
+        per_pair = [[s] if isinstance(s, PIVParameters) else list(s) for s in passes]
+        if len(per_pair) != npairs:
+            raise DimensionMismatch(f"got {len(per_pair)} pass schedules for {npairs} pairs")
+    uniq, index = [], []
+    for s in per_pair:
+        if not s:
+            raise ArgumentError("at least one pass is required")
+        for k, u in enumerate(uniq):
+            if len(u) == len(s) and all(a is b or a == b for a, b in zip(u, s)):
+                index.append(k)
+                break
+        else:
+            uniq.append(s)
+            index.append(len(uniq) - 1)
+    return uniq, index
+
+
+class BatchRunner:
+    """A prepared batch: pair descriptors, pass tables and (page-locked)
+    result buffers built once; `run()` is one library call. Keep the images
+    (and masks) alive and unchanged in shape while the runner is used;
+    their contents may change between runs."""
+
+    def __init__(self, pairs, passes, *, masks=None, predictor_smoothing=True, mask_threshold=0.5, workspace=None,
+                 graph=True, pinned=True):
+        if not pairs:
+            raise ArgumentError("pairs must not be empty")
+        if not (0 < mask_threshold <= 1):
+            raise ArgumentError(f"mask_threshold must be in (0, 1], got {mask_threshold}")
+        n = len(pairs)
+        masks = [None] * n if masks is None else list(masks)
+        if len(masks) != n:
+            raise DimensionMismatch(f"got {len(masks)} masks for {n} pairs")
+        self.schedules, self.index = _schedules(passes, n)
+        for s in self.schedules:
+            check_backend_params(s)
+        self.device = _is_device_tensor(pairs[0][0])
+        self._keep = []
+        self.pairs = (_lib.hh_batch_pair * n)()
+        for p, ((A, B), M) in enumerate(zip(pairs, masks)):
+            if tuple(A.shape) != tuple(B.shape):
+                raise DimensionMismatch(f"images must have the same size, got {tuple(A.shape)} and {tuple(B.shape)}")
+            if len(A.shape) != 2:
+                raise DimensionMismatch("images must be matrices")
+            if M is not None and tuple(M.shape) != tuple(A.shape):
+                raise DimensionMismatch(f"mask must have the same size as the images, got {tuple(M.shape)}")
+            nr, nc = int(A.shape[0]), int(A.shape[1])
+            if self.device != _is_device_tensor(A) or self.device != _is_device_tensor(B):
+                raise ArgumentError("all images of a batch must be host arrays or all device tensors")
+            if self.device:
+                for t in (A, B) + ((M,) if M is not None else ()):
+                    if t.stride(0) != 1 or t.stride(1) != nr:
+                        raise ArgumentError("device images must be column-major (stride (1, nrows))")
+                ptrs = [t.data_ptr() if t is not None else None for t in (A, B, M)]
+                self._keep.append((A, B, M))
+            else:
+                a = _lib.as_f32_colmajor(A)
+                b = _lib.as_f32_colmajor(B)
+                m = None if M is None else np.asfortranarray(M, dtype=np.uint8)
+                self._keep.append((a, b, m))
+                ptrs = [x.ctypes.data if x is not None else None for x in (a, b, m)]
+            self.pairs[p] = _lib.hh_batch_pair(ptrs[0], ptrs[1], ptrs[2], nr, nc, self.index[p], 0)
+        flat = [p for s in self.schedules for p in s]
+        self.descs = (_lib.hh_pass_desc * len(flat))(*[p.to_desc() for p in flat])
+        offs = np.cumsum([0] + [len(s) for s in self.schedules]).astype(np.int32)
+        self.offsets_in = np.ascontiguousarray(offs)
+        self.ny = np.zeros(n, np.int32)
+        self.nx = np.zeros(n, np.int32)
+        self.offsets = np.zeros(n + 1, np.int64)
+        L = _lib.lib()
+        _lib.check(L.hh_batch_grid(self.pairs, n, self.descs, _lib.i32ptr(self.offsets_in), len(self.schedules),
+                                   _lib.i32ptr(self.ny), _lib.i32ptr(self.nx),
+                                   self.offsets.ctypes.data_as(_lib._I64)))
+        R = int(self.offsets[-1])
+        self.out = {k: self._buffer(R, np.float32, pinned) for k in _FIELDS}
+        self.outliers = self._buffer(R, np.uint8, pinned)
+        self.gmask = np.zeros(R, np.uint8)
+        self.sweeps = np.zeros(n, np.int32)
+        self.result = _lib.hh_batch_result(
+            _lib.i32ptr(self.ny), _lib.i32ptr(self.nx), self.offsets.ctypes.data_as(_lib._I64),
+            *[_lib.fptr(self.out[k]) for k in _FIELDS], _lib.u8ptr(self.outliers), _lib.u8ptr(self.gmask),
+            _lib.i32ptr(self.sweeps))
+        self.smoothing = int(bool(predictor_smoothing))
+        self.mask_threshold = float(mask_threshold)
+        self.flags = (_lib.HH_BATCH_DEVICE_INPUTS if self.device else 0) | (0 if graph else _lib.HH_BATCH_NO_GRAPH)
+        self._own_ws = workspace is None
+        self.ws = workspace if workspace is not None else PIVWorkspace()
+        self.npairs = n
+        self._grids = {}
+
+    def _buffer(self, n, dtype, pinned):
+        """Host result buffer; page-locked (through torch) when available so
+        the read-back is one asynchronous copy per field."""
+        if pinned:
+            try:
+                import torch
+                if torch.cuda.is_available():
+                    t = torch.empty(max(n, 1), dtype={np.float32: torch.float32, np.uint8: torch.uint8}[dtype],
+                                    pin_memory=True)
+                    self._keep.append(t)
+                    return t.numpy()[:n]
+            except Exception:  # noqa: BLE001 -- no CUDA torch: pageable buffers
+                pass
+        return np.empty(n, dtype)
+
+    @property
+    def final_vectors(self):
+        """Final-pass vectors of the batch (grid cells not masked)."""
+        return int(self.offsets[-1] - self.gmask.sum())
+
+    def run(self, read=True):
+        """Analyse the whole batch once; results land in the runner's buffers
+        (read=False leaves them on the device, for timing the device work)."""
+        L = _lib.lib()
+        st = L.hh_run_batched(self.ws.ctx, self.pairs, self.npairs, self.descs, _lib.i32ptr(self.offsets_in),
+                              len(self.schedules), self.mask_threshold, self.smoothing, self.flags,
+                              ctypes.byref(self.result) if read else None)
+        _lib.check(st, self.ws.ctx)
+        return self
+
+    def results(self, copy=True):
+        """PIVResult per pair (views into the runner's buffers unless copy)."""
+        res = []
+        for p in range(self.npairs):
+            a, b = int(self.offsets[p]), int(self.offsets[p + 1])
+            ny, nx = int(self.ny[p]), int(self.nx[p])
+            sched = self.schedules[self.index[p]]
+            nr, nc = int(self.pairs[p].nr), int(self.pairs[p].nc)
+            key = (nr, nc, self.index[p])
+            if key not in self._grids:
+                x, y, _, _ = pass_grid((nr, nc), sched[-1])
+                self._grids[key] = (x, y)
+            x, y = self._grids[key]
+
+            def f(arr):
+                v = arr[a:b].reshape((ny, nx), order="F")
+                return v.copy(order="F") if copy else v
+
+            sweeps = np.zeros(len(sched), np.int32)
+            sweeps[-1] = self.sweeps[p]
+            res.append(PIVResult(x.copy(), y.copy(), *[f(self.out[k]) for k in _FIELDS], f(self.outliers).astype(bool),
+                                 f(self.gmask).astype(bool), sched[-1], None, None, None, sweeps))
+        return res
+
+    def close(self):
+        if self._own_ws and self.ws is not None:
+            self.ws.close()
+        self.ws = None
+
+
+def run_piv_batch(pairs, passes, *, masks=None, predictor_smoothing=True, mask_threshold=0.5, workspace=None,
+                  graph=True):
+    """Analyse many pairs at once; returns one PIVResult per pair, equal to
+    run_piv(A, B, schedule) of each pair.
+
+    `pairs`: list of (A, B) images (numpy (rows, cols) arrays, or column-major
+    torch CUDA tensors); `passes`: one schedule (a PIVParameters or a list of
+    them) for every pair, or one schedule per pair; `masks`: None or one mask
+    (or None) per pair."""
+    runner = BatchRunner(pairs, passes, masks=masks, predictor_smoothing=predictor_smoothing,
+                         mask_threshold=mask_threshold, workspace=workspace, graph=graph, pinned=False)
+    try:
+        return runner.run().results(copy=True)
+    finally:
+        runner.close()
+
+
+def run_piv_sequence(pairs, params=None, *, preprocess=None, progress=False, on_result=None, mask=None,
+                     batch_size=64, predictor_smoothing=True, mask_threshold=0.5, workspace=None):
+    """run_piv_sequence (src/io.jl:229-247) for in-memory pairs: the pairs are
+    analysed in batches of `batch_size` with run_piv_batch; `on_result(i, r)`
+    and `progress(i, n)` are called per pair in order (1-based i). `mask` is
+    None, one mask for every pair, or a function (i, pair) -> mask."""
+    if not pairs:
+        raise ArgumentError("pairs must not be empty")
+    if params is None:
+        params = [PIVParameters()]
+    n = len(pairs)
+    out = []
+    for start in range(0, n, batch_size):
+        chunk = pairs[start:start + batch_size]
+        imgs = [(preprocess(a), preprocess(b)) if preprocess else (a, b) for a, b in chunk]
+        if mask is None:
+            ms = None
+        elif callable(mask):
+            ms = [mask(start + j + 1, chunk[j]) for j in range(len(chunk))]
+        else:
+            ms = [mask] * len(chunk)
+        res = run_piv_batch(imgs, params, masks=ms, predictor_smoothing=predictor_smoothing,
+                            mask_threshold=mask_threshold, workspace=workspace)
+        for j, r in enumerate(res):
+            i = start + j + 1
+            out.append(r)
+            if on_result is not None:
+                on_result(i, r)
+            if callable(progress):
+                progress(i, n)
+    return out

@@ -140,6 +140,52 @@ hh_status hh_run_piv_device(hh_ctx* ctx, const float* dA, const float* dB, int64
                             const hh_pass_desc* passes, int32_t npasses, const uint8_t* dmask,
                             double mask_threshold, int32_t predictor_smoothing, hh_result* out);
 
+/* ---- Batched schedule: many pairs of uneven size and schedule at once ------
+ *
+ * The reference analyses a stream of pairs with run_piv_sequence
+ * (src/io.jl:229-247, _run_sequence :307-361): one run_piv per pair, in
+ * order, with results identical to separate calls. hh_run_batched runs every pair's whole
+ * schedule together: pass slot k (the k-th pass of every pair that has one)
+ * is one launch per kernel for all pairs, each sweep's convergence test is
+ * decided on the device (no host round trip), and the launch sequence of a
+ * given batch shape is captured once in a CUDA graph and replayed. Results
+ * equal hh_run_piv on each pair.
+ *
+ * Pair p uses passes[schedule_offsets[s] .. schedule_offsets[s+1]) with
+ * s = pairs[p].schedule. Images are column-major float32 (host memory, or
+ * device memory of the context's device with HH_BATCH_DEVICE_INPUTS; then
+ * they must stay valid until the call returns). */
+typedef struct hh_batch_pair {
+  const float* A;
+  const float* B;
+  const uint8_t* mask;  /* nonzero = excluded, or NULL */
+  int64_t nr, nc;
+  int32_t schedule;
+  int32_t reserved;
+} hh_batch_pair;
+
+/* Final-pass results in compact host arrays: pair p's ny[p] x nx[p] grid
+ * (column-major) occupies [offsets[p], offsets[p+1]). Any pointer may be
+ * NULL. Page-locked buffers make the read-back one asynchronous copy each. */
+typedef struct hh_batch_result {
+  int32_t *ny, *nx;       /* npairs */
+  int64_t* offsets;       /* npairs + 1 */
+  float *u, *v, *peak_ratio, *correlation_moment, *uncertainty_u, *uncertainty_v;
+  uint8_t *outliers, *mask;
+  int32_t* sweeps;        /* npairs: sweeps run in each pair's final pass */
+} hh_batch_result;
+
+#define HH_BATCH_DEVICE_INPUTS 1 /* A, B, mask are device pointers */
+#define HH_BATCH_NO_GRAPH 2      /* launch directly instead of replaying a captured graph */
+
+/* Final grid sizes and result offsets of a batch (host-only). */
+hh_status hh_batch_grid(const hh_batch_pair* pairs, int32_t npairs, const hh_pass_desc* passes,
+                        const int32_t* schedule_offsets, int32_t nschedules, int32_t* ny, int32_t* nx,
+                        int64_t* offsets);
+hh_status hh_run_batched(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npairs, const hh_pass_desc* passes,
+                         const int32_t* schedule_offsets, int32_t nschedules, double mask_threshold,
+                         int32_t predictor_smoothing, int32_t flags, hh_batch_result* out);
+
 /* Per-pass timing of the last hh_run_piv* call on ctx, measured with CUDA
  * events on the context stream: ms[k] = device time of pass k (all sweeps,
  * deformation, validation, uncertainty); sweeps[k] = sweeps run. */

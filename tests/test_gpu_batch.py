@@ -1,0 +1,168 @@
+"""Batched schedule (hh_run_batched) against the per-pair schedule.
+
+The batched form runs the same per-window and per-cell device code as
+run_piv, only over every pair of a pass slot at once, with convergence
+decided on the device; so each pair's result must equal run_piv on that pair
+bit for bit (the property run_piv_sequence states for the reference,
+src/io.jl:225-228), for uneven pair sizes, mixed schedules, masks, early
+convergence, device-resident inputs, and graph replay.
+"""
+import numpy as np
+import pytest
+
+FIELDS = ("u", "v", "peak_ratio", "correlation_moment", "uncertainty_u", "uncertainty_v")
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(a, b):
+    for k in FIELDS:
+        x, y = getattr(a, k), getattr(b, k)
+        assert x.shape == y.shape, k
+        assert np.array_equal(x, y, equal_nan=True), (k, np.nanmax(np.abs(x - y)))
+    assert np.array_equal(a.outliers, b.outliers)
+    assert np.array_equal(a.mask, b.mask)
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
+
+
+def _mixed(hb, n=6, seed=7):
+    syn = hb.synthetic
+    shapes = [(256, 256), (192, 320), (320, 256), (256, 384), (128, 192), (384, 384)]
+    pairs, flows = [], []
+    for i in range(n):
+        flow = syn.sine_shear_flow(1.5 + i * 0.7, 160.0 + 40 * i) if i % 2 == 0 else syn.uniform_flow(2.3 - i, 1.1 + 0.4 * i)
+        A, B = syn.particle_pair(shapes[i % len(shapes)], flow, seed=seed + i)
+        pairs.append((A, B))
+        flows.append(flow)
+    return pairs, flows
+
+
+def _schedules(hb):
+    s1 = hb.multipass_parameters([64, 32, 16], padding=True, apodization="gauss",
+                                 final=dict(max_iterations=3, uncertainty=True))
+    s2 = hb.multipass_parameters([48, 24], padding=True, apodization="gauss",
+                                 final=dict(max_iterations=3, uncertainty=True))
+    return s1, s2
+
+
+def test_batch_equals_per_pair_mixed(hb, ws):
+    pairs, flows = _mixed(hb)
+    s1, s2 = _schedules(hb)
+    sched = [s1 if i % 2 == 0 else s2 for i in range(len(pairs))]
+    res = hb.run_piv_batch(pairs, sched, workspace=ws)
+    assert len(res) == len(pairs)
+    for (A, B), s, r, flow in zip(pairs, sched, res, flows):
+        ref = hb.run_piv(A, B, s, workspace=ws)
+        _same(r, ref)
+        assert r.sweeps[-1] == ref.sweeps[-1]
+        assert hb.rms_error(r, flow) < 0.1
+
+
+def test_batch_graph_replay_and_direct(hb, ws):
+    pairs, _ = _mixed(hb, n=4, seed=31)
+    s1, s2 = _schedules(hb)
+    sched = [s1, s2, s2, s1]
+    runner = hb.BatchRunner(pairs, sched, workspace=ws, graph=True)
+    first = runner.run().results()
+    again = runner.run().results()      # graph replay
+    for a, b in zip(first, again):
+        _same(a, b)
+    direct = hb.run_piv_batch(pairs, sched, workspace=ws, graph=False)
+    for a, b in zip(first, direct):
+        _same(a, b)
+    runner.close()
+
+
+def test_batch_new_images_same_shape(hb, ws):
+    # a replayed graph reads the image pointers from the descriptor tables,
+    # so new contents (and new arrays) of the same shapes are analysed
+    s1, s2 = _schedules(hb)
+    p1, _ = _mixed(hb, n=3, seed=101)
+    p2, _ = _mixed(hb, n=3, seed=202)
+    hb.run_piv_batch(p1, [s1, s2, s1], workspace=ws)
+    res = hb.run_piv_batch(p2, [s1, s2, s1], workspace=ws)
+    for (A, B), s, r in zip(p2, [s1, s2, s1], res):
+        _same(r, hb.run_piv(A, B, s, workspace=ws))
+
+
+def test_batch_masks(hb, ws):
+    pairs, _ = _mixed(hb, n=3, seed=55)
+    s1, s2 = _schedules(hb)
+    masks = []
+    for i, (A, _) in enumerate(pairs):
+        if i == 1:
+            masks.append(None)
+            continue
+        m = np.zeros(A.shape, bool)
+        r0, c0 = A.shape[0] // 3, A.shape[1] // 4
+        m[r0:r0 + 60, c0:c0 + 70] = True
+        masks.append(m)
+    sched = [s1, s2, s2]
+    res = hb.run_piv_batch(pairs, sched, masks=masks, workspace=ws)
+    for (A, B), s, m, r in zip(pairs, sched, masks, res):
+        ref = hb.run_piv(A, B, s, mask=m, workspace=ws)
+        _same(r, ref)
+    assert res[0].mask.any() and not res[1].mask.any()
+
+
+def test_batch_convergence_on_device(hb, ws):
+    # convergence_tol large enough that some pairs stop after 2 sweeps while
+    # others run all 4: the device-side test must reproduce each pair's count
+    pairs, _ = _mixed(hb, n=6, seed=77)
+    sched = hb.multipass_parameters([32, 16], padding=True, final=dict(max_iterations=4, convergence_tol=0.02))
+    res = hb.run_piv_batch(pairs, sched, workspace=ws)
+    counts = []
+    for (A, B), r in zip(pairs, res):
+        ref = hb.run_piv(A, B, sched, workspace=ws)
+        _same(r, ref)
+        assert r.sweeps[-1] == ref.sweeps[-1]
+        counts.append(int(ref.sweeps[-1]))
+    assert min(counts) >= 2
+
+
+def test_batch_options_split_classes(hb, ws):
+    # schedules differing in correlation method, peak finder, n_peaks,
+    # validators and uncertainty run as separate job classes of one slot
+    pairs, _ = _mixed(hb, n=4, seed=303)
+    a = [hb.PIVParameters(window_size=32, overlap=16, correlation_method="phase", n_peaks=1),
+         hb.PIVParameters(window_size=16, overlap=8, peak_finder="exclusion", n_peaks=3, uncertainty=True,
+                          validation=(hb.PeakRatioValidator(1.2), hb.VelocityMagnitudeValidator(0.0, 12.0)))]
+    b = [hb.PIVParameters(window_size=32, overlap=16, subpixel_method="gauss9", replace_outliers=False,
+                          max_iterations=2, uncertainty=True)]
+    c = [hb.PIVParameters(window_size=24, overlap=12, padding=True, min_peak_ratio=1.1)]
+    sched = [a, b, c, a]
+    res = hb.run_piv_batch(pairs, sched, workspace=ws)
+    for (A, B), s, r in zip(pairs, sched, res):
+        _same(r, hb.run_piv(A, B, s, workspace=ws))
+
+
+def test_batch_device_inputs(hb, ws):
+    import torch
+
+    pairs, _ = _mixed(hb, n=3, seed=404)
+    s1, s2 = _schedules(hb)
+    dev = [(torch.from_numpy(np.ascontiguousarray(A.T)).cuda().T, torch.from_numpy(np.ascontiguousarray(B.T)).cuda().T)
+           for A, B in pairs]
+    r_dev = hb.run_piv_batch(dev, [s1, s2, s1], workspace=ws)
+    r_host = hb.run_piv_batch(pairs, [s1, s2, s1], workspace=ws)
+    for a, b in zip(r_dev, r_host):
+        _same(a, b)
+
+
+def test_batch_launch_count(hb, ws):
+    # one launch per kernel per slot and sweep for the whole batch: the count
+    # does not grow with the number of pairs
+    from hammerhead_b200 import _lib
+
+    s1, s2 = _schedules(hb)
+    L = _lib.lib()
+    counts = []
+    for n in (2, 6):
+        pairs, _ = _mixed(hb, n=n, seed=500)
+        r = hb.BatchRunner(pairs, [s1 if i % 2 == 0 else s2 for i in range(n)], workspace=ws)
+        r.run()
+        c0 = L.hh_launch_count(ws.ctx)
+        r.run()
+        counts.append(L.hh_launch_count(ws.ctx) - c0)
+        r.close()
+    assert counts[0] == counts[1] and counts[0] < 200

@@ -182,3 +182,42 @@ def test_synthetic_generator(hb):
     r = np.linspace(1, 400, 4000)
     u, v = flow(512.5 + r, 512.5 + 0 * r)
     assert abs(np.hypot(u, v).max() - 8.0) < 1e-3
+
+
+def test_batch_grid_host(hb):
+    """hh_batch_grid: final grids and compact result offsets of a mixed batch,
+    equal to pass_grid of each pair's final pass (host-only, no GPU)."""
+    import ctypes
+
+    from hammerhead_b200 import _lib
+
+    s1 = hb.multipass_parameters([64, 32, 16], padding=True)
+    s2 = hb.multipass_parameters([48, 24], padding=True)
+    shapes = [(512, 512), (768, 1024), (200, 333)]
+    scheds = [s1, s2]
+    pairs = (_lib.hh_batch_pair * 3)()
+    for p, sh in enumerate(shapes):
+        pairs[p] = _lib.hh_batch_pair(1, 1, None, sh[0], sh[1], p % 2, 0)
+    flat = s1 + s2
+    descs = (_lib.hh_pass_desc * len(flat))(*[q.to_desc() for q in flat])
+    so = np.array([0, len(s1), len(s1) + len(s2)], np.int32)
+    ny, nx, off = np.zeros(3, np.int32), np.zeros(3, np.int32), np.zeros(4, np.int64)
+    L = _lib.lib()
+    _lib.check(L.hh_batch_grid(pairs, 3, descs, _lib.i32ptr(so), 2, _lib.i32ptr(ny), _lib.i32ptr(nx),
+                               off.ctypes.data_as(_lib._I64)))
+    tot = 0
+    for p, sh in enumerate(shapes):
+        x, y, _, _ = hb.pass_grid(sh, scheds[p % 2][-1])
+        assert (ny[p], nx[p]) == (len(y), len(x))
+        assert off[p] == tot
+        tot += len(x) * len(y)
+    assert off[3] == tot
+    # argument errors carry messages
+    bad = (_lib.hh_batch_pair * 1)(_lib.hh_batch_pair(1, 1, None, 64, 64, 5, 0))
+    with pytest.raises(hb.ArgumentError, match="schedule index"):
+        _lib.check(L.hh_batch_grid(bad, 1, descs, _lib.i32ptr(so), 2, None, None, None))
+    with pytest.raises(hb.ArgumentError, match="must not be empty"):
+        _lib.check(L.hh_batch_grid(bad, 0, descs, _lib.i32ptr(so), 2, None, None, None))
+    small = (_lib.hh_batch_pair * 1)(_lib.hh_batch_pair(1, 1, None, 40, 40, 0, 0))
+    with pytest.raises(hb.ArgumentError, match="exceeds image size"):
+        _lib.check(L.hh_batch_grid(small, 1, descs, _lib.i32ptr(so), 2, None, None, None))
