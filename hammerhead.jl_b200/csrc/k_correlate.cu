@@ -471,7 +471,9 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
       s_src[3 * tid + 2] = reinterpret_cast<uintptr_t>(M);
       s_ld[tid] = ld;
     }
-    __syncthreads();
+    // a group without a window to analyse (pairs that converged or have no
+    // further sweep, masked cells) is skipped as a whole
+    if (!__syncthreads_or(tid < WPC && s_job[4 * tid] >= 0)) continue;
     // ---- stages 1-3: each window's thread group loads its pixels (coalesced
     //      down the columns), reduces the window means in FP64, and stores
     //      apod * (x - mean) into the plane; masked pixels enter as zero and

@@ -21,6 +21,9 @@ namespace hh {
 struct UQOffsets {
   int8_t dr[40], dc[40];
   int8_t ring_start[5];
+  // ring position of the offset with natural index n: n = dr - 1 for dc = 0
+  // (dr = 1..4), else 4 + 9 (dc - 1) + (dr + 4)
+  int8_t nat2ring[40];
 };
 static UQOffsets make_offsets() {
   UQOffsets o{};
@@ -45,6 +48,11 @@ static UQOffsets make_offsets() {
     }
   }
   o.ring_start[4] = 40;
+  for (int k2 = 0; k2 < 40; ++k2) {
+    const int dr = o.dr[k2], dc = o.dc[k2];
+    const int n = dc == 0 ? dr - 1 : 4 + 9 * (dc - 1) + (dr + 4);
+    o.nat2ring[n] = (int8_t)k2;
+  }
   return o;
 }
 
@@ -229,14 +237,236 @@ __global__ void __launch_bounds__(UQ_THREADS) uq_kernel(const UQArgs a, const UQ
   }
 }
 
+// ---------------------------------------------------------------------------
+// Register form for windows up to 32 px: two warps per window, one per
+// component (u: the window as stored, v: its transpose). Lane c owns column c
+// of the component's W x (W-1) difference field dC for every row in
+// registers, so the smoothing along the columns and the 40 half-plane
+// covariance sums are register FMAs plus one shuffle per neighbour column
+// and row; the per-lane partial sums are combined through shared memory in
+// a fixed order. Same FP32 operations as uq_kernel, FP64 sums.
+constexpr int UQW_WINDOWS = 2;  // windows per CTA
+constexpr int UQW_THREADS = 64 * UQW_WINDOWS;
+
+template <int W> struct UQWCfg {
+  static constexpr int LD = W + 1;  // odd column stride: conflict-free column and row walks
+  static constexpr int M = W - 1;   // columns of dC
+  static constexpr size_t win_bytes = 2 * (size_t)LD * W * sizeof(float) + (size_t)W * W;
+  static constexpr size_t part_bytes = (44 * 33 + 44) * sizeof(double);  // per warp: partials + totals
+  static constexpr size_t smem() { return UQW_WINDOWS * win_bytes + 2 * UQW_WINDOWS * part_bytes + 16; }
+};
+
+template <int W>
+__global__ void __launch_bounds__(UQW_THREADS) uq_warp_kernel(const UQArgs a, const UQOffsets o) {
+  using C = UQWCfg<W>;
+  constexpr int LD = C::LD, M = C::M;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* part_all = reinterpret_cast<double*>(smem_raw);  // [warp][44][33]
+  unsigned char* wbase = smem_raw + 2 * UQW_WINDOWS * C::part_bytes;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int slot = warp >> 1, comp = warp & 1, t64 = tid & 63;
+  float* wa = reinterpret_cast<float*>(wbase + slot * C::win_bytes);  // W x W, column stride LD
+  float* wb = wa + LD * W;
+  uint8_t* mf = reinterpret_cast<uint8_t*>(wb + LD * W);
+  double* part = part_all + warp * (44 * 33 + 44);
+  for (int64_t base = (int64_t)blockIdx.x * UQW_WINDOWS; base < a.njobs; base += (int64_t)gridDim.x * UQW_WINDOWS) {
+    const int64_t job = base + slot;
+    // ---- the window's source (uniform within the warp pair)
+    bool on = job < a.njobs;
+    const float* A = a.A;
+    const float* B = a.B;
+    const uint8_t* Mk = a.mask;
+    int64_t ld = a.ld, gid = -1;
+    int rs = 0, cs = 0;
+    if (on) {
+      rs = a.jobs[4 * job + 2];
+      cs = a.jobs[4 * job + 3];
+      if (a.bp) {
+        const int p = a.jobs[4 * job];
+        const BPair& b = a.bp[p];
+        const int gij = a.jobs[4 * job + 1];
+        const int64_t cell = (int64_t)(gij & 0xFFFF) + (int64_t)(gij >> 16) * b.ny;
+        on = a.mode == 0 ? (b.unc_fused && bp_live(b, 1, a.done, p)) : (b.unc_post && b.live);
+        on = on && !(b.gmask && b.gmask[cell]);
+        const bool warped = a.mode == 1 || b.has_pred0;
+        A = warped ? b.warpA : b.A;
+        B = warped ? b.warpB : b.B;
+        Mk = b.mask;
+        ld = b.nr;
+        gid = b.goff + cell;
+      } else {
+        gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
+      }
+    }
+    // ---- raw windows into shared memory (both warps of the window)
+    if (on)
+      for (int k = t64; k < W * W; k += 64) {
+        const int p = k % W, q = k / W;
+        const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * ld;
+        wa[p + q * LD] = __ldg(A + off);
+        wb[p + q * LD] = __ldg(B + off);
+        mf[k] = Mk ? __ldg(Mk + off) : 0;
+      }
+    __syncthreads();
+    // ---- window means (load_uncertainty_windows!), FP64, computed by each warp
+    float ma = 0.f, mb = 0.f;
+    if (on) {
+      double sa = 0.0, sb = 0.0, cnt = 0.0;
+      for (int k = lane; k < W * W; k += 32)
+        if (!mf[k]) {
+          const int p = k % W, q = k / W;
+          sa += (double)wa[p + q * LD];
+          sb += (double)wb[p + q * LD];
+          cnt += 1.0;
+        }
+      sa = warp_sum(sa);
+      sb = warp_sum(sb);
+      cnt = warp_sum(cnt);
+      ma = cnt > 0 ? (float)(sa / cnt) : 0.f;
+      mb = cnt > 0 ? (float)(sb / cnt) : 0.f;
+    }
+    __syncthreads();  // every read of the raw values precedes the apodized writes
+    if (on)
+      for (int k = t64; k < W * W; k += 64) {
+        const int p = k % W, q = k / W;
+        const float ap = __ldg(a.apod + k);
+        const float va = wa[p + q * LD], vb = wb[p + q * LD];
+        wa[p + q * LD] = mf[k] ? 0.f : __fmul_rn(ap, __fsub_rn(va, ma));
+        wb[p + q * LD] = mf[k] ? 0.f : __fmul_rn(ap, __fsub_rn(vb, mb));
+      }
+    __syncthreads();
+    if (on) {
+      // ---- this component's dC column (lane c < M), and the C0 / C+ / C- sums
+      const int c = lane;
+      const bool col = c < M;
+      const int cc = col ? c : 0;
+      float dcol[W];
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+      for (int r = 0; r < W; ++r) {
+        // u: element (p, q) = (r, c); v: (p, q) = (c, r)
+        const int i0 = comp == 0 ? r + cc * LD : cc + r * LD;
+        const int i1 = comp == 0 ? r + (cc + 1) * LD : (cc + 1) + r * LD;
+        const float a0 = wa[i0], a1 = wa[i1], b0 = wb[i0], b1 = wb[i1];
+        dcol[r] = __fsub_rn(__fmul_rn(a0, b1), __fmul_rn(a1, b0));
+        if (col) {
+          s0 += (double)__fmul_rn(a0, b0);
+          s1 += (double)__fmul_rn(a0, b1);
+          s2 += (double)__fmul_rn(a1, b0);
+        }
+      }
+      // ---- (1,2,1)/4 smoothing along the columns, and its mean
+      double dd[W];
+      double msum = 0.0;
+#pragma unroll
+      for (int r = 0; r < W; ++r) {
+        const float left = __shfl_up_sync(0xffffffffu, dcol[r], 1);
+        const float right = __shfl_down_sync(0xffffffffu, dcol[r], 1);
+        const float l = c > 0 ? left : dcol[r];
+        const float rr = c < M - 1 ? right : dcol[r];
+        const float v = __fmul_rn(0.25f, __fadd_rn(__fadd_rn(l, __fmul_rn(2.0f, dcol[r])), rr));
+        dd[r] = (double)v;
+        if (col) msum += dd[r];
+      }
+      const double mu = warp_sum(msum) / (double)(W * M);
+#pragma unroll
+      for (int r = 0; r < W; ++r) dd[r] = col ? dd[r] - mu : 0.0;
+      // ---- S00 and the covariance sums: acc[dc][dr + 4] pairs (r, c) with (r + dr, c + dc)
+      double sq = 0.0;
+      double acc0[4];
+      double acc[4][9];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) acc0[i] = 0.0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 9; ++j) acc[i][j] = 0.0;
+#pragma unroll
+      for (int r = 0; r < W; ++r) {
+        sq = fma(dd[r], dd[r], sq);
+#pragma unroll
+        for (int dr = 1; dr <= 4; ++dr)
+          if (r + dr < W) acc0[dr - 1] = fma(dd[r], dd[r + dr], acc0[dr - 1]);
+      }
+#pragma unroll
+      for (int dc = 1; dc <= 4; ++dc) {
+        const bool ok = c + dc < M;
+#pragma unroll
+        for (int r2 = 0; r2 < W; ++r2) {
+          double x = __shfl_down_sync(0xffffffffu, dd[r2], dc);
+          x = ok ? x : 0.0;
+#pragma unroll
+          for (int dr = -4; dr <= 4; ++dr) {
+            const int r0 = r2 - dr;
+            if (r0 >= 0 && r0 < W) acc[dc - 1][dr + 4] = fma(dd[r0], x, acc[dc - 1][dr + 4]);
+          }
+        }
+      }
+      // ---- per-lane partials -> shared [stat][lane] in natural order, summed
+      //      in lane order into the totals in ring order
+      part[0 * 33 + lane] = s0;
+      part[1 * 33 + lane] = s1;
+      part[2 * 33 + lane] = s2;
+      part[3 * 33 + lane] = sq;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) part[(4 + i) * 33 + lane] = acc0[i];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 9; ++j) part[(8 + 9 * i + j) * 33 + lane] = acc[i][j];
+      __syncwarp();
+      double* tot = part + 44 * 33;
+      for (int st = lane; st < 44; st += 32) {
+        double t = 0.0;
+        for (int l = 0; l < 32; ++l) t += part[st * 33 + l];
+        const int ri = st < 4 ? st : 4 + o.nat2ring[st - 4];
+        tot[ri] = t;
+        if (a.stats) a.stats[job * 88 + comp * 44 + ri] = t;
+      }
+      __syncwarp();
+      if (lane == 0 && a.unc_u) (comp == 0 ? a.unc_u : a.unc_v)[gid] = uq_finalize(tot, o);
+    }
+    __syncthreads();  // the window buffers are reused by the next iteration
+  }
+}
+
+template <int W> static cudaError_t launch_uq_warp(const UQArgs& a, cudaStream_t s, int num_sms, const UQOffsets& offs) {
+  using C = UQWCfg<W>;
+  const size_t sm = C::smem();
+  cudaError_t e = cudaFuncSetAttribute(uq_warp_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, uq_warp_kernel<W>, UQW_THREADS, sm);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  int64_t grid = (int64_t)per_sm * num_sms;
+  const int64_t units = (a.njobs + UQW_WINDOWS - 1) / UQW_WINDOWS;
+  if (grid > units) grid = units;
+  uq_warp_kernel<W><<<(unsigned)grid, UQW_THREADS, sm, s>>>(a, offs);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_uq(const UQArgs& a, cudaStream_t s, int num_sms) {
   if (a.njobs <= 0) return cudaSuccess;
   static const UQOffsets offs = make_offsets();
-  const int W = a.W, WM = W * (W - 1);
-  const size_t sm = (size_t)(2 * WM + 88 + 12) * sizeof(double) + (size_t)(2 * W * W + 4 * WM) * sizeof(float) +
-                    (size_t)W * W + 16;
-  if (sm > 220 * 1024) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(uq_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  switch (a.W) {
+    case 8: return launch_uq_warp<8>(a, s, num_sms, offs);
+    case 12: return launch_uq_warp<12>(a, s, num_sms, offs);
+    case 16: return launch_uq_warp<16>(a, s, num_sms, offs);
+    case 24: return launch_uq_warp<24>(a, s, num_sms, offs);
+    case 32: return launch_uq_warp<32>(a, s, num_sms, offs);
+    default: break;
+  }
+  auto smem_of = [](int W) {
+    const int WM = W * (W - 1);
+    return (size_t)(2 * WM + 88 + 12) * sizeof(double) + (size_t)(2 * W * W + 4 * WM) * sizeof(float) +
+           (size_t)W * W + 16;
+  };
+  const size_t sm = smem_of(a.W);
+  if (a.W > 64 || sm > 220 * 1024) return cudaErrorInvalidValue;
+  // one attribute for every window size this kernel serves: the limit is a
+  // property of the function, and launches of different sizes may share a graph
+  cudaError_t e = cudaFuncSetAttribute(uq_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_of(64));
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, uq_kernel, UQ_THREADS, sm);

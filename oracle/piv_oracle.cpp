@@ -1080,6 +1080,142 @@ static void deform_columns(const T* CA, const T* CB, i64 nr, i64 nc, const T* pu
     }
 }
 
+// ---------------------------------------------------------------------------
+// Differentiable correlation loss (no counterpart in the reference; the
+// deformation it differentiates is deform_columns! above):
+//   L(P) = - sum over windows j of NCC0_j,
+//   NCC0_j = sum (a - abar)(b - bbar) / sqrt(sum (a - abar)^2 sum (b - bbar)^2)
+// over the W x W pixels of window j of the pair deformed by the predictor
+// P = (u, v) on a uniform node grid (bilinear, flat outside). Its gradient
+// follows the chain: dL/da_i, dL/db_i of the normalised correlation; the
+// sampling derivatives of the cubic B-spline at -+ (u, v)/2; the transpose of
+// the bilinear predictor interpolation.
+
+// derivative of the cubic B-spline weights with respect to the offset d
+template <class T> static inline void cubw_d(T d, T* w) {
+  T c = T(1) - d;
+  w[0] = -c * c / T(2);
+  w[1] = -T(2) * d + T(3) * d * d / T(2);
+  w[2] = T(2) * c - T(3) * c * c / T(2);
+  w[3] = d * d / T(2);
+}
+
+// value and gradient (d/dy, d/dx) of the zero-extrapolated B-spline sample
+template <class T> static T bspline_eval_grad(const T* C, i64 nr, i64 nc, T yy, T xx, T& gy, T& gx) {
+  gy = gx = T(0);
+  if (yy < 1 || yy > (T)nr || xx < 1 || xx > (T)nc) return T(0);
+  i64 iy = (i64)std::floor(yy);
+  if (iy > nr - 1) iy = nr - 1;
+  i64 ix = (i64)std::floor(xx);
+  if (ix > nc - 1) ix = nc - 1;
+  T wy[4], wx[4], dy[4], dx[4];
+  cubw(yy - (T)iy, wy);
+  cubw(xx - (T)ix, wx);
+  cubw_d(yy - (T)iy, dy);
+  cubw_d(xx - (T)ix, dx);
+  const i64 ld = nr + 2;
+  T s = 0, sy = 0, sx = 0;
+  for (int a = 0; a < 4; ++a) {
+    T t = 0, tx = 0;
+    for (int b = 0; b < 4; ++b) {
+      const T c = C[(iy - 1 + a) + (ix - 1 + b) * ld];
+      t += wx[b] * c;
+      tx += dx[b] * c;
+    }
+    s += wy[a] * t;
+    sy += dy[a] * t;
+    sx += wy[a] * tx;
+  }
+  gy = sy;
+  gx = sx;
+  return s;
+}
+
+// bilinear weights of the four nodes a query touches (flat outside)
+template <class T> struct BilinW {
+  int iy, ix, iy2, ix2;
+  T w00, w01, w10, w11;
+};
+template <class T>
+static BilinW<T> bilinear_w(int gny, int gnx, T y0, T ysp, T x0, T xsp, T qy, T qx) {
+  BilinW<T> b;
+  T dy, dx;
+  lin_axis(qy, y0, ysp, gny, b.iy, dy);
+  lin_axis(qx, x0, xsp, gnx, b.ix, dx);
+  b.iy2 = gny == 1 ? b.iy : b.iy + 1;
+  b.ix2 = gnx == 1 ? b.ix : b.ix + 1;
+  b.w00 = (T(1) - dy) * (T(1) - dx);
+  b.w01 = (T(1) - dy) * dx;
+  b.w10 = dy * (T(1) - dx);
+  b.w11 = dy * dx;
+  return b;
+}
+
+// Loss over the windows with 0-based origins wins[2j], wins[2j+1]; the
+// gradient (2 planes of gny x gnx: u then v) is accumulated when grad != 0.
+template <class T>
+static double ncc_loss_grad(const T* CA, const T* CB, i64 nr, i64 nc, const T* P, int gny, int gnx, T y0, T ysp, T x0,
+                            T xsp, int W, const int32_t* wins, i64 nwin, T* grad) {
+  const i64 G = (i64)gny * gnx;
+  const T* pu = P;
+  const T* pv = P + G;
+  const int n = W * W;
+  std::vector<T> a(n), b(n), ay(n), ax(n), by(n), bx(n);
+  std::vector<BilinW<T>> bw(n);
+  double L = 0;
+  for (i64 j = 0; j < nwin; ++j) {
+    const i64 rs = wins[2 * j], cs = wins[2 * j + 1];
+    for (int q = 0; q < W; ++q)
+      for (int p = 0; p < W; ++p) {
+        const int k = p + q * W;
+        const T R = (T)(rs + p + 1), Cc = (T)(cs + q + 1);
+        const T u2 = bilinear(pu, gny, gnx, y0, ysp, x0, xsp, R, Cc) / T(2);
+        const T v2 = bilinear(pv, gny, gnx, y0, ysp, x0, xsp, R, Cc) / T(2);
+        a[k] = bspline_eval_grad(CA, nr, nc, R - v2, Cc - u2, ay[k], ax[k]);
+        b[k] = bspline_eval_grad(CB, nr, nc, R + v2, Cc + u2, by[k], bx[k]);
+        bw[k] = bilinear_w(gny, gnx, y0, ysp, x0, xsp, R, Cc);
+      }
+    T ma = 0, mb = 0;
+    for (int k = 0; k < n; ++k) {
+      ma += a[k];
+      mb += b[k];
+    }
+    ma /= (T)n;
+    mb /= (T)n;
+    T saa = 0, sbb = 0, sab = 0;
+    for (int k = 0; k < n; ++k) {
+      const T da = a[k] - ma, db = b[k] - mb;
+      saa += da * da;
+      sbb += db * db;
+      sab += da * db;
+    }
+    if (!(saa > 0 && sbb > 0)) continue;  // a flat window contributes nothing
+    const T inv = T(1) / std::sqrt(saa * sbb), ncc = sab * inv;
+    L -= (double)ncc;
+    if (!grad) continue;
+    const T ca = ncc / saa, cb = ncc / sbb;
+    for (int k = 0; k < n; ++k) {
+      const T da = a[k] - ma, db = b[k] - mb;
+      const T ga = -db * inv + ca * da;  // dL/da_k
+      const T gb = -da * inv + cb * db;  // dL/db_k
+      const T gu = ga * (-ax[k] / T(2)) + gb * (bx[k] / T(2));
+      const T gv = ga * (-ay[k] / T(2)) + gb * (by[k] / T(2));
+      const BilinW<T>& w = bw[k];
+      T* gu_ = grad;
+      T* gv_ = grad + G;
+      gu_[w.iy + (i64)w.ix * gny] += w.w00 * gu;
+      gu_[w.iy + (i64)w.ix2 * gny] += w.w01 * gu;
+      gu_[w.iy2 + (i64)w.ix * gny] += w.w10 * gu;
+      gu_[w.iy2 + (i64)w.ix2 * gny] += w.w11 * gu;
+      gv_[w.iy + (i64)w.ix * gny] += w.w00 * gv;
+      gv_[w.iy + (i64)w.ix2 * gny] += w.w01 * gv;
+      gv_[w.iy2 + (i64)w.ix * gny] += w.w10 * gv;
+      gv_[w.iy2 + (i64)w.ix2 * gny] += w.w11 * gv;
+    }
+  }
+  return L;
+}
+
 template <class F> static void parallel_for(int nthreads, i64 n, F f) {
   nthreads = (int)std::max<i64>(1, std::min<i64>(nthreads, n));
   if (nthreads == 1) { f(0, (i64)0, n); return; }
@@ -1606,6 +1742,37 @@ int orc_pass_grid(int64_t nr, int64_t nc, const orc::Pass* p, const uint8_t* mas
 
 ORC_DEFINE(float, f32)
 ORC_DEFINE(double, f64)
+
+// NCC loss (and gradient when grad != NULL, zeroed here) over the given
+// windows of a prefiltered pair; threads split the windows, each thread
+// accumulating its own gradient, summed in thread order.
+#define ORC_NCC(T, SUF)                                                                                              \
+  double orc_ncc_loss_grad_##SUF(const T* CA, const T* CB, int64_t nr, int64_t nc, const T* P, int gny, int gnx,    \
+                                 double y0, double ysp, double x0, double xsp, int W, const int32_t* wins,          \
+                                 int64_t nwin, T* grad, int nthreads) {                                              \
+    const int64_t G2 = 2 * (int64_t)gny * gnx;                                                                       \
+    nthreads = (int)std::max<int64_t>(1, std::min<int64_t>(nthreads, nwin));                                        \
+    std::vector<double> Ls(nthreads, 0.0);                                                                           \
+    std::vector<std::vector<T>> gs(grad ? nthreads : 0, std::vector<T>(grad ? G2 : 0, T(0)));                        \
+    std::vector<std::thread> th;                                                                                     \
+    for (int t = 0; t < nthreads; ++t)                                                                               \
+      th.emplace_back([&, t]() {                                                                                     \
+        const int64_t j0 = nwin * t / nthreads, j1 = nwin * (t + 1) / nthreads;                                      \
+        Ls[t] = orc::ncc_loss_grad<T>(CA, CB, nr, nc, P, gny, gnx, (T)y0, (T)ysp, (T)x0, (T)xsp, W, wins + 2 * j0,  \
+                                      j1 - j0, grad ? gs[t].data() : nullptr);                                       \
+      });                                                                                                            \
+    for (auto& x : th) x.join();                                                                                     \
+    double L = 0;                                                                                                    \
+    for (int t = 0; t < nthreads; ++t) L += Ls[t];                                                                   \
+    if (grad) {                                                                                                      \
+      std::fill(grad, grad + G2, T(0));                                                                              \
+      for (int t = 0; t < nthreads; ++t)                                                                             \
+        for (int64_t k = 0; k < G2; ++k) grad[k] += gs[t][k];                                                        \
+    }                                                                                                                \
+    return L;                                                                                                        \
+  }
+ORC_NCC(float, f32)
+ORC_NCC(double, f64)
 
 void orc_uq_offsets(int32_t* out /*40x2*/, int32_t* ring_start /*5*/) {
   orc::uq_init();
