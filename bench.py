@@ -199,6 +199,26 @@ def cpu_baseline(hb, pairs, budget_s=20.0):
             "sample": f"{runs}x [{desc}] (oracle, float32, {threads} threads)"}
 
 
+def adjoint_bench(hb, ws, torch, stream, dev_time, reps):
+    """ms per pass of the correlation-loss adjoint on the differentiation case:
+    the 1024 x 1024 vortex pair, P on the 127 x 127 grid of 16-px windows at
+    50 % overlap (truth + N(0, 0.3 px)); one pass = loss and dL/dP over the
+    whole field, predictor and gradient resident on the device."""
+    A, B, _, P, grid = hb.synthetic.config2_case()
+    loss = hb.NCCLoss(A, B, window=16, overlap=8, workspace=ws)
+    gny, gnx = P.shape[:2]
+    Pd = torch.from_numpy(hb.adjoint.to_planes(P)).cuda()
+    gd = torch.empty_like(Pd)
+    for _ in range(3):
+        loss.device_value_and_grad(Pd, gny, gnx, grid, gd)
+    ms = dev_time(lambda: loss.device_value_and_grad(Pd, gny, gnx, grid, gd), reps)
+    ms_loss = dev_time(lambda: loss.device_value_and_grad(Pd, gny, gnx, grid, None), reps)
+    return {"ms_per_pass": ms, "loss_only_ms": ms_loss, "unit": "ms",
+            "config": "1024x1024 Lamb-Oseen pair, P 127x127x2 (truth + N(0, 0.3 px)), "
+                      "L = -sum NCC0 over 16x16 windows at 50% overlap, loss + dL/dP per pass",
+            "windows": int(((A.shape[0] - 16) // 8 + 1) * ((A.shape[1] - 16) // 8 + 1))}
+
+
 # ---------------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
@@ -326,6 +346,9 @@ def main():
     e2e_ms = max_over_ranks(dev_time(e2e_step, max(1, min(args.steps, 3))))
     e2e_value = nvec_total / (e2e_ms / 1e3)
 
+    # ---- differentiation: loss + adjoint gradient over the full predictor field
+    adj = adjoint_bench(hb, ws, torch, stream, dev_time, max(args.steps, 5))
+
     # ---- roofline of the dominant kernel (the fused correlation)
     c = prof["correlate"]
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
@@ -371,6 +394,7 @@ def main():
             "deform_roofline": {"bound": "hbm", "achieved": (d["bytes"] / (d["ms"] / 1e3) / 1e9) if d["ms"] else None,
                                 "peak": hbm_peak, "unit": "GB/s"},
             "kernel_share": shares,
+            "adjoint": adj,
             "clocks": clk.summary(sm_max),
             "cpu_baseline": base,
         }

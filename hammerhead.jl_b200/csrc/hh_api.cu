@@ -502,6 +502,67 @@ hh_status hh_stage_pair(hh_ctx* ctx, const float* A, const float* B, int64_t nr,
   return HH_OK;
 }
 
+hh_status hh_ncc_loss_grad(hh_ctx* ctx, const float* P, int32_t gny, int32_t gnx, float y0, float ysp, float x0,
+                           float xsp, int32_t window, int32_t overlap, int32_t device_ptrs, double* loss,
+                           float* dLdP) {
+  if (!ctx) return fail(nullptr, HH_ERR_ARG, "context is NULL");
+  HH_TRY(set_device(ctx));
+  if (!ctx->staged) return fail(ctx, HH_ERR_STATE, "no staged pair: call hh_stage_pair first");
+  if (!P || !loss) return fail(ctx, HH_ERR_ARG, "predictor and loss pointers must not be NULL");
+  if (gny < 1 || gnx < 1) return fail(ctx, HH_ERR_ARG, "predictor grid must be non-empty");
+  if (!(ysp > 0) || !(xsp > 0)) return fail(ctx, HH_ERR_ARG, "predictor node spacing must be positive");
+  if (window < 2 || window > 64) return fail(ctx, HH_ERR_UNSUPPORTED, "loss windows must be 2..64 px");
+  if (overlap < 0 || overlap >= window)
+    return fail(ctx, HH_ERR_ARG, "overlap must satisfy 0 \xe2\x89\xa4 overlap < window_size");
+  if (window > ctx->nr || window > ctx->nc) return fail(ctx, HH_ERR_ARG, "window exceeds the image size");
+  cudaStream_t s = ctx->stream;
+  const int64_t G2 = 2 * (int64_t)gny * gnx, Px = ctx->nr * ctx->nc;
+  hh::NccArgs a{};
+  a.CA = (const float*)ctx->bufs["coefA"].p;
+  a.CB = (const float*)ctx->bufs["coefB"].p;
+  a.nr = ctx->nr;
+  a.nc = ctx->nc;
+  a.gny = gny;
+  a.gnx = gnx;
+  a.y0 = y0;
+  a.ysp = ysp;
+  a.x0 = x0;
+  a.xsp = xsp;
+  a.W = window;
+  a.step = window - overlap;
+  a.wy = (int32_t)((ctx->nr - window) / a.step + 1);
+  a.wx = (int32_t)((ctx->nc - window) / a.step + 1);
+  float* dP = nullptr;
+  if (device_ptrs) {
+    a.P = P;
+  } else {
+    HH_TRY(buf(ctx, "ncc_P", (size_t)G2, &dP));
+    HH_CK(cudaMemcpyAsync(dP, P, G2 * sizeof(float), cudaMemcpyHostToDevice, s));
+    a.P = dP;
+  }
+  HH_TRY(buf(ctx, "ncc_wstat", (size_t)6 * a.wy * a.wx, &a.wstat));
+  HH_TRY(buf(ctx, "ncc_loss", 1, &a.loss));
+  float* dG = nullptr;
+  if (dLdP) {
+    HH_TRY(buf(ctx, "ncc_gpix", (size_t)2 * Px, &a.gpix));
+    if (device_ptrs) {
+      a.grad = dLdP;
+    } else {
+      HH_TRY(buf(ctx, "ncc_grad", (size_t)G2, &dG));
+      a.grad = dG;
+    }
+  }
+  const double nwin = (double)a.wy * a.wx;
+  HH_K(HH_K_DEFORM, dLdP ? 4 : 2, nwin * window * window * 80.0 + (dLdP ? Px * 240.0 : 0.0), 16.0 * Px,
+       (int64_t)nwin, hh::launch_ncc_loss_grad(a, s));
+  if (dLdP && !device_ptrs) HH_CK(cudaMemcpyAsync(dLdP, dG, G2 * sizeof(float), cudaMemcpyDeviceToHost, s));
+  double* hl = reinterpret_cast<double*>(ctx->pinned);
+  HH_CK(cudaMemcpyAsync(hl, a.loss, sizeof(double), cudaMemcpyDeviceToHost, s));
+  HH_CK(cudaStreamSynchronize(s));
+  *loss = *hl;
+  return flush_profile(ctx);
+}
+
 hh_status hh_apply_predictor(hh_ctx* ctx, const float* pu, const float* pv, int32_t gny, int32_t gnx, float y0,
                              float ysp, float x0, float xsp, const float* y, int32_t ny, const float* x, int32_t nx,
                              float* node_u, float* node_v, float* warpA_out, float* warpB_out) {

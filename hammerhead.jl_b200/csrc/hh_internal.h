@@ -120,4 +120,21 @@ struct UQArgs {
 };
 cudaError_t launch_uq(const UQArgs& a, cudaStream_t s, int num_sms);
 
+// --- adjoint of deformation + zero-lag correlation --------------------------
+struct NccArgs {
+  const float* CA;  // B-spline coefficients of both frames, (nr + 2) x (nc + 2)
+  const float* CB;
+  int64_t nr, nc;
+  const float* P;   // predictor: u plane then v plane, gny x gnx each
+  int32_t gny, gnx;
+  float y0, ysp, x0, xsp;
+  int32_t W, step;  // windows: W x W at origins (jr * step, jc * step)
+  int32_t wy, wx;   // window grid
+  double* wstat;    // 6 per window (scratch)
+  float* gpix;      // 2 x nr x nc pixel gradient (scratch), when grad
+  float* grad;      // 2 x gny x gnx dL/dP, or nullptr (loss only)
+  double* loss;     // device scalar
+};
+cudaError_t launch_ncc_loss_grad(const NccArgs& a, cudaStream_t s);
+
 }  // namespace hh

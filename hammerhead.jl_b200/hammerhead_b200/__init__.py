@@ -7,6 +7,7 @@ with the reference's public surface for the path:
     run_piv, piv_workspace, PIVWorkspace, PIVResult         (src/pipeline.jl, src/types.jl)
     run_piv_sequence (in-memory pairs), run_piv_batch,
     BatchRunner                                             (src/io.jl; batched device schedule)
+    NCCLoss                                                 (adjoint of deformation + correlation)
     validators: PeakRatioValidator, CorrelationMomentValidator,
                 VelocityMagnitudeValidator, UniversalOutlierValidator
     error_statistics                                        (src/statistics.jl)
@@ -19,6 +20,8 @@ from .params import (CorrelationMomentValidator, PeakRatioValidator, PIVParamete
                      VelocityMagnitudeValidator, effort_schedule, multipass_parameters, parse_validator)
 from .pipeline import (PhysicalScale, PIVResult, PIVWorkspace, check_backend_params, pass_grid, piv_workspace, run_piv,
                        with_scale)
+from . import adjoint
+from .adjoint import NCCLoss
 from .batch import BatchRunner, run_piv_batch, run_piv_sequence
 from .statistics import error_statistics, rms_error
 from . import synthetic
@@ -28,5 +31,5 @@ __all__ = [
     "effort_schedule", "parse_validator", "PeakRatioValidator", "CorrelationMomentValidator",
     "VelocityMagnitudeValidator", "UniversalOutlierValidator", "PIVResult", "PIVWorkspace", "PhysicalScale",
     "piv_workspace", "run_piv", "pass_grid", "check_backend_params", "with_scale", "error_statistics", "rms_error",
-    "synthetic", "BatchRunner", "run_piv_batch", "run_piv_sequence",
+    "synthetic", "BatchRunner", "run_piv_batch", "run_piv_sequence", "NCCLoss", "adjoint",
 ]

@@ -166,6 +166,10 @@ SIGNATURES = [
     ("hh_smooth_field", ctypes.c_int32, [_CTX, _F, ctypes.c_int32, ctypes.c_int32, _F]),
     ("hh_field_change", ctypes.c_int32, [_CTX, _F, _F, _F, _F, _U8, ctypes.c_int64, _F]),
     ("hh_finalize_uncertainty", ctypes.c_int32, [_D, ctypes.c_int64, _F, _F]),
+    ("hh_ncc_loss_grad", ctypes.c_int32,
+     [_CTX, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+      ctypes.c_float, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
+      ctypes.c_void_p]),
     ("hh_set_profiling", ctypes.c_int32, [_CTX, ctypes.c_int32]),
     ("hh_profile_read", ctypes.c_int32, [_CTX, ctypes.POINTER(hh_kernel_profile), ctypes.c_int32]),
     ("hh_launch_count", ctypes.c_int64, [_CTX]),

@@ -139,6 +139,22 @@ def config1_pair(seed=1001):
     return A, B, flow
 
 
+def config2_case(seed=1001, noise=0.3, window=16, overlap=8):
+    """The differentiation case: the 1024 x 1024 vortex pair and a predictor
+    P (gny, gnx, 2) = the true field on the window-centre grid of 16-px
+    windows at 50 % overlap (127 x 127 nodes) plus N(0, noise) px.
+    Returns A, B, flow, P, grid = (y0, ysp, x0, xsp)."""
+    A, B, flow = config1_pair(seed)
+    step = window - overlap
+    nodes = lambda n: (1 + np.arange((n - window) // step + 1) * step) + (window - 1) / 2.0
+    y, x = nodes(A.shape[0]), nodes(A.shape[1])
+    X, Y = np.meshgrid(x, y)
+    u, v = flow(X, Y)
+    rng = np.random.default_rng(seed + 7)
+    P = np.stack([u, v], axis=-1) + rng.normal(0.0, noise, (len(y), len(x), 2))
+    return A, B, flow, P.astype(np.float32), (float(y[0]), float(step), float(x[0]), float(step))
+
+
 def config3_pairs(n512=24, n768=24, n2048=16, seed0=1003):
     """The mixed batch: (shape, flow, schedule kind) per pair, drawn from the
     pair seed: sinusoidal shear (A ~ U[1,6], lambda ~ U[128,512]) or a uniform

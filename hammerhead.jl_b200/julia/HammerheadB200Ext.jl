@@ -8,6 +8,7 @@
 module HammerheadB200Ext
 
 using Hammerhead
+using ChainRulesCore: ChainRulesCore, NoTangent, unthunk
 import Hammerhead: _AbstractHammerheadBackend, _resolve_backend, _check_backend_params, _engine_nchunks,
     _supports_fft, _supports_batched_fft, _supports_fp64, PIVParameters, PIVResult, run_piv
 
@@ -151,6 +152,48 @@ function run_piv_b200(imgA::AbstractMatrix{<:Real}, imgB::AbstractMatrix{<:Real}
                     ctx.ptr, A, B, nr, nc, d, length(d), M, mask_threshold, predictor_smoothing, res), ctx.ptr)
     end
     return PIVResult(x, y, u, v, ratio, moment, su, sv, BitMatrix(outl .!= 0), BitMatrix(gm .!= 0), final)
+end
+
+# ---- differentiable correlation loss (hh_ncc_loss_grad) -------------------
+# A staged pair on a context; P is (gny, gnx, 2) Float32 (u, v) on nodes
+# y0 .+ ysp .* (0:gny-1), x0 .+ xsp .* (0:gnx-1).
+struct StagedPair
+    ctx::Context
+    window::Int
+    overlap::Int
+end
+
+function StagedPair(imgA::AbstractMatrix{<:Real}, imgB::AbstractMatrix{<:Real};
+                    window::Integer = 16, overlap::Integer = 8, ctx::Context = Context())
+    A = Matrix{Float32}(imgA)
+    B = Matrix{Float32}(imgB)
+    size(A) == size(B) || throw(DimensionMismatch("images must have the same size"))
+    check(ccall((:hh_stage_pair, LIB), Int32, (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Int64, Int64),
+                ctx.ptr, A, B, size(A, 1), size(A, 2)), ctx.ptr)
+    return StagedPair(ctx, window, overlap)
+end
+
+function _ncc(sp::StagedPair, P::AbstractArray{<:Real,3}, grid::NTuple{4,Real}, want_grad::Bool)
+    gny, gnx = size(P, 1), size(P, 2)
+    Pf = vcat(vec(Float32.(P[:, :, 1])), vec(Float32.(P[:, :, 2])))  # u then v, column-major planes
+    G = want_grad ? similar(Pf) : Float32[]
+    L = Ref{Float64}(0)
+    check(ccall((:hh_ncc_loss_grad, LIB), Int32,
+                (Ptr{Cvoid}, Ptr{Float32}, Int32, Int32, Float32, Float32, Float32, Float32, Int32, Int32, Int32,
+                 Ref{Float64}, Ptr{Float32}),
+                sp.ctx.ptr, Pf, gny, gnx, grid..., sp.window, sp.overlap, 0, L,
+                want_grad ? pointer(G) : Ptr{Float32}(C_NULL)), sp.ctx.ptr)
+    return L[], want_grad ? reshape(G, gny, gnx, 2) : nothing
+end
+
+"L = -sum of zero-lag NCC over the loss windows of the pair deformed by P."
+ncc_loss(sp::StagedPair, P::AbstractArray{<:Real,3}, grid::NTuple{4,Real}) = first(_ncc(sp, P, grid, false))
+
+# The rrule: the adjoint gradient comes from the device in the same call as the loss.
+function ChainRulesCore.rrule(::typeof(ncc_loss), sp::StagedPair, P::AbstractArray{<:Real,3}, grid::NTuple{4,Real})
+    L, G = _ncc(sp, P, grid, true)
+    pullback(dL) = (NoTangent(), NoTangent(), unthunk(dL) .* G, NoTangent())
+    return L, pullback
 end
 
 end # module

@@ -186,6 +186,27 @@ hh_status hh_run_batched(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npairs
                          const int32_t* schedule_offsets, int32_t nschedules, double mask_threshold,
                          int32_t predictor_smoothing, int32_t flags, hh_batch_result* out);
 
+/* ---- Differentiation: adjoint of deformation + correlation -------------
+ *
+ * No counterpart in the reference: a correlation loss of the predictor
+ * field, for gradient-based refinement of the field, built on the same
+ * symmetric deformation as a WIDIM sweep (deform_columns!,
+ * src/pipeline.jl:957-965; bilinear predictor with flat extrapolation,
+ * src/pipeline.jl:561-569):
+ *   L(P) = - sum over windows j of NCC0_j,
+ *   NCC0_j = sum (a - abar)(b - bbar) / sqrt(sum (a - abar)^2 sum (b - bbar)^2)
+ * over W x W windows at origins (jr*(W - overlap), jc*(W - overlap)) (the
+ * pass_grid rows and columns of a pass with that window and overlap) of the
+ * staged pair (hh_stage_pair) deformed by P. P holds u (gny x gnx,
+ * column-major) followed by v on nodes y0 + i*ysp, x0 + j*xsp. Returns L in
+ * *loss and, when dLdP != NULL, dL/dP in the layout of P. The deformed
+ * windows are recomputed, not stored. With device_ptrs, P and dLdP are
+ * device pointers and the call is stream-ordered on the context stream up
+ * to the final loss read. */
+hh_status hh_ncc_loss_grad(hh_ctx* ctx, const float* P, int32_t gny, int32_t gnx, float y0, float ysp, float x0,
+                           float xsp, int32_t window, int32_t overlap, int32_t device_ptrs, double* loss,
+                           float* dLdP);
+
 /* Per-pass timing of the last hh_run_piv* call on ctx, measured with CUDA
  * events on the context stream: ms[k] = device time of pass k (all sweeps,
  * deformation, validation, uncertainty); sweeps[k] = sweeps run. */

@@ -362,3 +362,42 @@ def uq_offsets():
     rs = np.empty(5, np.int32)
     lib().orc_uq_offsets(_i32(out), _i32(rs))
     return out.reshape(40, 2), rs
+
+
+def ncc_windows(shape, window, overlap):
+    """0-based origins (2 x n, column-major window order) of the loss windows."""
+    nr, nc = shape
+    step = window - overlap
+    wy = (nr - window) // step + 1
+    wx = (nc - window) // step + 1
+    jr, jc = np.meshgrid(np.arange(wy), np.arange(wx), indexing="ij")
+    w = np.stack([jr.ravel(order="F") * step, jc.ravel(order="F") * step], axis=1)
+    return np.ascontiguousarray(w, np.int32)
+
+
+def ncc_loss_grad(coefA, coefB, shape, P, grid, window=16, overlap=8, windows=None, grad=True, nthreads=8,
+                  dtype=np.float64):
+    """Correlation loss L = -sum NCC0 over the windows (all, or the given
+    0-based origins) of the pair deformed by P (gny, gnx, 2) on nodes
+    grid = (y0, ysp, x0, xsp); returns (L, dL/dP shaped like P or None)."""
+    T, ct, suf = _T(dtype)
+    nr, nc = shape
+    P = np.asarray(P)
+    gny, gnx = P.shape[0], P.shape[1]
+    flat = np.concatenate([P[..., 0].ravel(order="F"), P[..., 1].ravel(order="F")]).astype(T)
+    wins = ncc_windows(shape, window, overlap) if windows is None else np.ascontiguousarray(windows, np.int32)
+    g = np.zeros(2 * gny * gnx, T) if grad else None
+    f = _fn("ncc_loss_grad", suf)
+    f.restype = ctypes.c_double
+    y0, ysp, x0, xsp = grid
+    L = f(_p(np.asfortranarray(coefA, T), ct), _p(np.asfortranarray(coefB, T), ct), ctypes.c_int64(nr),
+          ctypes.c_int64(nc), _p(flat, ct), gny, gnx, ctypes.c_double(y0), ctypes.c_double(ysp), ctypes.c_double(x0),
+          ctypes.c_double(xsp), window, wins.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+          ctypes.c_int64(len(wins)), _p(g, ct) if grad else None, nthreads)
+    if not grad:
+        return L, None
+    G = gny * gnx
+    out = np.empty((gny, gnx, 2), T)
+    out[..., 0] = np.reshape(g[:G], (gny, gnx), order="F")
+    out[..., 1] = np.reshape(g[G:], (gny, gnx), order="F")
+    return L, out
