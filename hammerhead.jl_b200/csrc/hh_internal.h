@@ -41,6 +41,8 @@ struct CorrArgs {
   const BPair* bp;
   const int32_t* done;
   int32_t it;
+  // ensemble mode: planes += R (planes != nullptr) and no peak analysis
+  int32_t accumulate;
 };
 
 // Launch the correlation kernel for FFT size N (square) and window W.
@@ -56,6 +58,12 @@ struct AnalyzeArgs {
   int32_t npeaks, finder, subpixel;
   float* packed;
   int32_t* locs;
+  // optional grid outputs (as CorrArgs): plane j is job j of `jobs`
+  const int32_t* jobs;
+  int32_t ny;
+  int64_t G;
+  float *du, *dv, *ratio, *moment, *alt_u, *alt_v;
+  int32_t nalt;
 };
 cudaError_t launch_analyze_planes(const AnalyzeArgs& a, cudaStream_t s);
 
@@ -117,8 +125,13 @@ struct UQArgs {
   const BPair* bp;
   const int32_t* done;
   int32_t mode;
+  // ensemble mode: stats += this pair's statistics
+  int32_t accumulate;
 };
 cudaError_t launch_uq(const UQArgs& a, cudaStream_t s, int num_sms);
+// finalize_uncertainty of pooled statistics (88 per job) into grid cells
+cudaError_t launch_uq_finalize(const double* stats, const int32_t* jobs, int64_t njobs, int32_t ny, float* unc_u,
+                               float* unc_v, cudaStream_t s);
 
 // --- adjoint of deformation + zero-lag correlation --------------------------
 struct NccArgs {

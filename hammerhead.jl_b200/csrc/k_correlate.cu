@@ -50,22 +50,39 @@ struct TopK {
 #pragma unroll
     for (int m = 0; m < KMAX; ++m) hi[m] = lo[m] = 0u;
   }
-  // insert keeping (hi, lo) descending; K <= KMAX entries retained
+  // the K-th (last retained) key, read with unrolled selects so the arrays
+  // stay in registers for a run-time K
+  __device__ __forceinline__ uint32_t last_hi(int K) const {
+    uint32_t v = 0u;
+#pragma unroll
+    for (int m = 0; m < KMAX; ++m) v = (m == K - 1) ? hi[m] : v;
+    return v;
+  }
+  __device__ __forceinline__ uint32_t last_lo(int K) const {
+    uint32_t v = 0u;
+#pragma unroll
+    for (int m = 0; m < KMAX; ++m) v = (m == K - 1) ? lo[m] : v;
+    return v;
+  }
+  // insert keeping (hi, lo) descending; K <= KMAX entries retained. Valid
+  // keys are nonzero and empty slots hold 0, so the new key bubbles down
+  // through compare-and-select steps (no data-dependent indexing: the list
+  // stays in registers).
   __device__ __forceinline__ void insert(uint32_t h, uint32_t l, int K) {
-    if (cnt == K && !(h > hi[K - 1] || (h == hi[K - 1] && l > lo[K - 1]))) return;
+    if (cnt == K) {
+      const uint32_t lh = last_hi(K), ll = last_lo(K);
+      if (!(h > lh || (h == lh && l > ll))) return;
+    }
     uint32_t ch = h, cl = l;
 #pragma unroll
     for (int m = 0; m < KMAX; ++m) {
-      if (m < K && m <= cnt) {
-        bool better = ch > hi[m] || (ch == hi[m] && cl > lo[m]) || m == cnt;
-        if (better) {
-          uint32_t th = hi[m], tl = lo[m];
-          hi[m] = ch;
-          lo[m] = cl;
-          ch = th;
-          cl = tl;
-        }
-      }
+      const bool in = m < K;
+      const bool better = in && (ch > hi[m] || (ch == hi[m] && cl > lo[m]));
+      const uint32_t th = hi[m], tl = lo[m];
+      hi[m] = better ? ch : th;
+      lo[m] = better ? cl : tl;
+      ch = better ? th : ch;
+      cl = better ? tl : cl;
     }
     if (cnt < K) ++cnt;
   }
@@ -97,18 +114,31 @@ __device__ __forceinline__ bool is_local_max(const float* R, int nr, int nc, int
   return true;
 }
 
-// Group-wide argmax of (hi, lo) keys. All threads of the CTA call it (it
-// contains __syncthreads); each window group gets its own reduction slots.
+// Barrier of one thread group: a warp (count 32), the whole CTA (bar 0), or
+// the named barrier `bar` shared by `count` threads (whole warps).
+__device__ __forceinline__ void grp_sync(int bar, int count) {
+  if (count == 32) __syncwarp();
+  else if (bar == 0) __syncthreads();
+  else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+// Group-wide argmax of (hi, lo) keys. Every thread of the group calls it (it
+// synchronises the group); each group has its own reduction slots.
 __device__ __forceinline__ void group_argmax(uint32_t hi, uint32_t lo, uint32_t* red, int gwarp, int nwarps,
-                                             uint32_t& whi, uint32_t& wlo) {
+                                             uint32_t& whi, uint32_t& wlo, int bar) {
   const int lane = threadIdx.x & 31;
   uint32_t mhi = __reduce_max_sync(0xffffffffu, hi);
   uint32_t mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  if (nwarps == 1) {  // one warp: the shuffle reduction is the answer
+    whi = mhi;
+    wlo = mlo;
+    return;
+  }
   if (lane == 0) {
     red[2 * gwarp] = mhi;
     red[2 * gwarp + 1] = mlo;
   }
-  __syncthreads();
+  grp_sync(bar, nwarps * 32);
   whi = 0u;
   wlo = 0u;
   for (int w = 0; w < nwarps; ++w) {
@@ -118,7 +148,7 @@ __device__ __forceinline__ void group_argmax(uint32_t hi, uint32_t lo, uint32_t*
       wlo = l;
     }
   }
-  __syncthreads();
+  grp_sync(bar, nwarps * 32);
 }
 
 // subpixel_gauss3 (src/correlators.jl:499-520) with FP64 logarithms.
@@ -208,9 +238,12 @@ struct PeakOut {
 // Peak analysis of one plane by a group of threads (tid in [0, gsize)).
 // Every thread of the CTA must call this (uniform K and finder), because
 // the merge rounds synchronise the whole CTA.
-__device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
+__device__ __forceinline__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
                               int subpixel, int gtid, int gsize, uint32_t* red, bool active, float* s_vals,
-                              int* s_locs, int64_t grid_id, int64_t job, const PeakOut& o) {
+                              int* s_locs, int64_t grid_id, int64_t job, const PeakOut& o, bool poison, int bar) {
+  // a poisoned plane (non-finite window data: the reference's plane is all
+  // NaN there) yields no peak, so every output is NaN
+  const bool scan = active && !poison;
   const int gwarp = gtid >> 5, nwarps = gsize >> 5;
   const int P = nr * nc;
   int nfound = 0;
@@ -223,7 +256,7 @@ __device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, in
     // neighbours, which never block in the reference either.
     TopK tk;
     tk.init();
-    if (active) {
+    if (scan) {
       const int S = gsize / nc > 0 ? gsize / nc : 1;  // row segments per column
       const int rps = (nr + S - 1) / S;
       const float NaNf = __int_as_float(0x7fc00000);
@@ -252,7 +285,7 @@ __device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, in
           if (!isnan(v)) {
             const uint32_t h = fkey(v);
             // a later index cannot win a tie, so a full list rejects h <= last
-            if (tk.cnt < K || h > tk.hi[K - 1]) {
+            if (tk.cnt < K || h > tk.last_hi(K)) {
               const float e = fmaxf(fmaxf(lt, lm), fmaxf(lb, ct));
               const float l = fmaxf(fmaxf(rt, rm), fmaxf(rb, cb));
               if (!(e > v) && !(l >= v)) tk.insert(h, ~(uint32_t)(r + c * nr), K);
@@ -264,9 +297,9 @@ __device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, in
       }
     }
     bool done = false;
-    for (int round = 0; round < K; ++round) {  // every round runs: group_argmax synchronises the CTA
+    for (int round = 0; round < K; ++round) {  // every round runs: group_argmax synchronises the group
       uint32_t whi, wlo;
-      group_argmax(tk.cnt > 0 ? tk.hi[0] : 0u, tk.cnt > 0 ? tk.lo[0] : 0u, red, gwarp, nwarps, whi, wlo);
+      group_argmax(tk.cnt > 0 ? tk.hi[0] : 0u, tk.cnt > 0 ? tk.lo[0] : 0u, red, gwarp, nwarps, whi, wlo, bar);
       if (done || whi == 0u) { done = true; continue; }
       if (tk.cnt > 0 && tk.hi[0] == whi && tk.lo[0] == wlo) tk.pop();
       if (gtid == 0) {
@@ -280,9 +313,9 @@ __device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, in
   } else {
     // exclusion finder (src/correlators.jl:390-421): K scans, box +-2
     bool done = false;
-    for (int round = 0; round < K; ++round) {  // every round runs: group_argmax synchronises the CTA
+    for (int round = 0; round < K; ++round) {  // every round runs: group_argmax synchronises the group
       uint32_t bh = 0u, bl = 0u;
-      if (active && !done) {
+      if (scan && !done) {
         for (int lin = gtid; lin < P; lin += gsize) {
           const int r = lin % nr, c = lin / nr;
           bool ex = false;
@@ -296,7 +329,7 @@ __device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, in
         }
       }
       uint32_t whi, wlo;
-      group_argmax(bh, bl, red, gwarp, nwarps, whi, wlo);
+      group_argmax(bh, bl, red, gwarp, nwarps, whi, wlo, bar);
       if (!done && whi != 0u) {
         const int lin = (int)(~wlo);
         const float best = R[(lin / nr) * ldr + (lin % nr)];
@@ -313,7 +346,7 @@ __device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, in
       } else {
         done = true;
       }
-      __syncthreads();  // s_locs visible to the next round's exclusion test
+      grp_sync(bar, gsize);  // s_locs visible to the next round's exclusion test
     }
   }
   // Epilogue on the group's first warp: lane 0 refines the primary and forms
@@ -380,24 +413,48 @@ __device__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, in
   }
 }
 
+// S(k) = conj(FA(k)) FB(k) of the packed transform Z = F(a + i b), from
+// X = Z(k) and Zm = Z(-k): FA = (X + conj(Zm))/2, FB = (X - conj(Zm))/(2i)
+// (spectrum!, src/correlators.jl:266-279); the phase method divides by
+// |S| + eps(Float32) and applies the spectral filter weight wk.
+__device__ __forceinline__ float2 cross_spectrum(float2 X, float2 Zm, int method, float wk) {
+  const float2 Y = make_float2(Zm.x, -Zm.y);
+  const float Ar = 0.5f * (X.x + Y.x), Ai = 0.5f * (X.y + Y.y);
+  const float Br = 0.5f * (X.y - Y.y), Bi = -0.5f * (X.x - Y.x);
+  float2 S = cmul(make_float2(Ar, -Ai), make_float2(Br, Bi));
+  if (method == 1) {
+    const float den = hypotf(S.x, S.y) + 1.1920929e-7f;
+    S = make_float2((wk * S.x) / den, (wk * S.y) / den);
+  }
+  return S;
+}
+
 // ---------------------------------------------------------------------------
 template <int N, int W> struct CorrCfg {
   static constexpr int N1 = AxisSplit<N>::N1, N2 = AxisSplit<N>::N2;
   static constexpr int WPC = N <= 32 ? 4 : (N <= 64 ? 2 : 1);    // windows per CTA
   static constexpr int NT = N <= 48 ? 128 : (N <= 64 ? 256 : 512);
   static constexpr int G = NT / WPC;  // threads per window in the analysis
+  // CTAs per SM the register budget is sized for (the shared-memory limit
+  // allows at least this many)
+  static constexpr int MINB = N <= 32 ? 4 : (N <= 64 ? 3 : 1);
+  // The spectrum is Hermitian, so the inverse transforms only the N/2 + 1
+  // canonical columns along p and then rows p and p + N/2 together along q
+  // (their outputs are real: one lands in the real part, one in the
+  // imaginary part). Every window is transformed on its own.
+  static constexpr int NC = N / 2 + 1;
+  static constexpr int IPT = ((N / 2) * N2 + G - 1) / G;  // final inverse items per thread
   static constexpr int LD = N + 1;    // complex plane leading dimension (float2)
   static constexpr int LDR = N + 1;   // real plane leading dimension (float), overlays the complex plane
   static constexpr bool PADDED = (W * 2 == N);
   static constexpr int NZ1 = PADDED ? (W / N2) : N1;  // nonzero inputs of a forward pass-A line
-  static constexpr int IPT = (WPC * N * N2 + NT - 1) / NT;  // final inverse items per thread
+
   static constexpr int EPT = (W * W + G - 1) / G;             // window pixels per thread
   static constexpr size_t PLANE_B = (size_t)N * LD * sizeof(float2);
   static constexpr size_t smem() {
     return WPC * PLANE_B + WPC * (G / 32) * 3 * sizeof(double) + N * sizeof(float2) +
            WPC * (G / 32) * 2 * sizeof(uint32_t) +
-           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int) + 4 * sizeof(int)) +
-           WPC * (3 * sizeof(void*) + sizeof(int64_t)) + 64;
+           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int)) + 3 * N * sizeof(int) + 64;
   }
   static_assert(W == N || 2 * W == N, "window must equal the FFT size or half of it");
   static_assert(G >= 32 && G % 32 == 0, "analysis group must be whole warps");
@@ -405,88 +462,93 @@ template <int N, int W> struct CorrCfg {
 };
 
 template <int N, int W>
-__global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const CorrArgs a) {
+__global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correlate_kernel(const CorrArgs a) {
   using C = CorrCfg<N, W>;
   constexpr int WPC = C::WPC, NT = C::NT, LD = C::LD, LDR = C::LDR, N1 = C::N1, N2 = C::N2, IPT = C::IPT;
-  constexpr int G = C::G, EPT = C::EPT;
+  constexpr int G = C::G, EPT = C::EPT, NC = C::NC, H = N / 2;
   constexpr int PS = N * LD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* planes = reinterpret_cast<float2*>(smem_raw);
   double* s_part = reinterpret_cast<double*>(smem_raw + WPC * C::PLANE_B);  // 3 per warp: sum A, sum B, count
-  float2* tw = reinterpret_cast<float2*>(s_part + WPC * (C::G / 32) * 3);
+  float2* tw = reinterpret_cast<float2*>(s_part + WPC * (G / 32) * 3);
   uint32_t* red = reinterpret_cast<uint32_t*>(tw + N);
-  float* s_vals = reinterpret_cast<float*>(red + WPC * (C::G / 32) * 2);
+  float* s_vals = reinterpret_cast<float*>(red + WPC * (G / 32) * 2);
   int* s_locs = reinterpret_cast<int*>(s_vals + WPC * KMAX);
-  int* s_job = s_locs + WPC * 2 * KMAX;  // rs, cs, pair, unused per window
-  uintptr_t* s_src = reinterpret_cast<uintptr_t*>(
-      (reinterpret_cast<uintptr_t>(s_job + WPC * 4) + 7) & ~(uintptr_t)7);  // A, B, mask per window
-  int64_t* s_ld = reinterpret_cast<int64_t*>(s_src + 3 * WPC);
+  // per-axis storage tables (N2 > 1): frequency of storage slot a, storage
+  // slot of the negated frequency, canonical storage columns kq = 0..N/2
+  int* s_freq = reinterpret_cast<int*>(s_locs + WPC * 2 * KMAX);
+  int* s_neg = s_freq + N;
+  int* s_canon = s_neg + N;
 
   const int tid = threadIdx.x;
   const int K = a.npeaks > 2 ? a.npeaks : 2;
   if (N2 > 1) {
     for (int m = tid; m < N; m += NT) {
-      double s, c;
-      sincospi(-2.0 * (double)m / (double)N, &s, &c);
-      tw[m] = make_float2((float)c, (float)s);  // W_N^m = exp(-2 pi i m / N)
+      double sn, cs;
+      sincospi(-2.0 * (double)m / (double)N, &sn, &cs);
+      tw[m] = make_float2((float)cs, (float)sn);  // W_N^m = exp(-2 pi i m / N)
+    }
+    for (int q = tid; q < N; q += NT) {
+      const int k = q / N2 + N1 * (q % N2);  // storage slot q holds frequency k
+      const int m = (N - k) % N;
+      s_freq[q] = k;
+      s_neg[q] = N2 * (m % N1) + m / N1;
+      if (q <= N / 2) s_canon[q] = N2 * (q % N1) + q / N1;
     }
   }
+  __syncthreads();  // the only CTA-wide barrier: from here on the window groups run independently
+
+  // Thread group w (G threads, named barrier w + 1) owns plane w and walks
+  // its own sequence of jobs; a group waits only for itself.
+  const int w = tid / G, gt = tid % G, lane = tid & 31, gw = gt >> 5;
+  const int bar = WPC == 1 ? 0 : w + 1;
+  float2* P = planes + w * PS;
+  float* Rw = reinterpret_cast<float*>(P);  // real plane, overlays the complex one after stage 8
+  double* part = s_part + w * (G / 32) * 3;
   const float scale = 1.0f / (float)(N * N);
   PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
 
-  for (int64_t base = (int64_t)blockIdx.x * WPC; base < a.njobs; base += (int64_t)gridDim.x * WPC) {
-    if (tid < WPC) {
-      const int64_t job = base + tid;
-      int rs = -1, cs = -1, pr = -1;
-      const float* A = a.A;
-      const float* B = a.B;
-      const uint8_t* M = a.mask;
-      int64_t ld = a.ld;
-      if (job < a.njobs) {
-        if (a.bp) {
-          const int p = a.jobs[4 * job];
-          const BPair& b = a.bp[p];
-          const int gij = a.jobs[4 * job + 1];
-          const int64_t cell = (int64_t)(gij & 0xFFFF) + (int64_t)(gij >> 16) * b.ny;
-          if (bp_live(b, a.it, a.done, p) && !(b.gmask && b.gmask[cell])) {
-            pr = p;
-            rs = a.jobs[4 * job + 2];
-            cs = a.jobs[4 * job + 3];
-            const bool warped = a.it > 1 || b.has_pred0;
-            A = warped ? b.warpA : b.A;
-            B = warped ? b.warpB : b.B;
-            M = b.mask;
-            ld = b.nr;
-          }
-        } else {
-          rs = a.jobs[4 * job + 2];
-          cs = a.jobs[4 * job + 3];
-        }
-      }
-      s_job[4 * tid] = rs;
-      s_job[4 * tid + 1] = cs;
-      s_job[4 * tid + 2] = pr;
-      s_src[3 * tid] = reinterpret_cast<uintptr_t>(A);
-      s_src[3 * tid + 1] = reinterpret_cast<uintptr_t>(B);
-      s_src[3 * tid + 2] = reinterpret_cast<uintptr_t>(M);
-      s_ld[tid] = ld;
+  for (int64_t job = (int64_t)blockIdx.x * WPC + w; job < a.njobs; job += (int64_t)gridDim.x * WPC) {
+    // ---- the window's source (every thread of the group reads the same
+    //      descriptor words; they are broadcast from L1)
+    int rs, cs;
+    const float* A = a.A;
+    const float* B = a.B;
+    const uint8_t* M = a.mask;
+    int64_t ld = a.ld, gid;
+    PeakOut pw = po;
+    if (a.bp) {
+      const int p = a.jobs[4 * job];
+      const BPair& b = a.bp[p];
+      const int gij = a.jobs[4 * job + 1];
+      const int64_t cell = (int64_t)(gij & 0xFFFF) + (int64_t)(gij >> 16) * b.ny;
+      // pairs that converged or have no further sweep, and masked cells, are skipped
+      if (!bp_live(b, a.it, a.done, p) || (b.gmask && b.gmask[cell])) continue;
+      rs = a.jobs[4 * job + 2];
+      cs = a.jobs[4 * job + 3];
+      const bool warped = a.it > 1 || b.has_pred0;
+      A = warped ? b.warpA : b.A;
+      B = warped ? b.warpB : b.B;
+      M = b.mask;
+      ld = b.nr;
+      gid = b.goff + cell;
+      pw.G = (int64_t)b.ny * b.nx;
+      pw.nalt = b.nalt;
+      pw.alt_u = a.alt_u ? a.alt_u + b.aoff - b.goff : nullptr;  // indexed by gid + m*G
+      pw.alt_v = a.alt_v ? a.alt_v + b.aoff - b.goff : nullptr;
+    } else {
+      rs = a.jobs[4 * job + 2];
+      cs = a.jobs[4 * job + 3];
+      gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
     }
-    // a group without a window to analyse (pairs that converged or have no
-    // further sweep, masked cells) is skipped as a whole
-    if (!__syncthreads_or(tid < WPC && s_job[4 * tid] >= 0)) continue;
-    // ---- stages 1-3: each window's thread group loads its pixels (coalesced
-    //      down the columns), reduces the window means in FP64, and stores
+    // ---- stages 1-3: the group loads the window's pixels (coalesced down
+    //      the columns), reduces the window means in FP64, and stores
     //      apod * (x - mean) into the plane; masked pixels enter as zero and
     //      leave the mean (load_windows!, src/correlators.jl:188-263). The
     //      mean is the exact sum over n rounded once, where the reference
     //      folds in Float32 left to right; the two differ by a few ulp.
+    bool bad;
     {
-      const int w = tid / G, gt = tid % G, lane = tid & 31, gw = gt >> 5;
-      const int rs = s_job[4 * w], cs = s_job[4 * w + 1];
-      const float* wA = reinterpret_cast<const float*>(s_src[3 * w]);
-      const float* wB = reinterpret_cast<const float*>(s_src[3 * w + 1]);
-      const uint8_t* wM = reinterpret_cast<const uint8_t*>(s_src[3 * w + 2]);
-      const int64_t wld = s_ld[w];
       float2 z[EPT];
       bool mk[EPT];
       double sa = 0.0, sb = 0.0, cnt = 0.0;
@@ -495,11 +557,11 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
         const int e = gt + i * G;
         z[i] = make_float2(0.f, 0.f);
         mk[i] = true;
-        if (e < W * W && rs >= 0) {
+        if (e < W * W) {
           const int p = e % W, q = e / W;
-          const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * wld;
-          z[i] = make_float2(__ldg(wA + off), __ldg(wB + off));
-          mk[i] = wM ? __ldg(wM + off) != 0 : false;
+          const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * ld;
+          z[i] = make_float2(__ldg(A + off), __ldg(B + off));
+          mk[i] = M ? __ldg(M + off) != 0 : false;
           if (!mk[i]) {
             sa += (double)z[i].x;
             sb += (double)z[i].y;
@@ -513,37 +575,39 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
         sb += __shfl_xor_sync(0xffffffffu, sb, o);
         cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
       }
-      double* part = s_part + w * (G / 32) * 3;
-      if (lane == 0) {
-        part[3 * gw] = sa;
-        part[3 * gw + 1] = sb;
-        part[3 * gw + 2] = cnt;
-      }
-      __syncthreads();
-      double ta = 0.0, tb = 0.0, tn = 0.0;
-      for (int k = 0; k < G / 32; ++k) {
-        ta += part[3 * k];
-        tb += part[3 * k + 1];
-        tn += part[3 * k + 2];
+      double ta = sa, tb = sb, tn = cnt;
+      if (G > 32) {
+        if (lane == 0) {
+          part[3 * gw] = sa;
+          part[3 * gw + 1] = sb;
+          part[3 * gw + 2] = cnt;
+        }
+        grp_sync(bar, G);
+        ta = tb = tn = 0.0;
+        for (int k = 0; k < G / 32; ++k) {
+          ta += part[3 * k];
+          tb += part[3 * k + 1];
+          tn += part[3 * k + 2];
+        }
       }
       const float ma = tn > 0 ? (float)(ta / tn) : 0.f, mb = tn > 0 ? (float)(tb / tn) : 0.f;
+      bad = !(isfinite(ta) && isfinite(tb));  // the window holds NaN or Inf
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
         const int e = gt + i * G;
         if (e < W * W) {
           const int p = e % W, q = e / W;
           const float ap = __ldg(a.apod + e);
-          planes[w * PS + q * LD + p] =
-              mk[i] ? make_float2(0.f, 0.f) : make_float2(ap * (z[i].x - ma), ap * (z[i].y - mb));
+          P[q * LD + p] = (mk[i] || bad) ? make_float2(0.f, 0.f) : make_float2(ap * (z[i].x - ma), ap * (z[i].y - mb));
         }
       }
     }
-    __syncthreads();
+    grp_sync(bar, G);
 
     // ---- stage 4: forward transform along p (only the W data columns)
-    for (int it = tid; it < WPC * W * N2; it += NT) {
-      const int q = it % W, n2 = (it / W) % N2, w = it / (W * N2);
-      float2* L = planes + w * PS + q * LD;
+    for (int it = gt; it < W * N2; it += G) {
+      const int q = it % W, n2 = it / W;
+      float2* L = P + q * LD;
       float2 x[N1];
 #pragma unroll
       for (int n1 = 0; n1 < N1; ++n1) x[n1] = n1 < C::NZ1 ? L[N2 * n1 + n2] : make_float2(0.f, 0.f);
@@ -556,10 +620,10 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
       for (int k1 = 0; k1 < N1; ++k1) L[N2 * k1 + n2] = x[k1];
     }
     if (N2 > 1) {
-      __syncthreads();
-      for (int it = tid; it < WPC * W * N1; it += NT) {
-        const int q = it % W, k1 = (it / W) % N1, w = it / (W * N1);
-        float2* L = planes + w * PS + q * LD + N2 * k1;
+      grp_sync(bar, G);
+      for (int it = gt; it < W * N1; it += G) {
+        const int q = it % W, k1 = it / W;
+        float2* L = P + q * LD + N2 * k1;
         float2 x[N2];
 #pragma unroll
         for (int n2 = 0; n2 < N2; ++n2) x[n2] = L[n2];
@@ -568,11 +632,11 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
         for (int k2 = 0; k2 < N2; ++k2) L[k2] = x[k2];
       }
     }
-    __syncthreads();
+    grp_sync(bar, G);
     // ---- stage 5: forward transform along q for every row p
-    for (int it = tid; it < WPC * N * N2; it += NT) {
-      const int p = it % N, n2 = (it / N) % N2, w = it / (N * N2);
-      float2* L = planes + w * PS + p;
+    for (int it = gt; it < N * N2; it += G) {
+      const int p = it % N, n2 = it / N;
+      float2* L = P + p;
       float2 x[N1];
 #pragma unroll
       for (int n1 = 0; n1 < N1; ++n1) x[n1] = n1 < C::NZ1 ? L[(N2 * n1 + n2) * LD] : make_float2(0.f, 0.f);
@@ -585,10 +649,10 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
       for (int k1 = 0; k1 < N1; ++k1) L[(N2 * k1 + n2) * LD] = x[k1];
     }
     if (N2 > 1) {
-      __syncthreads();
-      for (int it = tid; it < WPC * N * N1; it += NT) {
-        const int p = it % N, k1 = (it / N) % N1, w = it / (N * N1);
-        float2* L = planes + w * PS + p + (N2 * k1) * LD;
+      grp_sync(bar, G);
+      for (int it = gt; it < N * N1; it += G) {
+        const int p = it % N, k1 = it / N;
+        float2* L = P + p + (N2 * k1) * LD;
         float2 x[N2];
 #pragma unroll
         for (int n2 = 0; n2 < N2; ++n2) x[n2] = L[n2 * LD];
@@ -597,85 +661,39 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
         for (int k2 = 0; k2 < N2; ++k2) L[k2 * LD] = x[k2];
       }
     }
-    __syncthreads();
+    grp_sync(bar, G);
     // ---- stage 6: cross-power (or filtered phase) spectrum over Hermitian
-    //      pairs (k, -k). For N <= 32 the frequencies are stored in natural
-    //      order and only the canonical half is enumerated; for larger N the
-    //      walk follows storage order so a warp reads consecutive words.
-    {
-      constexpr int NCAN = N2 == 1 ? (N / 2 + 1) * N : N * N;  // columns kq <= N/2 hold every pair
-      for (int it = tid; it < WPC * NCAN; it += NT) {
-        int ap, aq, kp, kq;
-        const int w = it / NCAN, r = it % NCAN;
-        if (N2 == 1) {
-          kp = r % N;
-          kq = r / N;
-          ap = kp;
-          aq = kq;
-        } else {
-          ap = r % N;
-          aq = r / N;
-          kp = ap / N2 + N1 * (ap % N2);
-          kq = aq / N2 + N1 * (aq % N2);
-        }
-        const int mp = (N - kp) % N, mq = (N - kq) % N;
-        const int bp = N2 * (mp % N1) + mp / N1, bq = N2 * (mq % N1) + mq / N1;
-        if (ap + aq * N > bp + bq * N) continue;  // the partner position does this pair
-        float2* P = planes + w * PS;
-        const float2 X = P[aq * LD + ap];
-        const float2 Zm = P[bq * LD + bp];
-        const float2 Y = make_float2(Zm.x, -Zm.y);  // conj(Z[-k])
-        // FA = (X + Y)/2, FB = (X - Y)/(2i); S = conj(FA) * FB
-        const float Ar = 0.5f * (X.x + Y.x), Ai = 0.5f * (X.y + Y.y);
-        const float Br = 0.5f * (X.y - Y.y), Bi = -0.5f * (X.x - Y.x);
-        float2 S = cmul(make_float2(Ar, -Ai), make_float2(Br, Bi));
-        if (a.method == 1) {
-          const float den = hypotf(S.x, S.y) + 1.1920929e-7f;  // eps(Float32)
-          const float wk = __ldg(a.phasew + kq * N + kp);
-          S = make_float2((wk * S.x) / den, (wk * S.y) / den);
-        }
-        P[aq * LD + ap] = S;
-        P[bq * LD + bp] = make_float2(S.x, -S.y);
+    //      pairs (k, -k) on the canonical columns kq = 0..N/2 (frequencies in
+    //      storage order for N2 > 1, natural order otherwise). Only canonical
+    //      columns are written: the inverse never reads the others.
+    for (int it = gt; it < NC * N; it += G) {
+      const int ap = it % N, c = it / N;
+      int aq, bq, bp, kp;
+      if (N2 == 1) {
+        aq = c;
+        bq = (N - c) % N;
+        bp = (N - ap) % N;
+        kp = ap;
+      } else {
+        aq = s_canon[c];
+        bq = s_neg[aq];
+        bp = s_neg[ap];
+        kp = s_freq[ap];
       }
+      const bool self = aq == bq;
+      if (self && ap > bp) continue;  // self-paired column: its partner row does this pair
+      const float wk = a.method == 1 ? __ldg(a.phasew + c * N + kp) : 1.f;
+      const float2 S = cross_spectrum(P[aq * LD + ap], P[bq * LD + bp], a.method, wk);
+      P[aq * LD + ap] = S;
+      if (self) P[bq * LD + bp] = make_float2(S.x, -S.y);
     }
-    __syncthreads();
-    // ---- stage 7: inverse along q (every row p), back to natural order
+    grp_sync(bar, G);
+    // ---- stage 7: inverse along p for the canonical columns, back to natural
+    //      p; the conjugate column -kq is filled in as conj of column kq
     if (N2 > 1) {
-      for (int it = tid; it < WPC * N * N1; it += NT) {
-        const int p = it % N, k1 = (it / N) % N1, w = it / (N * N1);
-        float2* L = planes + w * PS + p + (N2 * k1) * LD;
-        float2 x[N2];
-#pragma unroll
-        for (int k2 = 0; k2 < N2; ++k2) x[k2] = L[k2 * LD];
-        RDFT<N2, true>::run(x, N2);
-#pragma unroll
-        for (int n2 = 1; n2 < N2; ++n2) {
-          const float2 t = tw[(n2 * k1) % N];
-          x[n2] = cmul(x[n2], make_float2(t.x, -t.y));
-        }
-#pragma unroll
-        for (int n2 = 0; n2 < N2; ++n2) L[n2 * LD] = x[n2];
-      }
-      __syncthreads();
-    }
-    for (int it = tid; it < WPC * N * N2; it += NT) {
-      const int p = it % N, n2 = (it / N) % N2, w = it / (N * N2);
-      float2* L = planes + w * PS + p;
-      float2 x[N1];
-#pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) x[k1] = L[(N2 * k1 + n2) * LD];
-      RDFT<N1, true>::run(x, N1);
-#pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1) L[(N2 * n1 + n2) * LD] = x[n1];
-    }
-    __syncthreads();
-    // ---- stage 8: inverse along p (every column q). The fftshifted,
-    //      normalised, gain-weighted magnitudes are held in registers across
-    //      a barrier, then written as the real plane R over the complex one.
-    if (N2 > 1) {
-      for (int it = tid; it < WPC * N * N1; it += NT) {
-        const int q = it % N, k1 = (it / N) % N1, w = it / (N * N1);
-        float2* L = planes + w * PS + q * LD + N2 * k1;
+      for (int it = gt; it < NC * N1; it += G) {
+        const int c = it % NC, k1 = it / NC;
+        float2* L = P + s_canon[c] * LD + N2 * k1;
         float2 x[N2];
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) x[k2] = L[k2];
@@ -688,81 +706,116 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT) correlate_kernel(const Corr
 #pragma unroll
         for (int n2 = 0; n2 < N2; ++n2) L[n2] = x[n2];
       }
-      __syncthreads();
+      grp_sync(bar, G);
+    }
+    for (int it = gt; it < NC * N2; it += G) {
+      const int c = it % NC, n2 = it / NC;
+      const int aq = N2 == 1 ? c : s_canon[c];
+      const int bq = N2 == 1 ? (N - c) % N : s_neg[aq];
+      float2* L = P + aq * LD;
+      float2* Lb = P + bq * LD;
+      float2 x[N1];
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) x[k1] = L[N2 * k1 + n2];
+      RDFT<N1, true>::run(x, N1);
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) {
+        L[N2 * n1 + n2] = x[n1];
+        if (bq != aq) Lb[N2 * n1 + n2] = make_float2(x[n1].x, -x[n1].y);
+      }
+    }
+    grp_sync(bar, G);
+    // ---- stage 8: inverse along q for row pairs (p, p + N/2) packed as
+    //      T(p) + i T(p + N/2); the fftshifted, normalised, gain-weighted
+    //      magnitudes are held in registers across a barrier, then written
+    //      as the real plane R over the complex one.
+    if (N2 > 1) {
+      for (int it = gt; it < H * N1; it += G) {
+        const int p = it % H, k1 = it / H;
+        float2* L = P + p + (N2 * k1) * LD;
+        float2 x[N2];
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+          const float2 u = L[k2 * LD], v = L[k2 * LD + H];
+          x[k2] = make_float2(u.x - v.y, u.y + v.x);
+        }
+        RDFT<N2, true>::run(x, N2);
+#pragma unroll
+        for (int n2 = 1; n2 < N2; ++n2) {
+          const float2 t = tw[(n2 * k1) % N];
+          x[n2] = cmul(x[n2], make_float2(t.x, -t.y));
+        }
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) L[n2 * LD] = x[n2];
+      }
+      grp_sync(bar, G);
     }
     {
-      float rv[IPT][N1];
+      float rv[IPT][2][N1];
 #pragma unroll
       for (int i = 0; i < IPT; ++i) {
-        const int it = tid + i * NT;
-        if (it < WPC * N * N2) {
-          const int q = it % N, n2 = (it / N) % N2, w = it / (N * N2);
-          const float2* L = planes + w * PS + q * LD;
+        const int it = gt + i * G;
+        if (it < H * N2) {
+          const int p = it % H, n2 = it / H;
+          const float2* L = P + p;
           float2 x[N1];
 #pragma unroll
-          for (int k1 = 0; k1 < N1; ++k1) x[k1] = L[N2 * k1 + n2];
+          for (int k1 = 0; k1 < N1; ++k1) {
+            if (N2 == 1) {
+              const float2 u = L[k1 * LD], v = L[k1 * LD + H];
+              x[k1] = make_float2(u.x - v.y, u.y + v.x);
+            } else {
+              x[k1] = L[(N2 * k1 + n2) * LD];
+            }
+          }
           RDFT<N1, true>::run(x, N1);
-          const int qs = (q + N / 2) % N;
+          const int ps0 = (p + H) % N, ps1 = p;  // fftshifted rows of p and p + N/2
 #pragma unroll
           for (int n1 = 0; n1 < N1; ++n1) {
-            const int ps = (N2 * n1 + n2 + N / 2) % N;
-            float r = fabsf(x[n1].x) * scale;
-            if (a.gain) r *= __ldg(a.gain + qs * N + ps);
-            rv[i][n1] = r;
+            const int qs = (N2 * n1 + n2 + H) % N;
+            float r0 = fabsf(x[n1].x) * scale, r1 = fabsf(x[n1].y) * scale;
+            if (a.gain) {
+              r0 *= __ldg(a.gain + qs * N + ps0);
+              r1 *= __ldg(a.gain + qs * N + ps1);
+            }
+            rv[i][0][n1] = r0;
+            rv[i][1][n1] = r1;
           }
         }
       }
-      __syncthreads();
+      grp_sync(bar, G);
 #pragma unroll
       for (int i = 0; i < IPT; ++i) {
-        const int it = tid + i * NT;
-        if (it < WPC * N * N2) {
-          const int q = it % N, n2 = (it / N) % N2, w = it / (N * N2);
-          const int qs = (q + N / 2) % N;
-          float* Rw = reinterpret_cast<float*>(planes + w * PS);
+        const int it = gt + i * G;
+        if (it < H * N2) {
+          const int p = it % H, n2 = it / H;
+          const int ps0 = (p + H) % N, ps1 = p;
 #pragma unroll
-          for (int n1 = 0; n1 < N1; ++n1) Rw[qs * LDR + (N2 * n1 + n2 + N / 2) % N] = rv[i][n1];
-        }
-      }
-    }
-    __syncthreads();
-    if (a.planes) {
-      for (int it = tid; it < WPC * N * N; it += NT) {
-        const int p = it % N, q = (it / N) % N, w = it / (N * N);
-        const int64_t job = base + w;
-        if (job < a.njobs)
-          a.planes[job * (int64_t)(N * N) + q * N + p] = reinterpret_cast<const float*>(planes + w * PS)[q * LDR + p];
-      }
-    }
-    // ---- stage 9: peak analysis, one thread group per window
-    {
-      const int w = tid / C::G, gt = tid % C::G;
-      const int64_t job = base + w;
-      bool active = job < a.njobs;
-      int64_t gid = -1;
-      PeakOut pw = po;
-      if (active) {
-        if (a.bp) {
-          const int p = s_job[4 * w + 2];
-          active = p >= 0;
-          if (active) {
-            const BPair& b = a.bp[p];
-            const int gij = a.jobs[4 * job + 1];
-            gid = b.goff + (int64_t)(gij & 0xFFFF) + (int64_t)(gij >> 16) * b.ny;
-            pw.G = (int64_t)b.ny * b.nx;
-            pw.nalt = b.nalt;
-            pw.alt_u = a.alt_u ? a.alt_u + b.aoff - b.goff : nullptr;  // indexed by gid + m*G
-            pw.alt_v = a.alt_v ? a.alt_v + b.aoff - b.goff : nullptr;
+          for (int n1 = 0; n1 < N1; ++n1) {
+            const int qs = (N2 * n1 + n2 + H) % N;
+            Rw[qs * LDR + ps0] = rv[i][0][n1];
+            Rw[qs * LDR + ps1] = rv[i][1][n1];
           }
-        } else {
-          gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
         }
       }
-      analyze_group(reinterpret_cast<const float*>(planes + w * PS), N, N, LDR, K, a.npeaks, a.finder, a.subpixel,
-                    gt, C::G, red + w * (C::G / 32) * 2, active, s_vals + w * KMAX, s_locs + w * 2 * KMAX, gid, job,
-                    pw);
     }
-    __syncthreads();
+    grp_sync(bar, G);
+    if (a.planes) {
+      float* dst = a.planes + job * (int64_t)(N * N);
+      for (int it = gt; it < N * N; it += G) {
+        const int p = it % N, q = it / N;
+        const float r = Rw[q * LDR + p];
+        dst[q * N + p] = a.accumulate ? dst[q * N + p] + r : r;  // ensemble: per-pair planes summed in pair order
+      }
+      if (a.accumulate) {  // ensemble planes are analysed once, after the last pair
+        grp_sync(bar, G);
+        continue;
+      }
+    }
+    // ---- stage 9: peak analysis by the group
+    analyze_group(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, red + w * (G / 32) * 2, true,
+                  s_vals + w * KMAX, s_locs + w * 2 * KMAX, gid, job, pw, bad, bar);
+    grp_sync(bar, G);  // the plane is reused by the group's next window
   }
 }
 
@@ -775,12 +828,13 @@ __global__ void __launch_bounds__(128) analyze_planes_kernel(const AnalyzeArgs a
   float* s_vals = reinterpret_cast<float*>(red + 8);
   int* s_locs = reinterpret_cast<int*>(s_vals + KMAX);
   const int K = a.npeaks > 2 ? a.npeaks : 2;
-  PeakOut po{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, a.packed, a.locs};
+  PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
   for (int64_t pl = blockIdx.x; pl < a.nplanes; pl += gridDim.x) {
     for (int k = threadIdx.x; k < P; k += blockDim.x) R[k] = a.planes[pl * (int64_t)P + k];
     __syncthreads();
+    const int64_t gid = a.jobs ? (int64_t)a.jobs[4 * pl] + (int64_t)a.jobs[4 * pl + 1] * a.ny : -1;
     analyze_group(R, a.nr, a.nc, a.nr, K, a.npeaks, a.finder, a.subpixel, threadIdx.x, 128, red, true, s_vals,
-                  s_locs, -1, pl, po);
+                  s_locs, gid, pl, po, false, 0);
     __syncthreads();
   }
 }
@@ -792,6 +846,11 @@ template <int N, int W> static cudaError_t launch_nw(const CorrArgs& a, cudaStre
   static bool attr_set = false;
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(correlate_kernel<N, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    // the planes live in shared memory: ask for the largest carveout so the
+    // register budget, not the L1 split, sets the CTAs per SM
+    e = cudaFuncSetAttribute(correlate_kernel<N, W>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }

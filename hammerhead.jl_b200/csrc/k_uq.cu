@@ -227,7 +227,10 @@ __global__ void __launch_bounds__(UQ_THREADS) uq_kernel(const UQArgs a, const UQ
     }
     __syncthreads();
     if (a.stats)
-      for (int it = tid; it < 88; it += UQ_THREADS) a.stats[job * 88 + it] = stats[it];
+      for (int it = tid; it < 88; it += UQ_THREADS) {
+        if (a.accumulate) a.stats[job * 88 + it] += stats[it];
+        else a.stats[job * 88 + it] = stats[it];
+      }
     if (a.unc_u && tid < 2) {
       const float sg = uq_finalize(stats + 44 * tid, o);
       if (tid == 0) a.unc_u[gid] = sg;
@@ -421,12 +424,25 @@ __global__ void __launch_bounds__(UQW_THREADS) uq_warp_kernel(const UQArgs a, co
         for (int l = 0; l < 32; ++l) t += part[st * 33 + l];
         const int ri = st < 4 ? st : 4 + o.nat2ring[st - 4];
         tot[ri] = t;
-        if (a.stats) a.stats[job * 88 + comp * 44 + ri] = t;
+        if (a.stats) {
+          if (a.accumulate) a.stats[job * 88 + comp * 44 + ri] += t;
+          else a.stats[job * 88 + comp * 44 + ri] = t;
+        }
       }
       __syncwarp();
       if (lane == 0 && a.unc_u) (comp == 0 ? a.unc_u : a.unc_v)[gid] = uq_finalize(tot, o);
     }
     __syncthreads();  // the window buffers are reused by the next iteration
+  }
+}
+
+__global__ void uq_finalize_kernel(const double* __restrict__ stats, const int32_t* __restrict__ jobs, int64_t njobs,
+                                   int32_t ny, float* unc_u, float* unc_v, const UQOffsets o) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < 2 * njobs; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t job = k >> 1;
+    const int comp = (int)(k & 1);
+    const int64_t gid = (int64_t)jobs[4 * job] + (int64_t)jobs[4 * job + 1] * ny;
+    (comp == 0 ? unc_u : unc_v)[gid] = uq_finalize(stats + job * 88 + comp * 44, o);
   }
 }
 
@@ -475,6 +491,16 @@ cudaError_t launch_uq(const UQArgs& a, cudaStream_t s, int num_sms) {
   int64_t grid = (int64_t)per_sm * num_sms;
   if (grid > a.njobs) grid = a.njobs;
   uq_kernel<<<(unsigned)grid, UQ_THREADS, sm, s>>>(a, offs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_uq_finalize(const double* stats, const int32_t* jobs, int64_t njobs, int32_t ny, float* unc_u,
+                               float* unc_v, cudaStream_t s) {
+  if (njobs <= 0) return cudaSuccess;
+  static const UQOffsets offs = make_offsets();
+  int64_t blocks = (2 * njobs + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  uq_finalize_kernel<<<(unsigned)blocks, 256, 0, s>>>(stats, jobs, njobs, ny, unc_u, unc_v, offs);
   return cudaGetLastError();
 }
 

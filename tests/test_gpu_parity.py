@@ -7,6 +7,7 @@ kernels given identical inputs must match bit for bit.
 """
 import json
 import math
+import zlib
 import os
 
 import numpy as np
@@ -59,7 +60,7 @@ def _random_planes(rng, n, shape):
 @pytest.mark.parametrize("subpixel", ["gauss3", "gauss9", "none"])
 @pytest.mark.parametrize("npeaks", [1, 3, 5])
 def test_analyze_random_planes(ws, orc, hooks, finder, subpixel, npeaks):
-    rng = np.random.default_rng(hash((finder, subpixel, npeaks)) % 2 ** 32)
+    rng = np.random.default_rng(zlib.crc32(f"{finder}-{subpixel}-{npeaks}".encode()))
     planes = _random_planes(rng, 40, (32, 32))
     planes[3, 5:9, 5:9] = planes[3].max() + 1  # plateau
     out, locs = hooks.analyze_planes(ws, planes, n_peaks=npeaks, peak_finder=finder, subpixel_method=subpixel)
@@ -73,9 +74,12 @@ def test_analyze_random_planes(ws, orc, hooks, finder, subpixel, npeaks):
         assert out[k, 2] == ref[2] or (math.isnan(out[k, 2]) and math.isnan(ref[2]))
         np.testing.assert_allclose(out[k, 3], ref[3], rtol=1e-5, equal_nan=True)
         # alternative peaks on noise can be ill-conditioned fits (offsets of
-        # hundreds of px); FP64 vs Float32 logarithms then differ relatively
-        np.testing.assert_allclose(out[k, 5:5 + 2 * (K - 1)], ref[5:5 + 2 * (K - 1)], rtol=2e-4, atol=1e-5,
-                                   equal_nan=True)
+        # hundreds of px); FP64 vs Float32 logarithms then differ relatively,
+        # the more the further the fit lands outside the plane
+        alt, ralt = out[k, 5:5 + 2 * (K - 1)], ref[5:5 + 2 * (K - 1)]
+        inside = ~(np.abs(ralt) > 32)
+        np.testing.assert_allclose(alt[inside], ralt[inside], rtol=2e-4, atol=1e-5, equal_nan=True)
+        np.testing.assert_allclose(alt[~inside], ralt[~inside], rtol=1e-2, equal_nan=True)
 
 
 # --- correlation planes and per-window outputs ------------------------------------
