@@ -238,7 +238,7 @@ struct PeakOut {
 // Peak analysis of one plane by a group of threads (tid in [0, gsize)).
 // Every thread of the CTA must call this (uniform K and finder), because
 // the merge rounds synchronise the whole CTA.
-__device__ __forceinline__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
+__device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
                               int subpixel, int gtid, int gsize, uint32_t* red, bool active, float* s_vals,
                               int* s_locs, int64_t grid_id, int64_t job, const PeakOut& o, bool poison, int bar) {
   // a poisoned plane (non-finite window data: the reference's plane is all
@@ -805,7 +805,10 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
       for (int it = gt; it < N * N; it += G) {
         const int p = it % N, q = it / N;
         const float r = Rw[q * LDR + p];
-        dst[q * N + p] = a.accumulate ? dst[q * N + p] + r : r;  // ensemble: per-pair planes summed in pair order
+        // ensemble: per-pair planes summed in pair order; a window with
+        // non-finite data poisons its sum as the reference's NaN plane does
+        const float rr = bad ? __int_as_float(0x7fc00000) : r;
+        dst[q * N + p] = a.accumulate ? dst[q * N + p] + rr : rr;
       }
       if (a.accumulate) {  // ensemble planes are analysed once, after the last pair
         grp_sync(bar, G);

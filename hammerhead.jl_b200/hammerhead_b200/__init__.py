@@ -8,6 +8,7 @@ with the reference's public surface for the path:
     run_piv_sequence (in-memory pairs), run_piv_batch,
     BatchRunner                                             (src/io.jl; batched device schedule)
     NCCLoss                                                 (adjoint of deformation + correlation)
+    run_piv_ensemble                                        (src/ensemble.jl)
     validators: PeakRatioValidator, CorrelationMomentValidator,
                 VelocityMagnitudeValidator, UniversalOutlierValidator
     error_statistics                                        (src/statistics.jl)
@@ -23,6 +24,7 @@ from .pipeline import (PhysicalScale, PIVResult, PIVWorkspace, check_backend_par
 from . import adjoint
 from .adjoint import NCCLoss
 from .batch import BatchRunner, run_piv_batch, run_piv_sequence
+from .ensemble import run_piv_ensemble
 from .statistics import error_statistics, rms_error
 from . import synthetic
 
@@ -32,4 +34,5 @@ __all__ = [
     "VelocityMagnitudeValidator", "UniversalOutlierValidator", "PIVResult", "PIVWorkspace", "PhysicalScale",
     "piv_workspace", "run_piv", "pass_grid", "check_backend_params", "with_scale", "error_statistics", "rms_error",
     "synthetic", "BatchRunner", "run_piv_batch", "run_piv_sequence", "NCCLoss", "adjoint",
+    "run_piv_ensemble",
 ]

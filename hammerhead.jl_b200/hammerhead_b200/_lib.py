@@ -166,6 +166,9 @@ SIGNATURES = [
     ("hh_smooth_field", ctypes.c_int32, [_CTX, _F, ctypes.c_int32, ctypes.c_int32, _F]),
     ("hh_field_change", ctypes.c_int32, [_CTX, _F, _F, _F, _F, _U8, ctypes.c_int64, _F]),
     ("hh_finalize_uncertainty", ctypes.c_int32, [_D, ctypes.c_int64, _F, _F]),
+    ("hh_run_ensemble", ctypes.c_int32,
+     [_CTX, ctypes.POINTER(hh_batch_pair), ctypes.c_int32, _PASS, ctypes.c_int32, _U8, ctypes.c_double,
+      ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(hh_result)]),
     ("hh_ncc_loss_grad", ctypes.c_int32,
      [_CTX, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
       ctypes.c_float, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),

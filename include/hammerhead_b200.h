@@ -186,6 +186,19 @@ hh_status hh_run_batched(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npairs
                          const int32_t* schedule_offsets, int32_t nschedules, double mask_threshold,
                          int32_t predictor_smoothing, int32_t flags, hh_batch_result* out);
 
+/* ---- Ensemble (sum-of-correlation) PIV -----------------------------------
+ * Replaces run_piv_ensemble (src/ensemble.jl:51-205): per pass, every pair
+ * is deformed by the shared predictor, each window's correlation planes are
+ * summed over the pairs on the device (in pair order) and analysed once; the
+ * uncertainty statistics pool by summation; one sweep per pass. Pairs share
+ * one image size; pairs[q].schedule is ignored. mask is a HOST image mask
+ * (or NULL) shared by every pair. Images are host pointers, or device
+ * pointers with HH_BATCH_DEVICE_INPUTS. The final pass is returned in *out
+ * (grid dims from hh_pass_grid of the final pass). */
+hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npairs, const hh_pass_desc* passes,
+                          int32_t npasses, const uint8_t* mask, double mask_threshold,
+                          int32_t predictor_smoothing, int32_t flags, hh_result* out);
+
 /* ---- Differentiation: adjoint of deformation + correlation -------------
  *
  * No counterpart in the reference: a correlation loss of the predictor

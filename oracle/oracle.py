@@ -401,3 +401,43 @@ def ncc_loss_grad(coefA, coefB, shape, P, grid, window=16, overlap=8, windows=No
     out[..., 0] = np.reshape(g[:G], (gny, gnx), order="F")
     out[..., 1] = np.reshape(g[G:], (gny, gnx), order="F")
     return L, out
+
+
+def run_ensemble(pairs, passes, mask=None, mask_threshold=0.5, predictor_smoothing=True, nthreads=1,
+                 dtype=np.float32):
+    """run_piv_ensemble on the CPU: pairs is a list of (A, B) of one size;
+    returns the final pass as a dict of grids like run_piv."""
+    T, ct, suf = _T(dtype)
+    if not isinstance(passes, (list, tuple)):
+        passes = [passes]
+    imgs = [(np.asfortranarray(A, T), np.asfortranarray(B, T)) for A, B in pairs]
+    nr, nc = imgs[0][0].shape
+    ny, nx, _, _ = pass_grid((nr, nc), passes[-1], mask, mask_threshold)
+    out = {k: np.empty((ny, nx), T, order="F") for k in
+           ("u", "v", "peak_ratio", "correlation_moment", "uncertainty_u", "uncertainty_v")}
+    out["x"] = np.empty(nx, T)
+    out["y"] = np.empty(ny, T)
+    outl = np.empty((ny, nx), np.uint8, order="F")
+    gm = np.empty((ny, nx), np.uint8, order="F")
+
+    class Res(ctypes.Structure):
+        _fields_ = [("ny", ctypes.c_int32), ("nx", ctypes.c_int32)] + [
+            (k, ctypes.POINTER(ct)) for k in ("x", "y", "u", "v", "peak_ratio", "moment", "unc_u", "unc_v")] + [
+            ("outliers", ctypes.POINTER(ctypes.c_uint8)), ("mask", ctypes.POINTER(ctypes.c_uint8))]
+
+    res = Res(0, 0, _p(out["x"], ct), _p(out["y"], ct), _p(out["u"], ct), _p(out["v"], ct),
+              _p(out["peak_ratio"], ct), _p(out["correlation_moment"], ct), _p(out["uncertainty_u"], ct),
+              _p(out["uncertainty_v"], ct), _u8(outl), _u8(gm))
+    PT = ctypes.POINTER(ct)
+    As = (PT * len(imgs))(*[_p(a, ct) for a, _ in imgs])
+    Bs = (PT * len(imgs))(*[_p(b, ct) for _, b in imgs])
+    descs = (Pass * len(passes))(*[to_pass(p) for p in passes])
+    m = None if mask is None else np.asfortranarray(mask, np.uint8)
+    st = _fn("run_ensemble", suf)(As, Bs, len(imgs), ctypes.c_int64(nr), ctypes.c_int64(nc), descs, len(passes),
+                                  _u8(m), ctypes.c_double(mask_threshold), int(bool(predictor_smoothing)),
+                                  int(nthreads), ctypes.byref(res))
+    if st != 0:
+        raise ValueError("oracle run_ensemble rejected the arguments")
+    out["outliers"] = outl.astype(bool)
+    out["mask"] = gm.astype(bool)
+    return out

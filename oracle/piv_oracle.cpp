@@ -1592,6 +1592,168 @@ static int run_piv(const T* A, const T* B, i64 nr, i64 nc, const Pass* passes, i
   return 0;
 }
 
+// run_piv_ensemble (src/ensemble.jl:51-205): per pass, every pair is
+// deformed by the shared predictor, each window's correlation planes are
+// summed over the pairs in pair order (accumulate_planes!, :310-343) and
+// analysed once (ensemble_analyze!, :273-305); the Wieneke statistics pool
+// by summation; then validate_and_replace! with replacement forced on
+// intermediate passes. One sweep per pass (max_iterations is not used).
+template <class T>
+static int run_ensemble(const T* const* As, const T* const* Bs, int npairs, i64 nr, i64 nc, const Pass* passes,
+                        int npasses, const uint8_t* mask, double mask_thr, bool smoothing, int nthreads,
+                        Result<T>& res) {
+  std::vector<T> CA, CB, wA, wB;
+  bool have_pred = false;
+  std::vector<T> pred_u, pred_v;
+  Predictor pg;
+  Result<T> cur;
+  const T NaN = std::numeric_limits<T>::quiet_NaN();
+  for (int k = 0; k < npasses; ++k) {
+    const Pass& p = passes[k];
+    const bool force_replace = k < npasses - 1;
+    if (k > 0) {
+      std::vector<T> pu = cur.u, pv = cur.v;
+      bool anym = false;
+      for (auto m : cur.grid.gmask) anym |= m != 0;
+      if (anym) replace_vectors(pu.data(), pv.data(), cur.grid.ny, cur.grid.nx, cur.grid.gmask.data());
+      if (smoothing) {
+        pred_u.resize(pu.size());
+        pred_v.resize(pv.size());
+        smooth_field(pu.data(), cur.grid.ny, cur.grid.nx, pred_u.data());
+        smooth_field(pv.data(), cur.grid.ny, cur.grid.nx, pred_v.data());
+      } else {
+        pred_u = pu;
+        pred_v = pv;
+      }
+      pg.gny = cur.grid.ny;
+      pg.gnx = cur.grid.nx;
+      pg.y0 = cur.y[0];
+      pg.x0 = cur.x[0];
+      pg.ysp = cur.grid.ny > 1 ? (double)(cur.y[1] - cur.y[0]) : 1.0;
+      pg.xsp = cur.grid.nx > 1 ? (double)(cur.x[1] - cur.x[0]) : 1.0;
+      have_pred = true;
+    }
+    Result<T> r;
+    if (make_grid(nr, nc, p, mask, mask_thr, r.grid) != 0) return -1;
+    const int ny = r.grid.ny, nx = r.grid.nx;
+    const i64 G = (i64)ny * nx;
+    r.x.resize(nx);
+    r.y.resize(ny);
+    for (int j = 0; j < nx; ++j) r.x[j] = (T)(r.grid.cols[j] + (p.window[1] - 1) / 2.0);
+    for (int i = 0; i < ny; ++i) r.y[i] = (T)(r.grid.rows[i] + (p.window[0] - 1) / 2.0);
+    const i64 njobs = (i64)r.grid.jobs.size() / 4;
+    const int nalt = p.n_peaks - 1, K = std::max(p.n_peaks, 2);
+    const bool unc = p.uncertainty && !force_replace;
+    // node values of the shared predictor (zero without one)
+    std::vector<T> u(G, T(0)), v(G, T(0));
+    if (have_pred)
+      for (int gj = 0; gj < nx; ++gj)
+        for (int gi = 0; gi < ny; ++gi) {
+          u[gi + (i64)gj * ny] =
+              bilinear(pred_u.data(), pg.gny, pg.gnx, (T)pg.y0, (T)pg.ysp, (T)pg.x0, (T)pg.xsp, r.y[gi], r.x[gj]);
+          v[gi + (i64)gj * ny] =
+              bilinear(pred_v.data(), pg.gny, pg.gnx, (T)pg.y0, (T)pg.ysp, (T)pg.x0, (T)pg.xsp, r.y[gi], r.x[gj]);
+        }
+    int nch = (int)std::max<i64>(1, std::min<i64>(nthreads, njobs));
+    std::vector<Correlator<T>*> cors;
+    for (int t = 0; t < nch; ++t) cors.push_back(new Correlator<T>(p));
+    const i64 PN = (i64)cors[0]->nr * cors[0]->nc;
+    std::vector<T> acc((size_t)std::max<i64>(njobs, 1) * PN, T(0));
+    std::vector<double> uacc(unc ? (size_t)njobs * 88 : 0, 0.0);
+    std::vector<T> apod((size_t)p.window[0] * p.window[1]);
+    apodization_window(p.window[0], p.window[1], p.apod, apod.data());
+    const int wr = p.window[0], wc = p.window[1];
+    const int mr = (p.search[0] - wr) / 2, mc = (p.search[1] - wc) / 2;
+    for (int q = 0; q < npairs; ++q) {
+      const T* srcA = As[q];
+      const T* srcB = Bs[q];
+      if (have_pred) {
+        CA.resize((size_t)(nr + 2) * (nc + 2));
+        CB.resize((size_t)(nr + 2) * (nc + 2));
+        wA.resize((size_t)nr * nc);
+        wB.resize((size_t)nr * nc);
+        std::thread ta([&]() { prefilter(As[q], nr, nc, CA.data()); });
+        prefilter(Bs[q], nr, nc, CB.data());
+        ta.join();
+        parallel_for(nthreads, nc, [&](int, i64 a, i64 b) {
+          deform_columns(CA.data(), CB.data(), nr, nc, pred_u.data(), pred_v.data(), pg, wA.data(), wB.data(), a, b);
+        });
+        srcA = wA.data();
+        srcB = wB.data();
+      }
+      const i64 chunk = (njobs + nch - 1) / std::max(nch, 1);
+      parallel_for(nch, nch, [&](int, i64 a, i64 b) {
+        for (i64 t = a; t < b; ++t) {
+          const i64 j0 = t * chunk, j1 = std::min(njobs, j0 + chunk);
+          for (i64 j = j0; j < j1; ++j) {
+            const int* jb = r.grid.jobs.data() + 4 * j;
+            const int rs = jb[2] - 1, cs = jb[3] - 1;
+            const T* subA = srcA + rs + (i64)cs * nr;
+            const T* subB = srcB + (rs - mr) + (i64)(cs - mc) * nr;
+            const uint8_t* mA = nullptr;
+            const uint8_t* mB = nullptr;
+            if (mask) {
+              mA = mask + rs + (i64)cs * nr;
+              bool any = false;
+              for (int jj = 0; jj < wc && !any; ++jj)
+                for (int ii = 0; ii < wr; ++ii)
+                  if (mA[ii + (i64)jj * nr]) { any = true; break; }
+              if (!any) mA = nullptr;
+              mB = mA;
+            }
+            const T* R = correlation_plane(*cors[t], subA, subB, nr, mA, mB, nr);
+            T* dst = acc.data() + j * PN;
+            for (i64 e = 0; e < PN; ++e) dst[e] += R[e];
+            if (unc) {
+              double st[88] = {0};
+              uq_window_stats(st, subA, srcB + rs + (i64)cs * nr, nr, mA, nr, wr, wc, apod.data());
+              for (int e = 0; e < 88; ++e) uacc[j * 88 + e] += st[e];
+            }
+          }
+        }
+      });
+    }
+    std::vector<T> ratio(G, T(0)), moment(G, T(0));
+    std::vector<T> altu(nalt > 0 ? G * nalt : 0, NaN), altv(nalt > 0 ? G * nalt : 0, NaN);
+    r.unc_u.assign(G, NaN);
+    r.unc_v.assign(G, NaN);
+    std::vector<T> out(5 + 2 * (K - 1));
+    for (i64 j = 0; j < njobs; ++j) {
+      const int gi = r.grid.jobs[4 * j], gj = r.grid.jobs[4 * j + 1];
+      const i64 id = gi + (i64)gj * ny;
+      analyze_plane(acc.data() + j * PN, cors[0]->nr, cors[0]->nc, p.n_peaks, p.finder, p.subpixel, out.data(),
+                    (int*)nullptr);
+      const int found = (int)out[4];
+      for (int m = 2; m <= std::min(found, p.n_peaks); ++m) {
+        altu[id + (i64)(m - 2) * G] = u[id] + out[5 + (m - 2)];
+        altv[id + (i64)(m - 2) * G] = v[id] + out[5 + (K - 1) + (m - 2)];
+      }
+      u[id] += out[0];
+      v[id] += out[1];
+      ratio[id] = out[2];
+      moment[id] = out[3];
+      if (unc) {
+        r.unc_u[id] = finalize_uq<T>(uacc.data() + j * 88);
+        r.unc_v[id] = finalize_uq<T>(uacc.data() + j * 88 + 44);
+      }
+    }
+    for (i64 q = 0; q < G; ++q)
+      if (r.grid.gmask[q]) u[q] = v[q] = ratio[q] = moment[q] = NaN;
+    std::vector<uint8_t> outl(G, 0);
+    validate_and_replace(u.data(), v.data(), ratio.data(), moment.data(), outl.data(), r.grid.gmask.data(), ny, nx, p,
+                         force_replace, nalt > 0 ? altu.data() : nullptr, nalt > 0 ? altv.data() : nullptr, nalt);
+    for (auto* c : cors) delete c;
+    r.u = u;
+    r.v = v;
+    r.ratio = ratio;
+    r.moment = moment;
+    r.outliers = outl;
+    cur = std::move(r);
+  }
+  res = std::move(cur);
+  return 0;
+}
+
 }  // namespace orc
 
 // ===========================================================================
@@ -1773,6 +1935,30 @@ ORC_DEFINE(double, f64)
   }
 ORC_NCC(float, f32)
 ORC_NCC(double, f64)
+
+#define ORC_ENS(T, SUF)                                                                                              \
+  int orc_run_ensemble_##SUF(const T* const* As, const T* const* Bs, int npairs, int64_t nr, int64_t nc,            \
+                             const orc::Pass* passes, int npasses, const uint8_t* mask, double thr, int smoothing,  \
+                             int nthreads, orc_result_##SUF* out) {                                                  \
+    orc::Result<T> r;                                                                                                \
+    if (orc::run_ensemble<T>(As, Bs, npairs, nr, nc, passes, npasses, mask, thr, smoothing != 0, nthreads, r) != 0) \
+      return -1;                                                                                                     \
+    out->ny = r.grid.ny;                                                                                             \
+    out->nx = r.grid.nx;                                                                                             \
+    if (out->x) std::copy(r.x.begin(), r.x.end(), out->x);                                                           \
+    if (out->y) std::copy(r.y.begin(), r.y.end(), out->y);                                                           \
+    if (out->u) std::copy(r.u.begin(), r.u.end(), out->u);                                                           \
+    if (out->v) std::copy(r.v.begin(), r.v.end(), out->v);                                                           \
+    if (out->peak_ratio) std::copy(r.ratio.begin(), r.ratio.end(), out->peak_ratio);                                 \
+    if (out->moment) std::copy(r.moment.begin(), r.moment.end(), out->moment);                                       \
+    if (out->unc_u) std::copy(r.unc_u.begin(), r.unc_u.end(), out->unc_u);                                           \
+    if (out->unc_v) std::copy(r.unc_v.begin(), r.unc_v.end(), out->unc_v);                                           \
+    if (out->outliers) std::copy(r.outliers.begin(), r.outliers.end(), out->outliers);                               \
+    if (out->mask) std::copy(r.grid.gmask.begin(), r.grid.gmask.end(), out->mask);                                   \
+    return 0;                                                                                                        \
+  }
+ORC_ENS(float, f32)
+ORC_ENS(double, f64)
 
 void orc_uq_offsets(int32_t* out /*40x2*/, int32_t* ring_start /*5*/) {
   orc::uq_init();
