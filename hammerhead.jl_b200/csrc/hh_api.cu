@@ -169,6 +169,8 @@ hh_status run_schedule(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr
       ca.apod = tb.apod;
       ca.gain = tb.gain;
       ca.phasew = tb.phasew;
+      ca.box_lo = tb.box_lo;
+      ca.box_hi = tb.box_hi;
       ca.method = p.method;
       ca.npeaks = p.n_peaks;
       ca.finder = p.peak_finder;
@@ -664,6 +666,8 @@ static hh_status hook_correlate(hh_ctx* ctx, const hh_pass_desc* p, const int32_
   ca.apod = tb.apod;
   ca.gain = tb.gain;
   ca.phasew = tb.phasew;
+  ca.box_lo = tb.box_lo;
+  ca.box_hi = tb.box_hi;
   ca.method = p->method;
   ca.npeaks = p->n_peaks;
   ca.finder = p->peak_finder;

@@ -53,6 +53,7 @@ struct BPlan {
   uint8_t* d_gmask = nullptr;
   float *warpA = nullptr, *warpB = nullptr, *coefA = nullptr, *coefB = nullptr, *dbuf = nullptr;
   float *stageA = nullptr, *stageB = nullptr;
+  uint16_t *stage16A = nullptr, *stage16B = nullptr;  // host UInt16 frames before conversion
   uint8_t* stageM = nullptr;
   hh::BGrid g{};
   hh::BResult r{};
@@ -104,6 +105,8 @@ static hh_status check_batch(hh_ctx* ctx, const hh_batch_pair* pairs, int npairs
       return fail(ctx, HH_ERR_ARG, "pair " + std::to_string(p + 1) + ": schedule index out of range");
     if (q.nr < 1 || q.nc < 1) return fail(ctx, HH_ERR_ARG, "images must be non-empty");
     if (!q.A || !q.B) return fail(ctx, HH_ERR_ARG, "pair " + std::to_string(p + 1) + ": image pointer is NULL");
+    if (q.format < HH_PIX_F32 || q.format > HH_PIX_U16_RAW)
+      return fail(ctx, HH_ERR_ARG, "pair " + std::to_string(p + 1) + ": unknown pixel format " + std::to_string(q.format));
   }
   return HH_OK;
 }
@@ -123,6 +126,7 @@ static std::string plan_key(const hh_batch_pair* pairs, int npairs, const hh_pas
     put(&pairs[p].schedule, 4);
     const int hm = pairs[p].mask != nullptr;
     put(&hm, 4);
+    put(&pairs[p].format, 4);
   }
   for (int i = 0; i < so[nsched]; ++i) {
     hh_pass_desc d = passes[i];
@@ -403,6 +407,8 @@ static hh_status issue(hh_ctx* ctx, BPlan& P) {
         ca.apod = c.tb.apod;
         ca.gain = c.tb.gain;
         ca.phasew = c.tb.phasew;
+        ca.box_lo = c.tb.box_lo;
+        ca.box_hi = c.tb.box_hi;
         ca.method = c.method;
         ca.npeaks = c.npeaks;
         ca.finder = c.finder;
@@ -503,24 +509,47 @@ static hh_status stage_inputs(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs,
   cudaStream_t s = ctx->stream;
   const int np = P.npairs;
   const bool any_mask = P.d_gmask != nullptr;
-  if (!device_inputs) {
-    if (!P.stageA) {
-      HH_TRY(plan_alloc(ctx, P, P.itot, &P.stageA));
-      HH_TRY(plan_alloc(ctx, P, P.itot, &P.stageB));
-      if (any_mask) HH_TRY(plan_alloc(ctx, P, P.itot, &P.stageM));
+  bool any_u16 = false;
+  for (int p = 0; p < np; ++p) any_u16 |= pairs[p].format != HH_PIX_F32;
+  if ((!device_inputs || any_u16) && !P.stageA) {
+    HH_TRY(plan_alloc(ctx, P, P.itot, &P.stageA));
+    HH_TRY(plan_alloc(ctx, P, P.itot, &P.stageB));
+  }
+  if (!device_inputs && any_mask && !P.stageM) HH_TRY(plan_alloc(ctx, P, P.itot, &P.stageM));
+  if (!device_inputs && any_u16 && !P.stage16A) {
+    HH_TRY(plan_alloc(ctx, P, P.itot, &P.stage16A));
+    HH_TRY(plan_alloc(ctx, P, P.itot, &P.stage16B));
+  }
+  for (int p = 0; p < np; ++p) {
+    const size_t n = (size_t)(pairs[p].nr * pairs[p].nc);
+    const int fmt = pairs[p].format;
+    if (fmt == HH_PIX_F32) {
+      if (!device_inputs) {
+        HH_CK(cudaMemcpyAsync(P.stageA + P.ioff[p], pairs[p].A, n * sizeof(float), cudaMemcpyHostToDevice, s));
+        HH_CK(cudaMemcpyAsync(P.stageB + P.ioff[p], pairs[p].B, n * sizeof(float), cudaMemcpyHostToDevice, s));
+      }
+    } else {  // UInt16 frames: (copy and) convert into the float staging
+      const uint16_t* a16 = reinterpret_cast<const uint16_t*>(pairs[p].A);
+      const uint16_t* b16 = reinterpret_cast<const uint16_t*>(pairs[p].B);
+      if (!device_inputs) {
+        HH_CK(cudaMemcpyAsync(P.stage16A + P.ioff[p], a16, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        HH_CK(cudaMemcpyAsync(P.stage16B + P.ioff[p], b16, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        a16 = P.stage16A + P.ioff[p];
+        b16 = P.stage16B + P.ioff[p];
+      }
+      const int norm = fmt == HH_PIX_U16;
+      HH_K(HH_K_PREFILTER, 2, 0, 12.0 * n, (int64_t)n, hh::launch_u16_to_f32(a16, (int64_t)n, norm, P.stageA + P.ioff[p], s));
+      HH_K(HH_K_PREFILTER, 0, 0, 0, 0, hh::launch_u16_to_f32(b16, (int64_t)n, norm, P.stageB + P.ioff[p], s));
     }
-    for (int p = 0; p < np; ++p) {
-      const size_t n = (size_t)(pairs[p].nr * pairs[p].nc);
-      HH_CK(cudaMemcpyAsync(P.stageA + P.ioff[p], pairs[p].A, n * sizeof(float), cudaMemcpyHostToDevice, s));
-      HH_CK(cudaMemcpyAsync(P.stageB + P.ioff[p], pairs[p].B, n * sizeof(float), cudaMemcpyHostToDevice, s));
-      if (pairs[p].mask) HH_CK(cudaMemcpyAsync(P.stageM + P.ioff[p], pairs[p].mask, n, cudaMemcpyHostToDevice, s));
-    }
+    if (!device_inputs && pairs[p].mask)
+      HH_CK(cudaMemcpyAsync(P.stageM + P.ioff[p], pairs[p].mask, n, cudaMemcpyHostToDevice, s));
   }
   std::vector<uint8_t> hmask;
   for (int p = 0; p < np; ++p) {
     const hh_batch_pair& q = pairs[p];
-    const float* A = device_inputs ? q.A : P.stageA + P.ioff[p];
-    const float* B = device_inputs ? q.B : P.stageB + P.ioff[p];
+    const bool staged = !device_inputs || q.format != HH_PIX_F32;
+    const float* A = staged ? P.stageA + P.ioff[p] : q.A;
+    const float* B = staged ? P.stageB + P.ioff[p] : q.B;
     const uint8_t* M = q.mask ? (device_inputs ? q.mask : P.stageM + P.ioff[p]) : nullptr;
     const uint8_t* hm = nullptr;
     if (q.mask) {

@@ -37,6 +37,7 @@ struct Tables {
   float* apod = nullptr;
   float* gain = nullptr;
   float* phasew = nullptr;
+  int box_lo = 0, box_hi = 0;  // support of the gain in fftshifted rows/columns (0, 0: whole plane)
 };
 
 }  // namespace hhd
@@ -246,6 +247,18 @@ inline hh_status get_tables(hh_ctx* ctx, const hh_pass_desc& p, Tables& t) {
   HH_CK(cudaMemcpy(nt.apod, ap.data(), ap.size() * sizeof(float), cudaMemcpyHostToDevice));
   if (p.padding) {
     gain_table(W, ap, gn);
+    // bounding box of the nonzero gain (square and centred, by symmetry)
+    int lo = N, hi = -1;
+    for (int q = 0; q < N; ++q)
+      for (int r = 0; r < N; ++r)
+        if (gn[r + (size_t)q * N] != 0.f) {
+          lo = std::min(lo, std::min(r, q));
+          hi = std::max(hi, std::max(r, q));
+        }
+    if (hi > 0) {
+      nt.box_lo = lo;
+      nt.box_hi = hi;
+    }
     HH_CK(cudaMalloc(&nt.gain, gn.size() * sizeof(float)));
     HH_CK(cudaMemcpy(nt.gain, gn.data(), gn.size() * sizeof(float), cudaMemcpyHostToDevice));
   }

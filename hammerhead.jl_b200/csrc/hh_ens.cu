@@ -25,6 +25,8 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
                                        std::to_string(nc) + "), got (" + std::to_string(pairs[q].nr) + ", " +
                                        std::to_string(pairs[q].nc) + ")");
     if (!pairs[q].A || !pairs[q].B) return fail(ctx, HH_ERR_ARG, "image pointer is NULL");
+    if (pairs[q].format < HH_PIX_F32 || pairs[q].format > HH_PIX_U16_RAW)
+      return fail(ctx, HH_ERR_ARG, "unknown pixel format " + std::to_string(pairs[q].format));
   }
   const bool device_inputs = (flags & HH_BATCH_DEVICE_INPUTS) != 0;
   cudaStream_t s = ctx->stream;
@@ -43,9 +45,16 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
   float *dA = nullptr, *dB = nullptr, *coefA, *coefB, *warpA, *warpB, *acc;
   uint8_t* dmask = nullptr;
   double* stats;
-  if (!device_inputs) {
+  bool any_u16 = false;
+  for (int q = 0; q < npairs; ++q) any_u16 |= pairs[q].format != HH_PIX_F32;
+  uint16_t *d16A = nullptr, *d16B = nullptr;
+  if (!device_inputs || any_u16) {
     HH_TRY(buf(ctx, "ens_A", (size_t)P, &dA));
     HH_TRY(buf(ctx, "ens_B", (size_t)P, &dB));
+  }
+  if (!device_inputs && any_u16) {
+    HH_TRY(buf(ctx, "ens_A16", (size_t)P, &d16A));
+    HH_TRY(buf(ctx, "ens_B16", (size_t)P, &d16B));
   }
   if (hmask) {
     HH_TRY(buf(ctx, "ens_mask", (size_t)P, &dmask));
@@ -149,7 +158,21 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
     for (int q = 0; q < npairs; ++q) {
       const float* A = pairs[q].A;
       const float* B = pairs[q].B;
-      if (!device_inputs) {
+      if (pairs[q].format != HH_PIX_F32) {  // UInt16 frames: (copy and) convert on the device
+        const uint16_t* a16 = reinterpret_cast<const uint16_t*>(A);
+        const uint16_t* b16 = reinterpret_cast<const uint16_t*>(B);
+        if (!device_inputs) {
+          HH_CK(cudaMemcpyAsync(d16A, a16, P * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+          HH_CK(cudaMemcpyAsync(d16B, b16, P * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+          a16 = d16A;
+          b16 = d16B;
+        }
+        const int norm = pairs[q].format == HH_PIX_U16;
+        HH_K(HH_K_PREFILTER, 2, 0, 12.0 * P, P, hh::launch_u16_to_f32(a16, P, norm, dA, s));
+        HH_K(HH_K_PREFILTER, 0, 0, 0, 0, hh::launch_u16_to_f32(b16, P, norm, dB, s));
+        A = dA;
+        B = dB;
+      } else if (!device_inputs) {
         HH_CK(cudaMemcpyAsync(dA, A, P * sizeof(float), cudaMemcpyHostToDevice, s));
         HH_CK(cudaMemcpyAsync(dB, B, P * sizeof(float), cudaMemcpyHostToDevice, s));
         A = dA;
@@ -175,6 +198,8 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
         ca.apod = tb.apod;
         ca.gain = tb.gain;
         ca.phasew = tb.phasew;
+        ca.box_lo = tb.box_lo;
+        ca.box_hi = tb.box_hi;
         ca.method = p.method;
         ca.npeaks = p.n_peaks;
         ca.finder = p.peak_finder;

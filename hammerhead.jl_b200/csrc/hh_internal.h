@@ -43,6 +43,9 @@ struct CorrArgs {
   int32_t it;
   // ensemble mode: planes += R (planes != nullptr) and no peak analysis
   int32_t accumulate;
+  // fftshifted rows/columns [box_lo, box_hi] outside which the overlap gain
+  // is zero (box_hi == 0: the whole plane)
+  int32_t box_lo, box_hi;
 };
 
 // Launch the correlation kernel for FFT size N (square) and window W.
@@ -105,6 +108,10 @@ cudaError_t launch_field_change(const float* u, const float* v, const float* pu,
 cudaError_t launch_restore_measured(float* u, float* v, const float* meas_u, const float* meas_v,
                                     const uint8_t* outl, int64_t G, cudaStream_t s);
 cudaError_t launch_fill(float* p, float value, int64_t n, cudaStream_t s);
+
+// --- ingestion -------------------------------------------------------------------
+// UInt16 frame -> float32: value / 65535 (normalise) or value * 1
+cudaError_t launch_u16_to_f32(const uint16_t* src, int64_t n, int32_t normalise, float* dst, cudaStream_t s);
 
 // --- uncertainty -------------------------------------------------------------
 struct UQArgs {

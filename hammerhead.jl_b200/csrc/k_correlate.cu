@@ -45,8 +45,10 @@ struct TopK {
   uint32_t hi[KMAX];
   uint32_t lo[KMAX];
   int cnt;
+  uint32_t thr;  // key of the K-th entry once the list is full, else 0
   __device__ __forceinline__ void init() {
     cnt = 0;
+    thr = 0u;
 #pragma unroll
     for (int m = 0; m < KMAX; ++m) hi[m] = lo[m] = 0u;
   }
@@ -85,6 +87,7 @@ struct TopK {
       cl = better ? tl : cl;
     }
     if (cnt < K) ++cnt;
+    if (cnt == K) thr = last_hi(K);
   }
   __device__ __forceinline__ void pop() {
 #pragma unroll
@@ -94,6 +97,7 @@ struct TopK {
     }
     hi[KMAX - 1] = lo[KMAX - 1] = 0u;
     if (cnt > 0) --cnt;
+    thr = 0u;
   }
 };
 
@@ -153,25 +157,21 @@ __device__ __forceinline__ void group_argmax(uint32_t hi, uint32_t lo, uint32_t*
 
 // subpixel_gauss3 (src/correlators.jl:499-520) with FP64 logarithms.
 // (i, j) 0-based; returns 1-based refined (row, col).
+// One axis: (ln Im - ln Ip) / (2 (ln Im - 2 ln I0 + ln Ip)), formed as
+// ln(Im/Ip) / (2 ln(Im Ip / I0^2)) with the ratios in FP64 (exact products
+// of floats, one rounding each): two logarithms instead of three.
+__device__ __forceinline__ double gauss3_axis(float Im, float I0, float Ip) {
+  if (!(Im > 0.f && I0 > 0.f && Ip > 0.f)) return 0.0;
+  const double m = (double)Im, z = (double)I0, p = (double)Ip;
+  const double den = log((m * p) / (z * z));
+  return den != 0.0 ? log(m / p) / (2.0 * den) : 0.0;
+}
+
 __device__ __forceinline__ void gauss3_fp64(const float* R, int nr, int nc, int ldr, int i, int j, float* out) {
   double di = 0.0, dj = 0.0;
   const float I0 = R[j * ldr + i];
-  if (i > 0 && i < nr - 1) {
-    float Im = R[j * ldr + i - 1], Ip = R[j * ldr + i + 1];
-    if (Im > 0.f && I0 > 0.f && Ip > 0.f) {
-      double lm = log((double)Im), l0 = log((double)I0), lp = log((double)Ip);
-      double den = lm - 2.0 * l0 + lp;
-      di = den != 0.0 ? (lm - lp) / (2.0 * den) : 0.0;
-    }
-  }
-  if (j > 0 && j < nc - 1) {
-    float Im = R[(j - 1) * ldr + i], Ip = R[(j + 1) * ldr + i];
-    if (Im > 0.f && I0 > 0.f && Ip > 0.f) {
-      double lm = log((double)Im), l0 = log((double)I0), lp = log((double)Ip);
-      double den = lm - 2.0 * l0 + lp;
-      dj = den != 0.0 ? (lm - lp) / (2.0 * den) : 0.0;
-    }
-  }
+  if (i > 0 && i < nr - 1) di = gauss3_axis(R[j * ldr + i - 1], I0, R[j * ldr + i + 1]);
+  if (j > 0 && j < nc - 1) dj = gauss3_axis(R[(j - 1) * ldr + i], I0, R[(j + 1) * ldr + i]);
   out[0] = (float)((double)(i + 1) + di);
   out[1] = (float)((double)(j + 1) + dj);
 }
@@ -238,9 +238,14 @@ struct PeakOut {
 // Peak analysis of one plane by a group of threads (tid in [0, gsize)).
 // Every thread of the CTA must call this (uniform K and finder), because
 // the merge rounds synchronise the whole CTA.
+// Only the box rows [rlo, rhi] x columns [clo, chi] can hold positive
+// values (outside it the overlap gain is zero, so R is exactly 0 there); the
+// scans cover it, plus the last pixel, the only place outside where a zero
+// can be a regional maximum (every other pixel has a later neighbour >= 0).
 __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
                               int subpixel, int gtid, int gsize, uint32_t* red, bool active, float* s_vals,
-                              int* s_locs, int64_t grid_id, int64_t job, const PeakOut& o, bool poison, int bar) {
+                              int* s_locs, int64_t grid_id, int64_t job, const PeakOut& o, bool poison, int bar,
+                              int rlo, int rhi, int clo, int chi) {
   // a poisoned plane (non-finite window data: the reference's plane is all
   // NaN there) yields no peak, so every output is NaN
   const bool scan = active && !poison;
@@ -257,12 +262,13 @@ __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int l
     TopK tk;
     tk.init();
     if (scan) {
-      const int S = gsize / nc > 0 ? gsize / nc : 1;  // row segments per column
-      const int rps = (nr + S - 1) / S;
+      const int bw = chi - clo + 1, bh = rhi - rlo + 1;  // box columns, rows
+      const int S = gsize / bw > 0 ? gsize / bw : 1;    // row segments per column
+      const int rps = (bh + S - 1) / S;
       const float NaNf = __int_as_float(0x7fc00000);
-      for (int strip = gtid; strip < nc * S; strip += gsize) {
-        const int c = strip % nc, seg = strip / nc;
-        const int r0 = seg * rps, r1 = min(nr, r0 + rps);
+      for (int strip = gtid; strip < bw * S; strip += gsize) {
+        const int c = clo + strip % bw, seg = strip / bw;
+        const int r0 = rlo + seg * rps, r1 = min(rhi + 1, r0 + rps);
         if (r0 >= r1) continue;
         const float* Cl = c > 0 ? R + (c - 1) * ldr : nullptr;
         const float* Cc = R + c * ldr;
@@ -285,7 +291,7 @@ __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int l
           if (!isnan(v)) {
             const uint32_t h = fkey(v);
             // a later index cannot win a tie, so a full list rejects h <= last
-            if (tk.cnt < K || h > tk.last_hi(K)) {
+            if (h > tk.thr) {
               const float e = fmaxf(fmaxf(lt, lm), fmaxf(lb, ct));
               const float l = fmaxf(fmaxf(rt, rm), fmaxf(rb, cb));
               if (!(e > v) && !(l >= v)) tk.insert(h, ~(uint32_t)(r + c * nr), K);
@@ -294,6 +300,10 @@ __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int l
           lt = lm; ct = cm; rt = rm;
           lm = lb; cm = cb; rm = rb;
         }
+      }
+      if (gtid == 0 && (rhi < nr - 1 || chi < nc - 1)) {  // the last pixel, outside the box
+        const int r = nr - 1, c = nc - 1;
+        if (is_local_max(R, nr, nc, ldr, r, c, R[c * ldr + r])) tk.insert(fkey(R[c * ldr + r]), ~(uint32_t)(r + c * nr), K);
       }
     }
     bool done = false;
@@ -314,22 +324,29 @@ __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int l
     // exclusion finder (src/correlators.jl:390-421): K scans, box +-2
     bool done = false;
     for (int round = 0; round < K; ++round) {  // every round runs: group_argmax synchronises the group
-      uint32_t bh = 0u, bl = 0u;
-      if (scan && !done) {
-        for (int lin = gtid; lin < P; lin += gsize) {
-          const int r = lin % nr, c = lin / nr;
-          bool ex = false;
-          for (int q = 0; q < nfound; ++q)
-            if (abs(r - s_locs[2 * q]) <= 2 && abs(c - s_locs[2 * q + 1]) <= 2) { ex = true; break; }
-          if (ex) continue;
-          const float v = R[c * ldr + r];
-          if (!(v > -INFINITY)) continue;  // NaN and -Inf never beat the initial -Inf
-          const uint32_t h = fkey(v), l = ~(uint32_t)lin;
-          if (h > bh || (h == bh && l > bl)) { bh = h; bl = l; }
+      // the box first; when its best is not positive the maximum can lie
+      // outside it (a zero earlier in column-major order), so rescan all
+      uint32_t whi = 0u, wlo = 0u;
+      for (int pass = 0; pass < 2; ++pass) {
+        const int bw = chi - clo + 1, bht = rhi - rlo + 1;
+        const int n = pass == 0 ? bw * bht : P;
+        uint32_t bh = 0u, bl = 0u;
+        if (scan && !done) {
+          for (int t = gtid; t < n; t += gsize) {
+            const int r = pass == 0 ? rlo + t % bht : t % nr, c = pass == 0 ? clo + t / bht : t / nr;
+            bool ex = false;
+            for (int q = 0; q < nfound; ++q)
+              if (abs(r - s_locs[2 * q]) <= 2 && abs(c - s_locs[2 * q + 1]) <= 2) { ex = true; break; }
+            if (ex) continue;
+            const float v = R[c * ldr + r];
+            if (!(v > -INFINITY)) continue;  // NaN and -Inf never beat the initial -Inf
+            const uint32_t h = fkey(v), l = ~(uint32_t)(r + c * nr);
+            if (h > bh || (h == bh && l > bl)) { bh = h; bl = l; }
+          }
         }
+        group_argmax(bh, bl, red, gwarp, nwarps, whi, wlo, bar);
+        if (whi > fkey(0.f) || (rlo == 0 && clo == 0 && rhi == nr - 1 && chi == nc - 1)) break;  // positive, or the box is the plane
       }
-      uint32_t whi, wlo;
-      group_argmax(bh, bl, red, gwarp, nwarps, whi, wlo, bar);
       if (!done && whi != 0u) {
         const int lin = (int)(~wlo);
         const float best = R[(lin / nr) * ldr + (lin % nr)];
@@ -506,6 +523,9 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
   float* Rw = reinterpret_cast<float*>(P);  // real plane, overlays the complex one after stage 8
   double* part = s_part + w * (G / 32) * 3;
   const float scale = 1.0f / (float)(N * N);
+  // fftshifted rows / columns that can hold a nonzero correlation value (the
+  // support of the overlap gain; the whole plane without padding)
+  const int blo = a.box_hi > 0 ? a.box_lo : 0, bhi = a.box_hi > 0 ? a.box_hi : N - 1;
   PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
 
   for (int64_t job = (int64_t)blockIdx.x * WPC + w; job < a.njobs; job += (int64_t)gridDim.x * WPC) {
@@ -725,28 +745,36 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
       }
     }
     grp_sync(bar, G);
-    // ---- stage 8: inverse along q for row pairs (p, p + N/2) packed as
-    //      T(p) + i T(p + N/2); the fftshifted, normalised, gain-weighted
-    //      magnitudes are held in registers across a barrier, then written
-    //      as the real plane R over the complex one.
+    // ---- stage 8: inverse along q for the rows R needs: fftshifted rows
+    //      blo..bhi (the overlap gain is zero on every other row, so R is
+    //      exactly 0 there), taken in pairs (blo + t, blo + t + nh) packed as
+    //      T(p) + i T(p'). The normalised, gain-weighted magnitudes are held
+    //      in registers across a barrier, then written as the real plane R
+    //      over the complex one; the other rows are written as zeros.
+    const int nb = bhi - blo + 1, nh = (nb + 1) / 2;
     if (N2 > 1) {
-      for (int it = gt; it < H * N1; it += G) {
-        const int p = it % H, k1 = it / H;
-        float2* L = P + p + (N2 * k1) * LD;
+#pragma unroll 1
+      for (int it = gt; it < nh * N1; it += G) {
+        const int t = it % nh, k1 = it / nh;
+        const bool hasb = t + nh < nb;
+        const int pa = (blo + t + H) % N, pb = hasb ? (blo + t + nh + H) % N : pa;
+        float2* La = P + pa + (N2 * k1) * LD;
+        const float2* Lb = P + pb + (N2 * k1) * LD;
         float2 x[N2];
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) {
-          const float2 u = L[k2 * LD], v = L[k2 * LD + H];
+          const float2 u = La[k2 * LD];
+          const float2 v = hasb ? Lb[k2 * LD] : make_float2(0.f, 0.f);
           x[k2] = make_float2(u.x - v.y, u.y + v.x);
         }
         RDFT<N2, true>::run(x, N2);
 #pragma unroll
         for (int n2 = 1; n2 < N2; ++n2) {
-          const float2 t = tw[(n2 * k1) % N];
-          x[n2] = cmul(x[n2], make_float2(t.x, -t.y));
+          const float2 tt = tw[(n2 * k1) % N];
+          x[n2] = cmul(x[n2], make_float2(tt.x, -tt.y));
         }
 #pragma unroll
-        for (int n2 = 0; n2 < N2; ++n2) L[n2 * LD] = x[n2];
+        for (int n2 = 0; n2 < N2; ++n2) La[n2 * LD] = x[n2];
       }
       grp_sync(bar, G);
     }
@@ -755,28 +783,32 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
 #pragma unroll
       for (int i = 0; i < IPT; ++i) {
         const int it = gt + i * G;
-        if (it < H * N2) {
-          const int p = it % H, n2 = it / H;
-          const float2* L = P + p;
+        if (it < nh * N2) {
+          const int t = it % nh, n2 = it / nh;
+          const bool hasb = t + nh < nb;
+          const int pa = (blo + t + H) % N, pb = hasb ? (blo + t + nh + H) % N : pa;
+          const float2* La = P + pa;
+          const float2* Lb = P + pb;
           float2 x[N1];
 #pragma unroll
           for (int k1 = 0; k1 < N1; ++k1) {
             if (N2 == 1) {
-              const float2 u = L[k1 * LD], v = L[k1 * LD + H];
+              const float2 u = La[k1 * LD];
+              const float2 v = hasb ? Lb[k1 * LD] : make_float2(0.f, 0.f);
               x[k1] = make_float2(u.x - v.y, u.y + v.x);
             } else {
-              x[k1] = L[(N2 * k1 + n2) * LD];
+              x[k1] = La[(N2 * k1 + n2) * LD];
             }
           }
           RDFT<N1, true>::run(x, N1);
-          const int ps0 = (p + H) % N, ps1 = p;  // fftshifted rows of p and p + N/2
+          const int ps0 = blo + t, ps1 = blo + t + nh;  // fftshifted rows of pa and pb
 #pragma unroll
           for (int n1 = 0; n1 < N1; ++n1) {
             const int qs = (N2 * n1 + n2 + H) % N;
             float r0 = fabsf(x[n1].x) * scale, r1 = fabsf(x[n1].y) * scale;
             if (a.gain) {
               r0 *= __ldg(a.gain + qs * N + ps0);
-              r1 *= __ldg(a.gain + qs * N + ps1);
+              r1 *= hasb ? __ldg(a.gain + qs * N + ps1) : 0.f;
             }
             rv[i][0][n1] = r0;
             rv[i][1][n1] = r1;
@@ -787,16 +819,23 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
 #pragma unroll
       for (int i = 0; i < IPT; ++i) {
         const int it = gt + i * G;
-        if (it < H * N2) {
-          const int p = it % H, n2 = it / H;
-          const int ps0 = (p + H) % N, ps1 = p;
+        if (it < nh * N2) {
+          const int t = it % nh, n2 = it / nh;
+          const bool hasb = t + nh < nb;
+          const int ps0 = blo + t, ps1 = blo + t + nh;
 #pragma unroll
           for (int n1 = 0; n1 < N1; ++n1) {
             const int qs = (N2 * n1 + n2 + H) % N;
             Rw[qs * LDR + ps0] = rv[i][0][n1];
-            Rw[qs * LDR + ps1] = rv[i][1][n1];
+            if (hasb) Rw[qs * LDR + ps1] = rv[i][1][n1];
           }
         }
+      }
+      const int nz = N - nb;  // rows outside [blo, bhi]
+#pragma unroll 1
+      for (int it = gt; it < nz * N; it += G) {
+        const int j = it % nz, qs = it / nz;
+        Rw[qs * LDR + (j < blo ? j : j + nb)] = 0.f;
       }
     }
     grp_sync(bar, G);
@@ -817,7 +856,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
     }
     // ---- stage 9: peak analysis by the group
     analyze_group(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, red + w * (G / 32) * 2, true,
-                  s_vals + w * KMAX, s_locs + w * 2 * KMAX, gid, job, pw, bad, bar);
+                  s_vals + w * KMAX, s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, blo, bhi, blo, bhi);
     grp_sync(bar, G);  // the plane is reused by the group's next window
   }
 }
@@ -837,7 +876,7 @@ __global__ void __launch_bounds__(128) analyze_planes_kernel(const AnalyzeArgs a
     __syncthreads();
     const int64_t gid = a.jobs ? (int64_t)a.jobs[4 * pl] + (int64_t)a.jobs[4 * pl + 1] * a.ny : -1;
     analyze_group(R, a.nr, a.nc, a.nr, K, a.npeaks, a.finder, a.subpixel, threadIdx.x, 128, red, true, s_vals,
-                  s_locs, gid, pl, po, false, 0);
+                  s_locs, gid, pl, po, false, 0, 0, a.nr - 1, 0, a.nc - 1);
     __syncthreads();
   }
 }

@@ -92,7 +92,7 @@ class hh_batch_pair(ctypes.Structure):
         ("nr", ctypes.c_int64),
         ("nc", ctypes.c_int64),
         ("schedule", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("format", ctypes.c_int32),
     ]
 
 
@@ -115,6 +115,9 @@ class hh_batch_result(ctypes.Structure):
 
 HH_BATCH_DEVICE_INPUTS = 1
 HH_BATCH_NO_GRAPH = 2
+HH_PIX_F32 = 0
+HH_PIX_U16 = 1
+HH_PIX_U16_RAW = 2
 
 
 class hh_kernel_profile(ctypes.Structure):

@@ -43,6 +43,24 @@ def _schedules(passes, npairs):
     return uniq, index
 
 
+def _is_u16(a):
+    dt = getattr(a, "dtype", None)
+    return dt is not None and str(dt) in ("uint16", "torch.uint16")
+
+
+def _pixel_format(A, B, u16):
+    """HH_PIX_* of a pair: UInt16 frames (12/16-bit camera counts) are sent
+    as they are and converted on the device -- "normalised" to value/65535
+    like load_image's Float32 of a 16-bit image, or "raw" counts."""
+    if _is_u16(A) != _is_u16(B):
+        raise ArgumentError("both frames of a pair must have the same pixel type")
+    if not _is_u16(A):
+        return _lib.HH_PIX_F32
+    if u16 not in ("normalised", "raw"):
+        raise ArgumentError(f"u16 must be 'normalised' or 'raw', got {u16!r}")
+    return _lib.HH_PIX_U16 if u16 == "normalised" else _lib.HH_PIX_U16_RAW
+
+
 class BatchRunner:
     """A prepared batch: pair descriptors, pass tables and (page-locked)
     result buffers built once; `run()` is one library call. Keep the images
@@ -50,7 +68,7 @@ class BatchRunner:
     their contents may change between runs."""
 
     def __init__(self, pairs, passes, *, masks=None, predictor_smoothing=True, mask_threshold=0.5, workspace=None,
-                 graph=True, pinned=True):
+                 graph=True, pinned=True, u16="normalised"):
         if not pairs:
             raise ArgumentError("pairs must not be empty")
         if not (0 < mask_threshold <= 1):
@@ -75,6 +93,7 @@ class BatchRunner:
             nr, nc = int(A.shape[0]), int(A.shape[1])
             if self.device != _is_device_tensor(A) or self.device != _is_device_tensor(B):
                 raise ArgumentError("all images of a batch must be host arrays or all device tensors")
+            fmt = _pixel_format(A, B, u16)
             if self.device:
                 for t in (A, B) + ((M,) if M is not None else ()):
                     if t.stride(0) != 1 or t.stride(1) != nr:
@@ -82,12 +101,16 @@ class BatchRunner:
                 ptrs = [t.data_ptr() if t is not None else None for t in (A, B, M)]
                 self._keep.append((A, B, M))
             else:
-                a = _lib.as_f32_colmajor(A)
-                b = _lib.as_f32_colmajor(B)
+                if fmt == _lib.HH_PIX_F32:
+                    a = _lib.as_f32_colmajor(A)
+                    b = _lib.as_f32_colmajor(B)
+                else:
+                    a = np.asfortranarray(A, np.uint16)
+                    b = np.asfortranarray(B, np.uint16)
                 m = None if M is None else np.asfortranarray(M, dtype=np.uint8)
                 self._keep.append((a, b, m))
                 ptrs = [x.ctypes.data if x is not None else None for x in (a, b, m)]
-            self.pairs[p] = _lib.hh_batch_pair(ptrs[0], ptrs[1], ptrs[2], nr, nc, self.index[p], 0)
+            self.pairs[p] = _lib.hh_batch_pair(ptrs[0], ptrs[1], ptrs[2], nr, nc, self.index[p], fmt)
         flat = [p for s in self.schedules for p in s]
         self.descs = (_lib.hh_pass_desc * len(flat))(*[p.to_desc() for p in flat])
         offs = np.cumsum([0] + [len(s) for s in self.schedules]).astype(np.int32)
@@ -194,28 +217,53 @@ def run_piv_batch(pairs, passes, *, masks=None, predictor_smoothing=True, mask_t
 
 
 def run_piv_sequence(pairs, params=None, *, preprocess=None, progress=False, on_result=None, mask=None,
-                     batch_size=64, predictor_smoothing=True, mask_threshold=0.5, workspace=None):
-    """run_piv_sequence (src/io.jl:229-247) for in-memory pairs: the pairs are
-    analysed in batches of `batch_size` with run_piv_batch; `on_result(i, r)`
-    and `progress(i, n)` are called per pair in order (1-based i). `mask` is
-    None, one mask for every pair, or a function (i, pair) -> mask."""
+                     batch_size=16, predictor_smoothing=True, mask_threshold=0.5, workspace=None, u16="normalised",
+                     pipeline=True):
+    """run_piv_sequence (src/io.jl:229-247) for in-memory pairs.
+
+    Pairs are analysed in batches of `batch_size` with the batched schedule;
+    `on_result(i, r)` and `progress(i, n)` are called per pair in order
+    (1-based i), as each batch completes. `mask` is None, one mask for every
+    pair, or a function (i, pair) -> mask. Frames may be float32 or UInt16
+    (converted on the device, see BatchRunner).
+
+    With `pipeline` (CUDA available, every pair of one shape and pixel type,
+    no masks), the frames of batch k+1 are copied to the device through
+    page-locked double buffers on a copy stream while batch k is analysed,
+    so ingestion overlaps the analysis (the reference prefetches the next
+    pair's frames on a background task, src/io.jl:296-306)."""
     if not pairs:
         raise ArgumentError("pairs must not be empty")
     if params is None:
         params = [PIVParameters()]
     n = len(pairs)
+    if preprocess is not None:
+        pairs = [(preprocess(a), preprocess(b)) for a, b in pairs]
+    same = len({(tuple(a.shape), str(a.dtype), tuple(b.shape), str(b.dtype)) for a, b in pairs}) == 1
+    if pipeline and mask is None and same and not _is_device(pairs[0][0]):
+        try:
+            import torch
+            ok = torch.cuda.is_available()
+        except Exception:  # noqa: BLE001 -- no torch: unpipelined path
+            ok = False
+        if ok:
+            return _sequence_pipelined(pairs, params, on_result, progress, batch_size, predictor_smoothing,
+                                       mask_threshold, workspace, u16)
     out = []
     for start in range(0, n, batch_size):
         chunk = pairs[start:start + batch_size]
-        imgs = [(preprocess(a), preprocess(b)) if preprocess else (a, b) for a, b in chunk]
         if mask is None:
             ms = None
         elif callable(mask):
             ms = [mask(start + j + 1, chunk[j]) for j in range(len(chunk))]
         else:
             ms = [mask] * len(chunk)
-        res = run_piv_batch(imgs, params, masks=ms, predictor_smoothing=predictor_smoothing,
-                            mask_threshold=mask_threshold, workspace=workspace)
+        runner = BatchRunner(chunk, params, masks=ms, predictor_smoothing=predictor_smoothing,
+                             mask_threshold=mask_threshold, workspace=workspace, pinned=False, u16=u16)
+        try:
+            res = runner.run().results(copy=True)
+        finally:
+            runner.close()
         for j, r in enumerate(res):
             i = start + j + 1
             out.append(r)
@@ -224,3 +272,86 @@ def run_piv_sequence(pairs, params=None, *, preprocess=None, progress=False, on_
             if callable(progress):
                 progress(i, n)
     return out
+
+
+def _is_device(a):
+    return hasattr(a, "data_ptr") and getattr(a, "is_cuda", False)
+
+
+def _sequence_pipelined(pairs, params, on_result, progress, batch_size, smoothing, thr, workspace, u16):
+    import concurrent.futures as cf
+
+    import torch
+
+    n = len(pairs)
+    nr, nc = pairs[0][0].shape
+    tdt = torch.uint16 if _is_u16(pairs[0][0]) else torch.float32
+    ndt = np.uint16 if tdt == torch.uint16 else np.float32
+    B = min(batch_size, n)
+    own = workspace is None
+    ws = workspace if workspace is not None else PIVWorkspace()
+    copy_stream = torch.cuda.Stream()
+    # two sets of (pinned host, device) frame buffers, column-major (stride (1, nr))
+    host = [torch.empty((2 * B, nc, nr), dtype=tdt, pin_memory=True) for _ in range(2)]
+    dev = [torch.empty((2 * B, nc, nr), dtype=tdt, device="cuda") for _ in range(2)]
+    events = [torch.cuda.Event(), torch.cuda.Event()]
+    runners = {}
+
+    def stage(k, slot):
+        """Host -> page-locked -> device copy of batch k into buffer set `slot`."""
+        chunk = pairs[k * B:(k + 1) * B]
+        hv = host[slot].numpy()
+        for j, (a, b) in enumerate(chunk):
+            hv[2 * j] = np.asarray(a, ndt).T
+            hv[2 * j + 1] = np.asarray(b, ndt).T
+        with torch.cuda.stream(copy_stream):
+            dev[slot][:2 * len(chunk)].copy_(host[slot][:2 * len(chunk)], non_blocking=True)
+            events[slot].record(copy_stream)
+        return len(chunk)
+
+    def runner_for(slot, m):
+        key = (slot, m)
+        if key not in runners:
+            frames = [(dev[slot][2 * j].T, dev[slot][2 * j + 1].T) for j in range(m)]
+            runners[key] = BatchRunner(frames, params, predictor_smoothing=smoothing, mask_threshold=thr,
+                                       workspace=ws, u16=u16)
+        return runners[key]
+
+    nb = (n + B - 1) // B
+    out = []
+    try:
+        with cf.ThreadPoolExecutor(max_workers=1) as pool:
+            fut = pool.submit(stage, 0, 0)
+            for k in range(nb):
+                slot = k % 2
+                m = fut.result()
+                if k + 1 < nb:  # batch k+1 streams in while batch k is analysed
+                    fut = pool.submit(stage, k + 1, (k + 1) % 2)
+                events[slot].synchronize()
+                res = runner_for(slot, m).run().results(copy=True)
+                if k + 1 < nb:
+                    fut.result()  # the next buffers are filled before this set is refilled
+                    fut = _Done(fut.result())
+                for j, r in enumerate(res):
+                    i = k * B + j + 1
+                    out.append(r)
+                    if on_result is not None:
+                        on_result(i, r)
+                    if callable(progress):
+                        progress(i, n)
+    finally:
+        for r in runners.values():
+            r.close()
+        if own:
+            ws.close()
+    return out
+
+
+class _Done:
+    """A finished future (the staged size of the next batch)."""
+
+    def __init__(self, v):
+        self.v = v
+
+    def result(self):
+        return self.v

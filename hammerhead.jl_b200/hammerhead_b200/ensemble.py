@@ -11,13 +11,14 @@ import numpy as np
 from . import _lib
 from ._lib import ArgumentError, DimensionMismatch
 from .params import PIVParameters, effort_schedule
+from .batch import _pixel_format
 from .pipeline import PIVResult, PIVWorkspace, _is_device_tensor, check_backend_params, pass_grid
 
 _FIELDS = ("u", "v", "peak_ratio", "correlation_moment", "uncertainty_u", "uncertainty_v")
 
 
 def run_piv_ensemble(pairs, params=None, *, effort=None, predictor_smoothing=True, mask=None, mask_threshold=0.5,
-                     preprocess=None, workspace=None, scale=None):
+                     preprocess=None, workspace=None, scale=None, u16="normalised"):
     """Ensemble PIV over `pairs` (a list of (A, B) images: numpy (rows, cols)
     arrays, or column-major torch CUDA tensors); `params` is a
     PIVParameters or a pass schedule. Returns the PIVResult of the final
@@ -52,6 +53,7 @@ def run_piv_ensemble(pairs, params=None, *, effort=None, predictor_smoothing=Tru
         elif tuple(A.shape) != shape:
             raise DimensionMismatch(f"all pairs must share the image size {shape}, got {tuple(A.shape)}")
         nr, nc = shape
+        fmt = _pixel_format(A, B, u16)
         if device:
             for t in (A, B):
                 if not _is_device_tensor(t) or t.stride(0) != 1 or t.stride(1) != nr:
@@ -59,10 +61,13 @@ def run_piv_ensemble(pairs, params=None, *, effort=None, predictor_smoothing=Tru
             ptrs = (A.data_ptr(), B.data_ptr())
             keep.append((A, B))
         else:
-            a, b = _lib.as_f32_colmajor(A), _lib.as_f32_colmajor(B)
+            if fmt == _lib.HH_PIX_F32:
+                a, b = _lib.as_f32_colmajor(A), _lib.as_f32_colmajor(B)
+            else:
+                a, b = np.asfortranarray(A, np.uint16), np.asfortranarray(B, np.uint16)
             keep.append((a, b))
             ptrs = (a.ctypes.data, b.ctypes.data)
-        arr[q] = _lib.hh_batch_pair(ptrs[0], ptrs[1], None, nr, nc, 0, 0)
+        arr[q] = _lib.hh_batch_pair(ptrs[0], ptrs[1], None, nr, nc, 0, fmt)
     if mask is not None and tuple(mask.shape) != shape:
         raise DimensionMismatch(f"mask must have the same size as the images, got {tuple(mask.shape)}")
     m = None if mask is None else np.asfortranarray(mask, dtype=np.uint8)

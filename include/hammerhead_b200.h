@@ -156,13 +156,22 @@ hh_status hh_run_piv_device(hh_ctx* ctx, const float* dA, const float* dB, int64
  * device memory of the context's device with HH_BATCH_DEVICE_INPUTS; then
  * they must stay valid until the call returns). */
 typedef struct hh_batch_pair {
-  const float* A;
+  const float* A;       /* frame data; with format != HH_PIX_F32 a const uint16_t* cast to float* */
   const float* B;
   const uint8_t* mask;  /* nonzero = excluded, or NULL */
   int64_t nr, nc;
   int32_t schedule;
-  int32_t reserved;
+  int32_t format;       /* HH_PIX_*: pixel type of A and B */
 } hh_batch_pair;
+
+/* Pixel formats of a batch pair. Camera frames (12- or 16-bit counts stored
+ * as UInt16) cross PCIe at half the bytes and are converted on the device:
+ * HH_PIX_U16 gives value / 65535 (the Float32 of a Gray{N0f16} pixel, as
+ * load_image returns it, src/io.jl:20-25), HH_PIX_U16_RAW the count itself
+ * (value * 1). Both are correctly rounded IEEE operations. */
+#define HH_PIX_F32 0
+#define HH_PIX_U16 1
+#define HH_PIX_U16_RAW 2
 
 /* Final-pass results in compact host arrays: pair p's ny[p] x nx[p] grid
  * (column-major) occupies [offsets[p], offsets[p+1]). Any pointer may be

@@ -166,3 +166,49 @@ def test_batch_launch_count(hb, ws):
         counts.append(L.hh_launch_count(ws.ctx) - c0)
         r.close()
     assert counts[0] == counts[1] and counts[0] < 200
+
+
+def test_batch_uint16_frames(hb, ws):
+    # 12-bit counts in UInt16 are converted on the device: normalised (x/65535)
+    # equals the float32 path on the same values, raw equals x itself
+    import torch
+
+    syn = hb.synthetic
+    s1, s2 = _schedules(hb)
+    pairs16 = []
+    for i, shape in enumerate([(256, 256), (192, 320)]):
+        A, B = syn.particle_pair(shape, syn.uniform_flow(1.7, -0.9), seed=60 + i)
+        pairs16.append((syn.to_uint16_12bit(A), syn.to_uint16_12bit(B)))
+    sched = [s1, s2]
+    res16 = hb.run_piv_batch(pairs16, sched, workspace=ws)
+    as_f = [(a.astype(np.float32) / np.float32(65535), b.astype(np.float32) / np.float32(65535)) for a, b in pairs16]
+    resf = hb.run_piv_batch(as_f, sched, workspace=ws)
+    for a, b in zip(res16, resf):
+        _same(a, b)
+    runner = hb.BatchRunner(pairs16, sched, workspace=ws, u16="raw")
+    rr = runner.run().results()
+    runner.close()
+    resr = hb.run_piv_batch([(a.astype(np.float32), b.astype(np.float32)) for a, b in pairs16], sched, workspace=ws)
+    for a, b in zip(rr, resr):
+        _same(a, b)
+    # device-resident UInt16 frames
+    dev = [(torch.from_numpy(np.ascontiguousarray(a.T)).cuda().T, torch.from_numpy(np.ascontiguousarray(b.T)).cuda().T)
+           for a, b in pairs16]
+    for a, b in zip(hb.run_piv_batch(dev, sched, workspace=ws), res16):
+        _same(a, b)
+
+
+def test_sequence_pipelined_equals_batch(hb, ws):
+    syn = hb.synthetic
+    s1, _ = _schedules(hb)
+    pairs = [tuple(syn.to_uint16_12bit(x) for x in syn.particle_pair((256, 256), syn.sine_shear_flow(2.0, 180.0),
+                                                                     seed=80 + i)) for i in range(7)]
+    seen = []
+    seq = hb.run_piv_sequence(pairs, s1, batch_size=3, workspace=ws, on_result=lambda i, r: seen.append(i))
+    assert seen == list(range(1, 8))
+    ref = hb.run_piv_batch(pairs, s1, workspace=ws)
+    for a, b in zip(seq, ref):
+        _same(a, b)
+    unpiped = hb.run_piv_sequence(pairs, s1, batch_size=3, workspace=ws, pipeline=False)
+    for a, b in zip(unpiped, ref):
+        _same(a, b)
