@@ -355,11 +355,11 @@ def main():
     fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s, FMA = 2 FLOP
     achieved = (c["flops"] / (c["ms"] / 1e3)) / 1e12 if c["ms"] > 0 else None
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "correlate_traffic.json")
-    if os.path.exists(tpath):
-        tr = json.load(open(tpath))
-        if c["units"] > 0:
-            traffic = tr["dram_bytes_per_window"] * c["units"] / max(c["launches"], 1)
+    tpath = os.path.join(ROOT, "profiles", "correlate_traffic.txt")
+    if os.path.exists(tpath) and c["units"] > 0:
+        per_window = {ln.split()[0]: float(ln.split()[1]) for ln in open(tpath)
+                      if ln.strip() and not ln.startswith("#")}["dram_bytes_per_window"]
+        traffic = per_window * c["units"] / max(c["launches"], 1)
     shares = {k: round(v["ms"] / max(sum(x["ms"] for x in prof.values()), 1e-9), 4) for k, v in prof.items()}
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     d = prof["deform"]
