@@ -242,10 +242,35 @@ struct PeakOut {
 // values (outside it the overlap gain is zero, so R is exactly 0 there); the
 // scans cover it, plus the last pixel, the only place outside where a zero
 // can be a regional maximum (every other pixel has a later neighbour >= 0).
+// A thread's share of the box scan, fixed for a launch (the box and the
+// group size do not change), so the integer divisions are done once:
+// column strips of rps rows, S strips per column; this thread's first
+// strip is column c, rows [r0, r1).
+struct ScanPlan {
+  int rlo, rhi, clo, chi;
+  int bw, S, rps;
+  int c, r0, r1;
+};
+__device__ __forceinline__ ScanPlan scan_plan(int gtid, int gsize, int rlo, int rhi, int clo, int chi) {
+  ScanPlan sp;
+  sp.rlo = rlo;
+  sp.rhi = rhi;
+  sp.clo = clo;
+  sp.chi = chi;
+  sp.bw = chi - clo + 1;
+  sp.S = gsize / sp.bw > 0 ? gsize / sp.bw : 1;  // row segments per column
+  sp.rps = (rhi - rlo + 1 + sp.S - 1) / sp.S;
+  sp.c = clo + gtid % sp.bw;
+  sp.r0 = rlo + (gtid / sp.bw) * sp.rps;
+  sp.r1 = min(rhi + 1, sp.r0 + sp.rps);
+  return sp;
+}
+
 __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
                               int subpixel, int gtid, int gsize, uint32_t* red, bool active, float* s_vals,
                               int* s_locs, int64_t grid_id, int64_t job, const PeakOut& o, bool poison, int bar,
-                              int rlo, int rhi, int clo, int chi) {
+                              const ScanPlan sp) {
+  const int rlo = sp.rlo, rhi = sp.rhi, clo = sp.clo, chi = sp.chi;
   // a poisoned plane (non-finite window data: the reference's plane is all
   // NaN there) yields no peak, so every output is NaN
   const bool scan = active && !poison;
@@ -262,13 +287,15 @@ __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int l
     TopK tk;
     tk.init();
     if (scan) {
-      const int bw = chi - clo + 1, bh = rhi - rlo + 1;  // box columns, rows
-      const int S = gsize / bw > 0 ? gsize / bw : 1;    // row segments per column
-      const int rps = (bh + S - 1) / S;
+      const int bw = sp.bw, S = sp.S, rps = sp.rps;
       const float NaNf = __int_as_float(0x7fc00000);
       for (int strip = gtid; strip < bw * S; strip += gsize) {
-        const int c = clo + strip % bw, seg = strip / bw;
-        const int r0 = rlo + seg * rps, r1 = min(rhi + 1, r0 + rps);
+        int c = sp.c, r0 = sp.r0, r1 = sp.r1;
+        if (strip != gtid) {  // a further strip: only when the box is wider than the group
+          c = clo + strip % bw;
+          r0 = rlo + (strip / bw) * rps;
+          r1 = min(rhi + 1, r0 + rps);
+        }
         if (r0 >= r1) continue;
         const float* Cl = c > 0 ? R + (c - 1) * ldr : nullptr;
         const float* Cc = R + c * ldr;
@@ -526,6 +553,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
   // fftshifted rows / columns that can hold a nonzero correlation value (the
   // support of the overlap gain; the whole plane without padding)
   const int blo = a.box_hi > 0 ? a.box_lo : 0, bhi = a.box_hi > 0 ? a.box_hi : N - 1;
+  const ScanPlan sp = scan_plan(tid % G, G, blo, bhi, blo, bhi);
   PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
 
   for (int64_t job = (int64_t)blockIdx.x * WPC + w; job < a.njobs; job += (int64_t)gridDim.x * WPC) {
@@ -754,8 +782,9 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
     const int nb = bhi - blo + 1, nh = (nb + 1) / 2;
     if (N2 > 1) {
 #pragma unroll 1
-      for (int it = gt; it < nh * N1; it += G) {
-        const int t = it % nh, k1 = it / nh;
+      for (int it = gt; it < H * N1; it += G) {  // items (t, k1) at it = t + H k1, t < nh used
+        const int t = it % H, k1 = it / H;
+        if (t >= nh) continue;
         const bool hasb = t + nh < nb;
         const int pa = (blo + t + H) % N, pb = hasb ? (blo + t + nh + H) % N : pa;
         float2* La = P + pa + (N2 * k1) * LD;
@@ -782,9 +811,9 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
       float rv[IPT][2][N1];
 #pragma unroll
       for (int i = 0; i < IPT; ++i) {
-        const int it = gt + i * G;
-        if (it < nh * N2) {
-          const int t = it % nh, n2 = it / nh;
+        const int it = gt + i * G;  // items (t, n2) at it = t + H n2, t < nh used
+        if (it < H * N2 && it % H < nh) {
+          const int t = it % H, n2 = it / H;
           const bool hasb = t + nh < nb;
           const int pa = (blo + t + H) % N, pb = hasb ? (blo + t + nh + H) % N : pa;
           const float2* La = P + pa;
@@ -819,8 +848,8 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
 #pragma unroll
       for (int i = 0; i < IPT; ++i) {
         const int it = gt + i * G;
-        if (it < nh * N2) {
-          const int t = it % nh, n2 = it / nh;
+        if (it < H * N2 && it % H < nh) {
+          const int t = it % H, n2 = it / H;
           const bool hasb = t + nh < nb;
           const int ps0 = blo + t, ps1 = blo + t + nh;
 #pragma unroll
@@ -832,10 +861,10 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
         }
       }
       const int nz = N - nb;  // rows outside [blo, bhi]
-#pragma unroll 1
-      for (int it = gt; it < nz * N; it += G) {
-        const int j = it % nz, qs = it / nz;
-        Rw[qs * LDR + (j < blo ? j : j + nb)] = 0.f;
+      for (int j = gt; j < nz; j += G) {
+        const int ps = j < blo ? j : j + nb;
+#pragma unroll 4
+        for (int qs = 0; qs < N; ++qs) Rw[qs * LDR + ps] = 0.f;
       }
     }
     grp_sync(bar, G);
@@ -856,7 +885,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
     }
     // ---- stage 9: peak analysis by the group
     analyze_group(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, red + w * (G / 32) * 2, true,
-                  s_vals + w * KMAX, s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, blo, bhi, blo, bhi);
+                  s_vals + w * KMAX, s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, sp);
     grp_sync(bar, G);  // the plane is reused by the group's next window
   }
 }
@@ -871,12 +900,13 @@ __global__ void __launch_bounds__(128) analyze_planes_kernel(const AnalyzeArgs a
   int* s_locs = reinterpret_cast<int*>(s_vals + KMAX);
   const int K = a.npeaks > 2 ? a.npeaks : 2;
   PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
+  const ScanPlan sp = scan_plan(threadIdx.x, 128, 0, a.nr - 1, 0, a.nc - 1);
   for (int64_t pl = blockIdx.x; pl < a.nplanes; pl += gridDim.x) {
     for (int k = threadIdx.x; k < P; k += blockDim.x) R[k] = a.planes[pl * (int64_t)P + k];
     __syncthreads();
     const int64_t gid = a.jobs ? (int64_t)a.jobs[4 * pl] + (int64_t)a.jobs[4 * pl + 1] * a.ny : -1;
     analyze_group(R, a.nr, a.nc, a.nr, K, a.npeaks, a.finder, a.subpixel, threadIdx.x, 128, red, true, s_vals,
-                  s_locs, gid, pl, po, false, 0, 0, a.nr - 1, 0, a.nc - 1);
+                  s_locs, gid, pl, po, false, 0, sp);
     __syncthreads();
   }
 }

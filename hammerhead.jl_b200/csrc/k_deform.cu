@@ -29,6 +29,14 @@ namespace hh {
 #define FS(a, b) __fsub_rn((a), (b))
 #define FD(a, b) __fdiv_rn((a), (b))
 
+// Correctly rounded float constants of 1/6 and 2/3 (what 1f0/6 and 2f0/3
+// evaluate to), and x/2 taken as x*0.5: halving by a power of two is the
+// same correctly rounded value either way, so the results are unchanged.
+static __device__ __forceinline__ float k_sixth() { return __int_as_float(0x3E2AAAAB); }
+static __device__ __forceinline__ float k_two_thirds() { return __int_as_float(0x3F2AAAAB); }
+#define kSixth k_sixth()
+#define kTwoThirds k_two_thirds()
+
 // Elimination factors for a line of padded length n: unknown rows
 // i = 3..n-2 (1-based). inv[k] = 1/den_k, cp[k] = (1/6)*inv[k], k = i - 3.
 __global__ void bspline_factors_kernel(int64_t n, float* cp, float* inv) {
@@ -68,7 +76,7 @@ __device__ __forceinline__ void bs_fwd_item(const float* __restrict__ in, float*
                                             int64_t es, int64_t ls, int64_t nlines, const float* __restrict__ inv,
                                             int64_t t) {
   const int64_t m = n - 4;
-  const float sixth = FD(1.0f, 6.0f);
+  const float sixth = kSixth;
   const int64_t line = t % nlines, seg = t / nlines;
   const float* x = in + line * ls;
   float* d = dbuf + line * ls;
@@ -191,10 +199,10 @@ __device__ __forceinline__ float bilinear(const float* f, const PredGrid& g, flo
 // Interpolations' cubic B-spline weights at fractional offset d.
 __device__ __forceinline__ void cubw(float d, float* w) {
   const float x3 = FM(FM(d, d), d), c = FS(1.f, d), c3 = FM(FM(c, c), c);
-  const float two3 = FD(2.f, 3.f);
+  const float two3 = kTwoThirds;
   w[0] = FD(c3, 6.f);
-  w[1] = FA(FS(two3, FM(d, d)), FD(x3, 2.f));
-  w[2] = FA(FS(two3, FM(c, c)), FD(c3, 2.f));
+  w[1] = FA(FS(two3, FM(d, d)), FM(x3, 0.5f));
+  w[2] = FA(FS(two3, FM(c, c)), FM(c3, 0.5f));
   w[3] = FD(x3, 6.f);
 }
 
@@ -224,11 +232,13 @@ __global__ void __launch_bounds__(256) deform_kernel(const float* __restrict__ C
                                                      int64_t nr, int64_t nc, const float* __restrict__ pu,
                                                      const float* __restrict__ pv, PredGrid g, float* wA, float* wB) {
   const int64_t total = nr * nc;
+  const bool small = total <= 0x7fffffff;
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = k % nr, c = k / nr;
+    const int64_t r = small ? (int64_t)((uint32_t)k % (uint32_t)nr) : k % nr;
+    const int64_t c = small ? (int64_t)((uint32_t)k / (uint32_t)nr) : k / nr;
     const float R = (float)(r + 1), Cc = (float)(c + 1);
-    const float du2 = FD(bilinear(pu, g, R, Cc), 2.f);
-    const float dv2 = FD(bilinear(pv, g, R, Cc), 2.f);
+    const float du2 = FM(bilinear(pu, g, R, Cc), 0.5f);
+    const float dv2 = FM(bilinear(pv, g, R, Cc), 0.5f);
     wA[k] = bspline_eval(CA, nr, nc, FS(R, dv2), FS(Cc, du2));
     wB[k] = bspline_eval(CB, nr, nc, FA(R, dv2), FA(Cc, du2));
   }
@@ -387,10 +397,17 @@ __global__ void __launch_bounds__(256) b_deform_kernel(const BPair* __restrict__
     const int64_t l = k - b.pcoff;
     if (!bp_live(b, it, done, p) || !(it > 1 || b.has_pred0) || !b.deforms || l >= b.nr * b.nc) continue;
     const PredGrid g = b_pred_grid(b, it);
-    const int64_t r = l % b.nr, c = l / b.nr;
+    int64_t r, c;
+    if (b.nr * b.nc <= 0x7fffffff) {  // 32-bit division when the pair's pixel index fits
+      r = (uint32_t)l % (uint32_t)b.nr;
+      c = (uint32_t)l / (uint32_t)b.nr;
+    } else {
+      r = l % b.nr;
+      c = l / b.nr;
+    }
     const float R = (float)(r + 1), Cc = (float)(c + 1);
-    const float du2 = FD(bilinear(pu + b.goff, g, R, Cc), 2.f);
-    const float dv2 = FD(bilinear(pv + b.goff, g, R, Cc), 2.f);
+    const float du2 = FM(bilinear(pu + b.goff, g, R, Cc), 0.5f);
+    const float dv2 = FM(bilinear(pv + b.goff, g, R, Cc), 0.5f);
     b.warpA[l] = bspline_eval(b.coefA, b.nr, b.nc, FS(R, dv2), FS(Cc, du2));
     b.warpB[l] = bspline_eval(b.coefB, b.nr, b.nc, FA(R, dv2), FA(Cc, du2));
   }
