@@ -405,14 +405,46 @@ __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int l
   }
   const float NaN = __int_as_float(0x7fc00000);
   const int cr = nr / 2 + 1, cc = nc / 2 + 1;
+  const int mmax = found < npeaks ? found : npeaks;  // peaks 1..mmax carry results
+  // The gauss3 logarithms of every peak refined by gauss3, one per lane:
+  // lane 4m + q takes peak m, q = 0 / 1: ln(Im/Ip), ln(Im Ip / I0^2) along
+  // the rows, q = 2 / 3 along the columns (gauss3_axis, spread over lanes so
+  // the warp evaluates one logarithm instead of four in a row).
+  double lg = 0.0;
+  int lv = 0;
+  {
+    const int m = lane >> 2, q = lane & 3;
+    const bool fit3 = m < K && m < found && (m == 0 ? (subpixel != 1 && subpixel != 3) : m < mmax);
+    if (fit3) {
+      const int i = s_locs[2 * m], j = s_locs[2 * m + 1];
+      const bool rows = q < 2;
+      if (rows ? (i > 0 && i < nr - 1) : (j > 0 && j < nc - 1)) {
+        const float I0 = R[j * ldr + i];
+        const float Im = rows ? R[j * ldr + i - 1] : R[(j - 1) * ldr + i];
+        const float Ip = rows ? R[j * ldr + i + 1] : R[(j + 1) * ldr + i];
+        if (Im > 0.f && I0 > 0.f && Ip > 0.f) {
+          const double dm = (double)Im, dz = (double)I0, dp = (double)Ip;
+          lg = log((q & 1) ? (dm * dp) / (dz * dz) : dm / dp);
+          lv = 1;
+        }
+      }
+    }
+  }
+  const double g0 = __shfl_sync(0xffffffffu, lg, (4 * lane) & 31), g1 = __shfl_sync(0xffffffffu, lg, (4 * lane + 1) & 31);
+  const double g2 = __shfl_sync(0xffffffffu, lg, (4 * lane + 2) & 31), g3 = __shfl_sync(0xffffffffu, lg, (4 * lane + 3) & 31);
+  const int v0 = __shfl_sync(0xffffffffu, lv, (4 * lane) & 31), v2 = __shfl_sync(0xffffffffu, lv, (4 * lane + 2) & 31);
   if (lane >= K) return;
   float ref[2] = {NaN, NaN};
-  const int mmax = found < npeaks ? found : npeaks;  // peaks 1..mmax carry results
   if (lane < found && (lane == 0 || lane < mmax)) {
     const int pr = s_locs[2 * lane], pc = s_locs[2 * lane + 1];
     if (lane == 0 && subpixel == 1) gauss9_fp64(R, nr, nc, ldr, pr, pc, ref);
     else if (lane == 0 && subpixel == 3) { ref[0] = (float)(pr + 1); ref[1] = (float)(pc + 1); }
-    else gauss3_fp64(R, nr, nc, ldr, pr, pc, ref);
+    else {  // gauss3 from the lanes' logarithms (gauss3_fp64)
+      const double di = v0 ? (g1 != 0.0 ? g0 / (2.0 * g1) : 0.0) : 0.0;
+      const double dj = v2 ? (g3 != 0.0 ? g2 / (2.0 * g3) : 0.0) : 0.0;
+      ref[0] = (float)((double)(pr + 1) + di);
+      ref[1] = (float)((double)(pc + 1) + dj);
+    }
   }
   const float d_col = ref[1] - (float)cc, d_row = ref[0] - (float)cr;
   if (lane == 0) {
@@ -710,12 +742,18 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
       }
     }
     grp_sync(bar, G);
-    // ---- stage 6: cross-power (or filtered phase) spectrum over Hermitian
-    //      pairs (k, -k) on the canonical columns kq = 0..N/2 (frequencies in
-    //      storage order for N2 > 1, natural order otherwise). Only canonical
-    //      columns are written: the inverse never reads the others.
-    for (int it = gt; it < NC * N; it += G) {
-      const int ap = it % N, c = it / N;
+    // ---- stages 6-7: cross-power (or filtered phase) spectrum over Hermitian
+    //      pairs (k, -k) and the inverse along p, on the canonical columns
+    //      kq = 0..N/2 only (frequencies in storage order for N2 > 1, natural
+    //      order otherwise); the conjugate column -kq is then filled in as
+    //      conj of column kq. (i) The two self-paired columns (kq = 0, N/2)
+    //      pair rows within the column: their spectrum is formed first, in
+    //      place (for N <= 32 every canonical column is done here: folding
+    //      the spectrum into the single-pass inverse costs more registers
+    //      than the separate pass costs time).
+#pragma unroll 1
+    for (int it = gt; it < (N2 == 1 ? NC : 2) * N; it += G) {
+      const int ap = it % N, c = N2 == 1 ? it / N : (it / N) * H;
       int aq, bq, bp, kp;
       if (N2 == 1) {
         aq = c;
@@ -723,28 +761,38 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
         bp = (N - ap) % N;
         kp = ap;
       } else {
-        aq = s_canon[c];
-        bq = s_neg[aq];
+        aq = bq = s_canon[c];
         bp = s_neg[ap];
         kp = s_freq[ap];
       }
       const bool self = aq == bq;
-      if (self && ap > bp) continue;  // self-paired column: its partner row does this pair
+      if (self && ap > bp) continue;  // its partner row does this pair
       const float wk = a.method == 1 ? __ldg(a.phasew + c * N + kp) : 1.f;
       const float2 S = cross_spectrum(P[aq * LD + ap], P[bq * LD + bp], a.method, wk);
       P[aq * LD + ap] = S;
-      if (self) P[bq * LD + bp] = make_float2(S.x, -S.y);
+      if (self) P[aq * LD + bp] = make_float2(S.x, -S.y);
     }
     grp_sync(bar, G);
-    // ---- stage 7: inverse along p for the canonical columns, back to natural
-    //      p; the conjugate column -kq is filled in as conj of column kq
+    //      (ii) for N > 32 every other canonical column forms its spectrum
+    //      while it is read for its first inverse pass; its partner column
+    //      -kq is read only by it, and written only after the pass.
     if (N2 > 1) {
+#pragma unroll 1
       for (int it = gt; it < NC * N1; it += G) {
         const int c = it % NC, k1 = it / NC;
-        float2* L = P + s_canon[c] * LD + N2 * k1;
+        const int aq = s_canon[c], bq = s_neg[aq];
+        float2* L = P + aq * LD + N2 * k1;
+        const float2* Lb = P + bq * LD;
         float2 x[N2];
 #pragma unroll
-        for (int k2 = 0; k2 < N2; ++k2) x[k2] = L[k2];
+        for (int k2 = 0; k2 < N2; ++k2) {
+          x[k2] = L[k2];
+          if (aq != bq) {
+            const int pos = N2 * k1 + k2;
+            const float wk = a.method == 1 ? __ldg(a.phasew + c * N + s_freq[pos]) : 1.f;
+            x[k2] = cross_spectrum(x[k2], Lb[s_neg[pos]], a.method, wk);
+          }
+        }
         RDFT<N2, true>::run(x, N2);
 #pragma unroll
         for (int n2 = 1; n2 < N2; ++n2) {
@@ -756,6 +804,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
       }
       grp_sync(bar, G);
     }
+#pragma unroll 1
     for (int it = gt; it < NC * N2; it += G) {
       const int c = it % NC, n2 = it / NC;
       const int aq = N2 == 1 ? c : s_canon[c];

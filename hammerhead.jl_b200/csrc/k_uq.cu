@@ -257,10 +257,11 @@ template <int W> struct UQWCfg {
   static constexpr size_t win_bytes = 2 * (size_t)LD * W * sizeof(float) + (size_t)W * W;
   static constexpr size_t part_bytes = (44 * 33 + 44) * sizeof(double);  // per warp: partials + totals
   static constexpr size_t smem() { return UQW_WINDOWS * win_bytes + 2 * UQW_WINDOWS * part_bytes + 16; }
+  static constexpr int MINB = W <= 16 ? 4 : 2;  // CTAs per SM the register budget is sized for
 };
 
 template <int W>
-__global__ void __launch_bounds__(UQW_THREADS) uq_warp_kernel(const UQArgs a, const UQOffsets o) {
+__global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(const UQArgs a, const UQOffsets o) {
   using C = UQWCfg<W>;
   constexpr int LD = C::LD, M = C::M;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -374,49 +375,53 @@ __global__ void __launch_bounds__(UQW_THREADS) uq_warp_kernel(const UQArgs a, co
       const double mu = warp_sum(msum) / (double)(W * M);
 #pragma unroll
       for (int r = 0; r < W; ++r) dd[r] = col ? dd[r] - mu : 0.0;
-      // ---- S00 and the covariance sums: acc[dc][dr + 4] pairs (r, c) with (r + dr, c + dc)
-      double sq = 0.0;
-      double acc0[4];
-      double acc[4][9];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) acc0[i] = 0.0;
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 9; ++j) acc[i][j] = 0.0;
-#pragma unroll
-      for (int r = 0; r < W; ++r) {
-        sq = fma(dd[r], dd[r], sq);
-#pragma unroll
-        for (int dr = 1; dr <= 4; ++dr)
-          if (r + dr < W) acc0[dr - 1] = fma(dd[r], dd[r + dr], acc0[dr - 1]);
-      }
-#pragma unroll
-      for (int dc = 1; dc <= 4; ++dc) {
-        const bool ok = c + dc < M;
-#pragma unroll
-        for (int r2 = 0; r2 < W; ++r2) {
-          double x = __shfl_down_sync(0xffffffffu, dd[r2], dc);
-          x = ok ? x : 0.0;
-#pragma unroll
-          for (int dr = -4; dr <= 4; ++dr) {
-            const int r0 = r2 - dr;
-            if (r0 >= 0 && r0 < W) acc[dc - 1][dr + 4] = fma(dd[r0], x, acc[dc - 1][dr + 4]);
-          }
-        }
-      }
-      // ---- per-lane partials -> shared [stat][lane] in natural order, summed
-      //      in lane order into the totals in ring order
+      // ---- S00 and the covariance sums: acc[dc][dr + 4] pairs (r, c) with
+      //      (r + dr, c + dc). Two neighbour columns at a time, so only 18
+      //      accumulators are live; each group's per-lane partials go to
+      //      shared [stat][lane] in natural order.
       part[0 * 33 + lane] = s0;
       part[1 * 33 + lane] = s1;
       part[2 * 33 + lane] = s2;
-      part[3 * 33 + lane] = sq;
+      {
+        double sq = 0.0, acc0[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-      for (int i = 0; i < 4; ++i) part[(4 + i) * 33 + lane] = acc0[i];
+        for (int r = 0; r < W; ++r) {
+          sq = fma(dd[r], dd[r], sq);
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+          for (int dr = 1; dr <= 4; ++dr)
+            if (r + dr < W) acc0[dr - 1] = fma(dd[r], dd[r + dr], acc0[dr - 1]);
+        }
+        part[3 * 33 + lane] = sq;
 #pragma unroll
-        for (int j = 0; j < 9; ++j) part[(8 + 9 * i + j) * 33 + lane] = acc[i][j];
+        for (int i = 0; i < 4; ++i) part[(4 + i) * 33 + lane] = acc0[i];
+      }
+#pragma unroll
+      for (int dg = 1; dg <= 3; dg += 2) {
+        double acc[2][9];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int jj = 0; jj < 9; ++jj) acc[i][jj] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int dc = dg + i;
+          const bool ok = c + dc < M;
+#pragma unroll
+          for (int r2 = 0; r2 < W; ++r2) {
+            double x = __shfl_down_sync(0xffffffffu, dd[r2], dc);
+            x = ok ? x : 0.0;
+#pragma unroll
+            for (int dr = -4; dr <= 4; ++dr) {
+              const int r0 = r2 - dr;
+              if (r0 >= 0 && r0 < W) acc[i][dr + 4] = fma(dd[r0], x, acc[i][dr + 4]);
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int jj = 0; jj < 9; ++jj) part[(8 + 9 * (dg - 1 + i) + jj) * 33 + lane] = acc[i][jj];
+      }
       __syncwarp();
       double* tot = part + 44 * 33;
       for (int st = lane; st < 44; st += 32) {
