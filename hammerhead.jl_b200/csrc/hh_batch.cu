@@ -195,7 +195,7 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
     if (deforms[p]) {
       Wt += nr * nc;
       Q += (nr + 2) * (nc + 2);
-      WC += nc * nseg_host(nr + 2);
+      WC += (nc + 31) / 32 * nseg_host(nr + 2);  // column tiles x segments
       WR += (nr + 2) * nseg_host(nc + 2);
     }
     roff[p] = R;

@@ -155,6 +155,27 @@ __device__ __forceinline__ void group_argmax(uint32_t hi, uint32_t lo, uint32_t*
   grp_sync(bar, nwarps * 32);
 }
 
+// The warp's K best keys over its lanes' lists, by K shuffle rounds (keys
+// are unique, so exactly one lane pops each winner): lane m receives the
+// m-th best in (mh, ml); returns how many exist (the same in every lane).
+__device__ __forceinline__ int warp_topk(TopK& tk, int K, int lane, uint32_t& mh, uint32_t& ml) {
+  int n = 0;
+  mh = ml = 0u;
+  for (int round = 0; round < K; ++round) {
+    const uint32_t h = tk.hi[0], l = tk.lo[0];  // empty slots hold 0
+    const uint32_t wh = __reduce_max_sync(0xffffffffu, h);
+    if (wh == 0u) break;
+    const uint32_t wl = __reduce_max_sync(0xffffffffu, h == wh ? l : 0u);
+    if (h == wh && l == wl) tk.pop();
+    if (lane == round) {
+      mh = wh;
+      ml = wl;
+    }
+    n = round + 1;
+  }
+  return n;
+}
+
 // subpixel_gauss3 (src/correlators.jl:499-520) with FP64 logarithms.
 // (i, j) 0-based; returns 1-based refined (row, col).
 // One axis: (ln Im - ln Ip) / (2 (ln Im - 2 ln I0 + ln Ip)), formed as
@@ -209,9 +230,15 @@ __device__ __forceinline__ float moment_fp64(const float* R, int nr, int nc, int
   int r0 = (int)rintf(pr), c0 = (int)rintf(pc);  // 1-based, ties to even
   int rlo = max(1, r0 - 1), rhi = min(nr, r0 + 1), clo = max(1, c0 - 1), chi = min(nc, c0 + 1);
   if (rlo > rhi || clo > chi) return __int_as_float(0x7fc00000);
+  // the 3 x 3 neighbourhood unrolled, clipped cells skipped: the loads issue
+  // together and the sums keep the column-major order
   double sumC = 0, sdx = 0, sdy = 0;
-  for (int c = clo; c <= chi; ++c)
-    for (int r = rlo; r <= rhi; ++r) {
+#pragma unroll
+  for (int dc = -1; dc <= 1; ++dc)
+#pragma unroll
+    for (int dr = -1; dr <= 1; ++dr) {
+      const int c = c0 + dc, r = r0 + dr;
+      if (c < clo || c > chi || r < rlo || r > rhi) continue;
       double w = fmax((double)R[(c - 1) * ldr + (r - 1)], 0.0);
       float dx = __fsub_rn((float)c, pc), dy = __fsub_rn((float)r, pr);
       sumC += w;
@@ -236,8 +263,8 @@ struct PeakOut {
 };
 
 // Peak analysis of one plane by a group of threads (tid in [0, gsize)).
-// Every thread of the CTA must call this (uniform K and finder), because
-// the merge rounds synchronise the whole CTA.
+// Every thread of the group must call this (uniform K and finder), because
+// the merge synchronises the group.
 // Only the box rows [rlo, rhi] x columns [clo, chi] can hold positive
 // values (outside it the overlap gain is zero, so R is exactly 0 there); the
 // scans cover it, plus the last pixel, the only place outside where a zero
@@ -266,10 +293,10 @@ __device__ __forceinline__ ScanPlan scan_plan(int gtid, int gsize, int rlo, int 
   return sp;
 }
 
-__device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
-                              int subpixel, int gtid, int gsize, uint32_t* red, bool active, float* s_vals,
-                              int* s_locs, int64_t grid_id, int64_t job, const PeakOut& o, bool poison, int bar,
-                              const ScanPlan sp) {
+__device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
+                                             int subpixel, int gtid, int gsize, uint32_t* red, bool active,
+                                             float* s_vals, int* s_locs, int64_t grid_id, int64_t job,
+                                             const PeakOut& o, bool poison, int bar, const ScanPlan sp) {
   const int rlo = sp.rlo, rhi = sp.rhi, clo = sp.clo, chi = sp.chi;
   // a poisoned plane (non-finite window data: the reference's plane is all
   // NaN there) yields no peak, so every output is NaN
@@ -297,35 +324,47 @@ __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int l
           r1 = min(rhi + 1, r0 + rps);
         }
         if (r0 >= r1) continue;
-        const float* Cl = c > 0 ? R + (c - 1) * ldr : nullptr;
+        const bool hl = c > 0, hr = c < nc - 1;
         const float* Cc = R + c * ldr;
-        const float* Cr = c < nc - 1 ? R + (c + 1) * ldr : nullptr;
+        const float* Cl = hl ? Cc - ldr : Cc;
+        const float* Cr = hr ? Cc + ldr : Cc;
         float lt = NaNf, ct = NaNf, rt = NaNf;  // row r - 1
         if (r0 > 0) {
-          lt = Cl ? Cl[r0 - 1] : NaNf;
+          lt = hl ? Cl[r0 - 1] : NaNf;
           ct = Cc[r0 - 1];
-          rt = Cr ? Cr[r0 - 1] : NaNf;
+          rt = hr ? Cr[r0 - 1] : NaNf;
         }
-        float lm = Cl ? Cl[r0] : NaNf, cm = Cc[r0], rm = Cr ? Cr[r0] : NaNf;  // row r
-        for (int r = r0; r < r1; ++r) {
-          float lb = NaNf, cb = NaNf, rb = NaNf;  // row r + 1
-          if (r + 1 < nr) {
-            lb = Cl ? Cl[r + 1] : NaNf;
-            cb = Cc[r + 1];
-            rb = Cr ? Cr[r + 1] : NaNf;
+        float lm = hl ? Cl[r0] : NaNf, cm = Cc[r0], rm = hr ? Cr[r0] : NaNf;  // row r
+        // blocks of SU rows: the next SU rows of the three columns are loaded
+        // together, so the loads of a block overlap instead of each row
+        // waiting on its own
+        constexpr int SU = 2;
+        for (int rb0 = r0; rb0 < r1; rb0 += SU) {
+          float lb[SU], cb[SU], rbv[SU];  // rows rb0 + 1 .. rb0 + SU
+#pragma unroll
+          for (int u = 0; u < SU; ++u) {
+            const int rr = rb0 + 1 + u;
+            const bool ok = rr < nr;
+            lb[u] = ok && hl ? Cl[rr] : NaNf;
+            cb[u] = ok ? Cc[rr] : NaNf;
+            rbv[u] = ok && hr ? Cr[rr] : NaNf;
           }
-          const float v = cm;
-          if (!isnan(v)) {
-            const uint32_t h = fkey(v);
-            // a later index cannot win a tie, so a full list rejects h <= last
-            if (h > tk.thr) {
-              const float e = fmaxf(fmaxf(lt, lm), fmaxf(lb, ct));
-              const float l = fmaxf(fmaxf(rt, rm), fmaxf(rb, cb));
-              if (!(e > v) && !(l >= v)) tk.insert(h, ~(uint32_t)(r + c * nr), K);
+#pragma unroll
+          for (int u = 0; u < SU; ++u) {
+            const int r = rb0 + u;
+            const float v = cm;
+            if (r < r1 && !isnan(v)) {
+              const uint32_t h = fkey(v);
+              // a later index cannot win a tie, so a full list rejects h <= last
+              if (h > tk.thr) {
+                const float e = fmaxf(fmaxf(lt, lm), fmaxf(lb[u], ct));
+                const float l = fmaxf(fmaxf(rt, rm), fmaxf(rbv[u], cb[u]));
+                if (!(e > v) && !(l >= v)) tk.insert(h, ~(uint32_t)(r + c * nr), K);
+              }
             }
+            lt = lm; ct = cm; rt = rm;
+            lm = lb[u]; cm = cb[u]; rm = rbv[u];
           }
-          lt = lm; ct = cm; rt = rm;
-          lm = lb; cm = cb; rm = rb;
         }
       }
       if (gtid == 0 && (rhi < nr - 1 || chi < nc - 1)) {  // the last pixel, outside the box
@@ -333,19 +372,37 @@ __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int l
         if (is_local_max(R, nr, nc, ldr, r, c, R[c * ldr + r])) tk.insert(fkey(R[c * ldr + r]), ~(uint32_t)(r + c * nr), K);
       }
     }
-    bool done = false;
-    for (int round = 0; round < K; ++round) {  // every round runs: group_argmax synchronises the group
-      uint32_t whi, wlo;
-      group_argmax(tk.cnt > 0 ? tk.hi[0] : 0u, tk.cnt > 0 ? tk.lo[0] : 0u, red, gwarp, nwarps, whi, wlo, bar);
-      if (done || whi == 0u) { done = true; continue; }
-      if (tk.cnt > 0 && tk.hi[0] == whi && tk.lo[0] == wlo) tk.pop();
-      if (gtid == 0) {
-        const int lin = (int)(~wlo);
-        s_vals[round] = R[(lin / nr) * ldr + (lin % nr)];
-        s_locs[2 * round] = lin % nr;
-        s_locs[2 * round + 1] = lin / nr;
+    // Merge: each warp takes its K best from its threads' lists by shuffle
+    // rounds (lane m keeps the m-th); with several warps the warps' lists
+    // meet in `red` behind one barrier and the first warp takes the group's
+    // K best from them the same way.
+    const int lane = gtid & 31;
+    uint32_t mh = 0u, ml = 0u;
+    int nw = warp_topk(tk, K, lane, mh, ml);
+    if (nwarps > 1) {
+      if (lane < K) {
+        red[2 * (gwarp * K + lane)] = mh;
+        red[2 * (gwarp * K + lane) + 1] = ml;
       }
-      nfound = round + 1;
+      grp_sync(bar, gsize);
+      if (gwarp == 0) {
+        TopK tg;
+        tg.init();
+        for (int e = lane; e < nwarps * K; e += 32) {
+          const uint32_t h = red[2 * e], l = red[2 * e + 1];
+          if (h != 0u) tg.insert(h, l, K);
+        }
+        nw = warp_topk(tg, K, lane, mh, ml);
+      }
+    }
+    if (gwarp == 0) {
+      nfound = nw;
+      if (lane < nw) {
+        const int lin = (int)(~ml);
+        s_vals[lane] = R[(lin / nr) * ldr + (lin % nr)];
+        s_locs[2 * lane] = lin % nr;
+        s_locs[2 * lane + 1] = lin / nr;
+      }
     }
   } else {
     // exclusion finder (src/correlators.jl:390-421): K scans, box +-2
@@ -489,6 +546,16 @@ __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int l
   }
 }
 
+// The analysis as a call: small planes keep it out of line (the kernel's
+// transform stages then keep their registers); large planes inline it.
+__device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
+                                           int subpixel, int gtid, int gsize, uint32_t* red, bool active,
+                                           float* s_vals, int* s_locs, int64_t grid_id, int64_t job,
+                                           const PeakOut& o, bool poison, int bar, const ScanPlan sp) {
+  analyze_body(R, nr, nc, ldr, K, npeaks, finder, subpixel, gtid, gsize, red, active, s_vals, s_locs, grid_id, job, o,
+               poison, bar, sp);
+}
+
 // S(k) = conj(FA(k)) FB(k) of the packed transform Z = F(a + i b), from
 // X = Z(k) and Zm = Z(-k): FA = (X + conj(Zm))/2, FB = (X - conj(Zm))/(2i)
 // (spectrum!, src/correlators.jl:266-279); the phase method divides by
@@ -509,11 +576,13 @@ __device__ __forceinline__ float2 cross_spectrum(float2 X, float2 Zm, int method
 template <int N, int W> struct CorrCfg {
   static constexpr int N1 = AxisSplit<N>::N1, N2 = AxisSplit<N>::N2;
   static constexpr int WPC = N <= 32 ? 4 : (N <= 64 ? 2 : 1);    // windows per CTA
-  static constexpr int NT = N <= 48 ? 128 : (N <= 64 ? 256 : 512);
+  static constexpr int NT = N <= 48 ? 128 : (N <= 96 ? 256 : 512);
   static constexpr int G = NT / WPC;  // threads per window in the analysis
   // CTAs per SM the register budget is sized for (the shared-memory limit
   // allows at least this many)
-  static constexpr int MINB = N <= 32 ? 4 : (N <= 64 ? 3 : 1);
+  static constexpr int MINB = N <= 48 ? 4 : (N <= 64 ? 3 : (N <= 96 ? 2 : 1));
+  // the peak analysis inline (one window per CTA: its latency is the CTA's)
+  static constexpr bool INLINE_ANALYSIS = N >= 96;
   // The spectrum is Hermitian, so the inverse transforms only the N/2 + 1
   // canonical columns along p and then rows p and p + N/2 together along q
   // (their outputs are real: one lands in the real part, one in the
@@ -529,7 +598,7 @@ template <int N, int W> struct CorrCfg {
   static constexpr size_t PLANE_B = (size_t)N * LD * sizeof(float2);
   static constexpr size_t smem() {
     return WPC * PLANE_B + WPC * (G / 32) * 3 * sizeof(double) + N * sizeof(float2) +
-           WPC * (G / 32) * 2 * sizeof(uint32_t) +
+           WPC * (G / 32) * 2 * KMAX * sizeof(uint32_t) +
            WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int)) + 3 * N * sizeof(int) + 64;
   }
   static_assert(W == N || 2 * W == N, "window must equal the FFT size or half of it");
@@ -548,7 +617,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
   double* s_part = reinterpret_cast<double*>(smem_raw + WPC * C::PLANE_B);  // 3 per warp: sum A, sum B, count
   float2* tw = reinterpret_cast<float2*>(s_part + WPC * (G / 32) * 3);
   uint32_t* red = reinterpret_cast<uint32_t*>(tw + N);
-  float* s_vals = reinterpret_cast<float*>(red + WPC * (G / 32) * 2);
+  float* s_vals = reinterpret_cast<float*>(red + WPC * (G / 32) * 2 * KMAX);
   int* s_locs = reinterpret_cast<int*>(s_vals + WPC * KMAX);
   // per-axis storage tables (N2 > 1): frequency of storage slot a, storage
   // slot of the negated frequency, canonical storage columns kq = 0..N/2
@@ -933,8 +1002,13 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
       }
     }
     // ---- stage 9: peak analysis by the group
-    analyze_group(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, red + w * (G / 32) * 2, true,
-                  s_vals + w * KMAX, s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, sp);
+    uint32_t* gred = red + w * (G / 32) * 2 * KMAX;
+    if (C::INLINE_ANALYSIS)
+      analyze_body(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
+                   s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, sp);
+    else
+      analyze_group(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
+                    s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, sp);
     grp_sync(bar, G);  // the plane is reused by the group's next window
   }
 }
@@ -945,7 +1019,7 @@ __global__ void __launch_bounds__(128) analyze_planes_kernel(const AnalyzeArgs a
   float* R = reinterpret_cast<float*>(smem_raw);
   const int P = a.nr * a.nc;
   uint32_t* red = reinterpret_cast<uint32_t*>(R + P);
-  float* s_vals = reinterpret_cast<float*>(red + 8);
+  float* s_vals = reinterpret_cast<float*>(red + 8 * KMAX);
   int* s_locs = reinterpret_cast<int*>(s_vals + KMAX);
   const int K = a.npeaks > 2 ? a.npeaks : 2;
   PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
@@ -1015,7 +1089,7 @@ cudaError_t launch_correlate(const CorrArgs& a, int N, int W, cudaStream_t s, in
 
 cudaError_t launch_analyze_planes(const AnalyzeArgs& a, cudaStream_t s) {
   if (a.nplanes <= 0) return cudaSuccess;
-  const size_t sm = (size_t)a.nr * a.nc * sizeof(float) + 8 * sizeof(uint32_t) + KMAX * sizeof(float) +
+  const size_t sm = (size_t)a.nr * a.nc * sizeof(float) + 8 * KMAX * sizeof(uint32_t) + KMAX * sizeof(float) +
                     2 * KMAX * sizeof(int) + 16;
   if (sm > 200 * 1024) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(analyze_planes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

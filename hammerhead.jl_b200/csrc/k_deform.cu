@@ -37,6 +37,21 @@ static __device__ __forceinline__ float k_two_thirds() { return __int_as_float(0
 #define kSixth k_sixth()
 #define kTwoThirds k_two_thirds()
 
+// x / 6 correctly rounded for every x whose quotient is a normal float (and
+// x = 0), without a division: q0 = x * RN(1/6), then one residual correction
+// by fused multiply-add (Markstein's correction for a divisor known in
+// advance; Brisebarre, Muller and Raina, IEEE Trans. Computers 53(8), 2004).
+// A comparison with IEEE division over every positive float with a normal
+// quotient finds no difference. The B-spline weights (1-d)^3 and d^3 it
+// divides are 0 or at least 2^-72 (d is 0 or a multiple of 2^-23 in [0, 1]),
+// so their quotients are normal.
+static __device__ __forceinline__ float div6(float x) {
+  const float r = k_sixth();
+  const float q0 = __fmul_rn(x, r);
+  const float e = __fmaf_rn(-q0, 6.0f, x);
+  return __fmaf_rn(e, r, q0);
+}
+
 // Elimination factors for a line of padded length n: unknown rows
 // i = 3..n-2 (1-based). inv[k] = 1/den_k, cp[k] = (1/6)*inv[k], k = i - 3.
 __global__ void bspline_factors_kernel(int64_t n, float* cp, float* inv) {
@@ -200,10 +215,10 @@ __device__ __forceinline__ float bilinear(const float* f, const PredGrid& g, flo
 __device__ __forceinline__ void cubw(float d, float* w) {
   const float x3 = FM(FM(d, d), d), c = FS(1.f, d), c3 = FM(FM(c, c), c);
   const float two3 = kTwoThirds;
-  w[0] = FD(c3, 6.f);
+  w[0] = div6(c3);
   w[1] = FA(FS(two3, FM(d, d)), FM(x3, 0.5f));
   w[2] = FA(FS(two3, FM(c, c)), FM(c3, 0.5f));
-  w[3] = FD(x3, 6.f);
+  w[3] = div6(x3);
 }
 
 __device__ __forceinline__ float bspline_eval(const float* C, int64_t nr, int64_t nc, float yy, float xx) {
@@ -284,41 +299,158 @@ static unsigned b_blocks(int64_t n, int cap_per_sm = 16) {
   return (unsigned)(b < 1 ? 1 : b);
 }
 
-// prefilter of both frames (blockIdx.y: 0 = A, 1 = B) of every deforming pair
-__global__ void b_pad_copy_kernel(const BPair* __restrict__ bp, int npairs, int64_t qtot) {
-  const int img = blockIdx.y;
-  B_STRIDE(k, qtot) {
-    const BPair& b = bp[bp_find<&BPair::qoff>(bp, npairs, k)];
-    const int64_t ld = b.nr + 2, l = k - b.qoff;
-    if (!b.deforms || l >= ld * (b.nc + 2)) continue;
-    const int64_t i = l % ld, j = l / ld;
-    const float* src = img ? b.B : b.A;
-    float* coef = img ? b.coefB : b.coefA;
-    coef[l] = (i >= 1 && i <= b.nr && j >= 1 && j <= b.nc) ? src[(i - 1) + (j - 1) * b.nr] : 0.f;
+// prefilter of both frames (blockIdx.y: 0 = A, 1 = B) of every deforming pair.
+//
+// dim 1 (down the image columns, contiguous in memory) runs on 32-column
+// tiles: a warp takes 32 neighbouring columns and one segment, the lanes
+// load and store down each column together (coalesced) through a staged
+// tile in shared memory, and each lane then runs its own column's sweep
+// from the tile with the arithmetic of bs_fwd_item / bs_bwd_item. The
+// forward pass reads the image itself (padded element e of column j + 1 is
+// image row e - 1), and the backward pass writes every element of the
+// padded column, the copied rows 1 and n - 2 included, so no padded copy of
+// the image is made first. Work items: (column tile, segment) per pair,
+// counted from BPair::wcol.
+__device__ __forceinline__ int64_t b_nseg(int64_t n) { return n >= 5 ? (n - 4 + BS_SEG - 1) / BS_SEG : 1; }
+
+constexpr int BS_TILE = BS_WARM + BS_SEG;  // rows staged per column
+constexpr int BS_TLD = BS_TILE + 1;        // odd stride: conflict-free by lane and by row
+constexpr int BSC_WARPS = 4;
+constexpr size_t BSC_SMEM = (size_t)BSC_WARPS * 32 * BS_TLD * sizeof(float);
+
+template <int PASS>
+__global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPair* __restrict__ bp, int npairs,
+                                                                      int64_t witems, float* dbuf, int64_t qtot) {
+  extern __shared__ float bsc_tile[];
+  const int img = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* T = bsc_tile + warp * 32 * BS_TLD;
+  for (int64_t t = (int64_t)blockIdx.x * BSC_WARPS + warp; t < witems; t += (int64_t)gridDim.x * BSC_WARPS) {
+    const BPair& b = bp[bp_find<&BPair::wcol>(bp, npairs, t)];
+    if (!b.deforms) continue;  // uniform across the warp
+    const int64_t nr = b.nr, nc = b.nc, n = nr + 2, m = n - 4;
+    const int64_t ncg = (nc + 31) / 32, l = t - b.wcol;
+    if (l >= ncg * b_nseg(n)) continue;
+    const int64_t cg = l % ncg, seg = l / ncg;
+    const int ncol = (int)min((int64_t)32, nc - cg * 32);  // columns of this tile
+    const float* im = (img ? b.B : b.A) + cg * 32 * nr;       // image column cg*32
+    float* coef = (img ? b.coefB : b.coefA) + (cg * 32 + 1) * n;  // padded column cg*32 + 1
+    float* d = dbuf + (int64_t)img * qtot + b.qoff + (cg * 32 + 1) * n;
+    const bool mine = lane < ncol;
+    if (m < 1) {  // n <= 4: nothing to solve; the backward pass writes the column
+      if (PASS == 1 && mine) {
+        const float* ic = im + lane * nr;
+        float* x = coef + lane * n;
+        if (n == 4) {
+          const float c1 = ic[0], c2 = ic[1];
+          x[0] = FS(FM(2.0f, c1), c2);
+          x[1] = c1;
+          x[2] = c2;
+          x[3] = FS(FM(2.0f, c2), c1);
+        } else {  // n == 3: the padded copy as it stands
+          x[0] = 0.f;
+          x[1] = ic[0];
+          x[2] = 0.f;
+        }
+      }
+      continue;
+    }
+    const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG);
+    if (PASS == 0) {
+      const int64_t ks = max((int64_t)0, k0 - BS_WARM);
+      const int cnt = (int)(k1 - ks);
+      // stage the right-hand sides: unknown k is padded element k + 2 = image row k + 1
+      for (int c = 0; c < ncol; ++c)
+        for (int r = lane; r < cnt; r += 32) T[c * BS_TLD + r] = __ldg(im + c * nr + ks + 1 + r);
+      __syncwarp();
+      if (mine) {
+        const float* ic = im + lane * nr;
+        const float sixth = kSixth;
+        const float c2 = __ldg(ic), cn1 = __ldg(ic + nr - 1);  // padded elements 1 and n - 2
+        float* x = T + lane * BS_TLD;
+        float dv = 0.f;
+        for (int64_t k = ks; k < k1; ++k) {
+          float rhs = x[k - ks];
+          if (k == 0) rhs = FS(rhs, FM(sixth, c2));
+          if (k == m - 1) rhs = FS(rhs, FM(sixth, cn1));
+          dv = k == 0 ? FM(rhs, __ldg(b.ivc)) : FM(FS(rhs, FM(sixth, dv)), __ldg(b.ivc + k));
+          x[k - ks] = dv;
+        }
+      }
+      __syncwarp();
+      const int nout = (int)(k1 - k0), o = (int)(k0 - ks);
+      for (int c = 0; c < ncol; ++c)
+        for (int r = lane; r < nout; r += 32) d[c * n + k0 + 2 + r] = T[c * BS_TLD + o + r];
+      __syncwarp();  // the tile is restaged by the next item
+    } else {
+      const int64_t ke = min(m - 1, k1 - 1 + BS_WARM);
+      const int cnt = (int)(ke - k0 + 1);
+      for (int c = 0; c < ncol; ++c)
+        for (int r = lane; r < cnt; r += 32) T[c * BS_TLD + r] = d[c * n + k0 + 2 + r];
+      __syncwarp();
+      if (mine) {
+        float* x = T + lane * BS_TLD;
+        float xv = 0.f, xlast = 0.f;
+        for (int64_t k = ke; k >= k0; --k) {
+          const float dk = x[k - k0];
+          xv = k == ke ? dk : FS(dk, FM(__ldg(b.cpc + k), xv));
+          x[k - k0] = xv;
+          if (k == m - 1) xlast = xv;
+        }
+        const float* ic = im + lane * nr;
+        float* xc = coef + lane * n;
+        if (k0 == 0) {  // padded element 1 is image row 0; element 0 the "Line" boundary
+          const float c1 = __ldg(ic);
+          xc[1] = c1;
+          xc[0] = FS(FM(2.0f, c1), xv);  // xv == x_0 here
+        }
+        if (k1 == m) {
+          const float cn = __ldg(ic + nr - 1);
+          xc[n - 2] = cn;
+          xc[n - 1] = FS(FM(2.0f, cn), xlast);
+        }
+      }
+      __syncwarp();
+      const int nout = (int)(k1 - k0);
+      for (int c = 0; c < ncol; ++c)
+        for (int r = lane; r < nout; r += 32) coef[c * n + k0 + 2 + r] = T[c * BS_TLD + r];
+      __syncwarp();
+    }
   }
 }
 
-__device__ __forceinline__ int64_t b_nseg(int64_t n) { return n >= 5 ? (n - 4 + BS_SEG - 1) / BS_SEG : 1; }
+// Padding columns 0 and nc + 1 are written by the row pass's "Line"
+// boundary; only rows too short to solve (nc + 2 < 4) keep them zero.
+__global__ void b_pad_cols_kernel(const BPair* __restrict__ bp, int npairs) {
+  const int img = blockIdx.y;
+  for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
+    const BPair& b = bp[p];
+    if (!b.deforms || b.nc + 2 >= 4) continue;
+    const int64_t n = b.nr + 2;
+    float* coef = img ? b.coefB : b.coefA;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+      coef[i] = 0.f;
+      coef[(b.nc + 1) * n + i] = 0.f;
+    }
+  }
+}
 
-// dim 1 (image columns, pass 0 = forward, 1 = backward) or dim 2 (padded rows)
-template <int DIM, int PASS>
-__global__ void b_bspline_kernel(const BPair* __restrict__ bp, int npairs, int64_t wtot, float* dbuf, int64_t qtot) {
+// dim 2 (padded rows, consecutive threads on consecutive rows: coalesced)
+template <int PASS>
+__global__ void b_bspline_row_kernel(const BPair* __restrict__ bp, int npairs, int64_t wtot, float* dbuf, int64_t qtot) {
   const int img = blockIdx.y;
   B_STRIDE(t, wtot) {
-    const BPair& b = bp[bp_find<DIM == 1 ? &BPair::wcol : &BPair::wrow>(bp, npairs, t)];
+    const BPair& b = bp[bp_find<&BPair::wrow>(bp, npairs, t)];
     if (!b.deforms) continue;
     const int64_t ld = b.nr + 2, ncols = b.nc + 2;
-    const int64_t n = DIM == 1 ? ld : ncols;
-    const int64_t nlines = DIM == 1 ? b.nc : ld;
-    const int64_t l = t - (DIM == 1 ? b.wcol : b.wrow);
+    const int64_t n = ncols, nlines = ld;
+    const int64_t l = t - b.wrow;
     if (l >= nlines * b_nseg(n)) continue;
     float* coef = img ? b.coefB : b.coefA;
     float* d = dbuf + (int64_t)img * qtot + b.qoff;
-    const int64_t off = DIM == 1 ? ld : 0, es = DIM == 1 ? 1 : ld, ls = DIM == 1 ? ld : 1;
     if (PASS == 0) {
-      if (n - 4 >= 1) bs_fwd_item(coef + off, d + off, n, es, ls, nlines, DIM == 1 ? b.ivc : b.ivr, l);
+      if (n - 4 >= 1) bs_fwd_item(coef, d, n, ld, 1, nlines, b.ivr, l);
     } else {
-      if (n >= 4) bs_bwd_item(coef + off, d + off, n, es, ls, nlines, DIM == 1 ? b.cpc : b.cpr, l);
+      if (n >= 4) bs_bwd_item(coef, d, n, ld, 1, nlines, b.cpr, l);
     }
   }
 }
@@ -326,14 +458,25 @@ __global__ void b_bspline_kernel(const BPair* __restrict__ bp, int npairs, int64
 cudaError_t launch_b_prefilter(const BPair* bp, int npairs, int64_t qtot, int64_t wcol_tot, int64_t wrow_tot,
                                float* dbuf, cudaStream_t s) {
   if (qtot <= 0) return cudaSuccess;
-  b_pad_copy_kernel<<<dim3(b_blocks(qtot), 2), 256, 0, s>>>(bp, npairs, qtot);
-  if (wcol_tot > 0) {
-    b_bspline_kernel<1, 0><<<dim3(b_blocks(wcol_tot, 32), 2), 256, 0, s>>>(bp, npairs, wcol_tot, dbuf, qtot);
-    b_bspline_kernel<1, 1><<<dim3(b_blocks(wcol_tot, 32), 2), 256, 0, s>>>(bp, npairs, wcol_tot, dbuf, qtot);
+  static bool attr_set = false;
+  if (!attr_set) {
+    for (cudaError_t e : {cudaFuncSetAttribute(b_bspline_col_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)BSC_SMEM),
+                          cudaFuncSetAttribute(b_bspline_col_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)BSC_SMEM)})
+      if (e != cudaSuccess) return e;
+    attr_set = true;
   }
+  if (wcol_tot > 0) {
+    int64_t blocks = (wcol_tot + BSC_WARPS - 1) / BSC_WARPS;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    b_bspline_col_kernel<0><<<dim3((unsigned)blocks, 2), 32 * BSC_WARPS, BSC_SMEM, s>>>(bp, npairs, wcol_tot, dbuf, qtot);
+    b_bspline_col_kernel<1><<<dim3((unsigned)blocks, 2), 32 * BSC_WARPS, BSC_SMEM, s>>>(bp, npairs, wcol_tot, dbuf, qtot);
+  }
+  b_pad_cols_kernel<<<dim3(npairs < 148 ? npairs : 148, 2), 128, 0, s>>>(bp, npairs);
   if (wrow_tot > 0) {
-    b_bspline_kernel<2, 0><<<dim3(b_blocks(wrow_tot, 32), 2), 256, 0, s>>>(bp, npairs, wrow_tot, dbuf, qtot);
-    b_bspline_kernel<2, 1><<<dim3(b_blocks(wrow_tot, 32), 2), 256, 0, s>>>(bp, npairs, wrow_tot, dbuf, qtot);
+    b_bspline_row_kernel<0><<<dim3(b_blocks(wrow_tot, 32), 2), 256, 0, s>>>(bp, npairs, wrow_tot, dbuf, qtot);
+    b_bspline_row_kernel<1><<<dim3(b_blocks(wrow_tot, 32), 2), 256, 0, s>>>(bp, npairs, wrow_tot, dbuf, qtot);
   }
   return cudaGetLastError();
 }

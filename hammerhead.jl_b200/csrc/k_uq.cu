@@ -248,34 +248,49 @@ __global__ void __launch_bounds__(UQ_THREADS) uq_kernel(const UQArgs a, const UQ
 // covariance sums are register FMAs plus one shuffle per neighbour column
 // and row; the per-lane partial sums are combined through shared memory in
 // a fixed order. Same FP32 operations as uq_kernel, FP64 sums.
-constexpr int UQW_WINDOWS = 2;  // windows per CTA
-constexpr int UQW_THREADS = 64 * UQW_WINDOWS;
+// When dC has at most 16 columns (W <= 17) a warp serves two windows, one
+// per 16-lane segment (shuffles of width 16), so no lane idles for want of
+// a column.
+constexpr int UQW_THREADS = 128;  // two warp pairs (u, v)
 
 template <int W> struct UQWCfg {
   static constexpr int LD = W + 1;  // odd column stride: conflict-free column and row walks
   static constexpr int M = W - 1;   // columns of dC
+  static constexpr int WPW = M <= 16 ? 2 : 1;  // windows per warp
+  static constexpr int SEG = 32 / WPW;         // lanes per window
+  static constexpr int NWIN = 2 * WPW;         // windows per CTA
   static constexpr size_t win_bytes = 2 * (size_t)LD * W * sizeof(float) + (size_t)W * W;
-  static constexpr size_t part_bytes = (44 * 33 + 44) * sizeof(double);  // per warp: partials + totals
-  static constexpr size_t smem() { return UQW_WINDOWS * win_bytes + 2 * UQW_WINDOWS * part_bytes + 16; }
-  static constexpr int MINB = W <= 16 ? 4 : 2;  // CTAs per SM the register budget is sized for
+  static constexpr size_t part_bytes = (44 * 33 + 44 * WPW) * sizeof(double);  // per warp: partials + totals
+  static constexpr size_t smem() { return NWIN * win_bytes + 4 * part_bytes + 16; }
+  static constexpr int MINB = W <= 16 ? 3 : 2;  // CTAs per SM the register budget is sized for
 };
+
+// sum over the lanes of one SEG-lane segment
+template <int SEG> __device__ __forceinline__ double seg_sum(double v) {
+#pragma unroll
+  for (int o = SEG / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
 
 template <int W>
 __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(const UQArgs a, const UQOffsets o) {
   using C = UQWCfg<W>;
-  constexpr int LD = C::LD, M = C::M;
+  constexpr int LD = C::LD, M = C::M, WPW = C::WPW, SEG = C::SEG, NWIN = C::NWIN;
+  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* part_all = reinterpret_cast<double*>(smem_raw);  // [warp][44][33]
-  unsigned char* wbase = smem_raw + 2 * UQW_WINDOWS * C::part_bytes;
+  double* part_all = reinterpret_cast<double*>(smem_raw);  // [warp][44][33] + totals
+  unsigned char* wbase = smem_raw + 4 * C::part_bytes;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int slot = warp >> 1, comp = warp & 1, t64 = tid & 63;
+  const int comp = warp & 1, seg = lane / SEG, c = lane % SEG;
+  const int slot = (warp >> 1) * WPW + seg;  // window of this lane
+  const int ts = comp * SEG + c;             // this lane among the 2*SEG threads of its window
   float* wa = reinterpret_cast<float*>(wbase + slot * C::win_bytes);  // W x W, column stride LD
   float* wb = wa + LD * W;
   uint8_t* mf = reinterpret_cast<uint8_t*>(wb + LD * W);
-  double* part = part_all + warp * (44 * 33 + 44);
-  for (int64_t base = (int64_t)blockIdx.x * UQW_WINDOWS; base < a.njobs; base += (int64_t)gridDim.x * UQW_WINDOWS) {
+  double* part = part_all + warp * (C::part_bytes / sizeof(double));
+  for (int64_t base = (int64_t)blockIdx.x * NWIN; base < a.njobs; base += (int64_t)gridDim.x * NWIN) {
     const int64_t job = base + slot;
-    // ---- the window's source (uniform within the warp pair)
+    // ---- the window's source (uniform within the window's lanes)
     bool on = job < a.njobs;
     const float* A = a.A;
     const float* B = a.B;
@@ -302,36 +317,47 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
         gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
       }
     }
-    // ---- raw windows into shared memory (both warps of the window)
-    if (on)
-      for (int k = t64; k < W * W; k += 64) {
+    // with two windows per warp every lane runs the arithmetic below (the
+    // shuffles span the warp, whose windows may differ in `on`); a window
+    // that is off computes on zeros and writes nothing. With one window per
+    // warp `on` is uniform and an idle warp pair skips the work.
+    const bool run = WPW == 1 ? on : true;
+    if (run)
+      for (int k = ts; k < W * W; k += 2 * SEG) {
         const int p = k % W, q = k / W;
-        const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * ld;
-        wa[p + q * LD] = __ldg(A + off);
-        wb[p + q * LD] = __ldg(B + off);
-        mf[k] = Mk ? __ldg(Mk + off) : 0;
+        float va = 0.f, vb = 0.f;
+        uint8_t mk = 1;
+        if (on) {
+          const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * ld;
+          va = __ldg(A + off);
+          vb = __ldg(B + off);
+          mk = Mk ? __ldg(Mk + off) : 0;
+        }
+        wa[p + q * LD] = va;
+        wb[p + q * LD] = vb;
+        mf[k] = mk;
       }
     __syncthreads();
     // ---- window means (load_uncertainty_windows!), FP64, computed by each warp
     float ma = 0.f, mb = 0.f;
-    if (on) {
+    if (run) {
       double sa = 0.0, sb = 0.0, cnt = 0.0;
-      for (int k = lane; k < W * W; k += 32)
+      for (int k = c; k < W * W; k += SEG)
         if (!mf[k]) {
           const int p = k % W, q = k / W;
           sa += (double)wa[p + q * LD];
           sb += (double)wb[p + q * LD];
           cnt += 1.0;
         }
-      sa = warp_sum(sa);
-      sb = warp_sum(sb);
-      cnt = warp_sum(cnt);
+      sa = seg_sum<SEG>(sa);
+      sb = seg_sum<SEG>(sb);
+      cnt = seg_sum<SEG>(cnt);
       ma = cnt > 0 ? (float)(sa / cnt) : 0.f;
       mb = cnt > 0 ? (float)(sb / cnt) : 0.f;
     }
     __syncthreads();  // every read of the raw values precedes the apodized writes
-    if (on)
-      for (int k = t64; k < W * W; k += 64) {
+    if (run)
+      for (int k = ts; k < W * W; k += 2 * SEG) {
         const int p = k % W, q = k / W;
         const float ap = __ldg(a.apod + k);
         const float va = wa[p + q * LD], vb = wb[p + q * LD];
@@ -339,9 +365,8 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
         wb[p + q * LD] = mf[k] ? 0.f : __fmul_rn(ap, __fsub_rn(vb, mb));
       }
     __syncthreads();
-    if (on) {
+    if (run) {
       // ---- this component's dC column (lane c < M), and the C0 / C+ / C- sums
-      const int c = lane;
       const bool col = c < M;
       const int cc = col ? c : 0;
       float dcol[W];
@@ -364,15 +389,15 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
       double msum = 0.0;
 #pragma unroll
       for (int r = 0; r < W; ++r) {
-        const float left = __shfl_up_sync(0xffffffffu, dcol[r], 1);
-        const float right = __shfl_down_sync(0xffffffffu, dcol[r], 1);
+        const float left = __shfl_up_sync(FULL, dcol[r], 1, SEG);
+        const float right = __shfl_down_sync(FULL, dcol[r], 1, SEG);
         const float l = c > 0 ? left : dcol[r];
         const float rr = c < M - 1 ? right : dcol[r];
         const float v = __fmul_rn(0.25f, __fadd_rn(__fadd_rn(l, __fmul_rn(2.0f, dcol[r])), rr));
         dd[r] = (double)v;
         if (col) msum += dd[r];
       }
-      const double mu = warp_sum(msum) / (double)(W * M);
+      const double mu = seg_sum<SEG>(msum) / (double)(W * M);
 #pragma unroll
       for (int r = 0; r < W; ++r) dd[r] = col ? dd[r] - mu : 0.0;
       // ---- S00 and the covariance sums: acc[dc][dr + 4] pairs (r, c) with
@@ -408,7 +433,7 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
           const bool ok = c + dc < M;
 #pragma unroll
           for (int r2 = 0; r2 < W; ++r2) {
-            double x = __shfl_down_sync(0xffffffffu, dd[r2], dc);
+            double x = __shfl_down_sync(FULL, dd[r2], dc, SEG);
             x = ok ? x : 0.0;
 #pragma unroll
             for (int dr = -4; dr <= 4; ++dr) {
@@ -423,19 +448,37 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
           for (int jj = 0; jj < 9; ++jj) part[(8 + 9 * (dg - 1 + i) + jj) * 33 + lane] = acc[i][jj];
       }
       __syncwarp();
+      // ---- per window and statistic, the sum of the M column lanes' partials
+      //      in lane order (the other lanes hold zeros)
       double* tot = part + 44 * 33;
-      for (int st = lane; st < 44; st += 32) {
+      bool on_s[WPW];
+      int64_t job_s[WPW];
+#pragma unroll
+      for (int g = 0; g < WPW; ++g) {
+        on_s[g] = __shfl_sync(FULL, on, g * SEG);
+        job_s[g] = base + (warp >> 1) * WPW + g;
+      }
+      for (int j = lane; j < 44 * WPW; j += 32) {
+        const int g = j / 44, st = j % 44;
         double t = 0.0;
-        for (int l = 0; l < 32; ++l) t += part[st * 33 + l];
+        for (int l = 0; l < (WPW == 1 ? 32 : M); ++l) t += part[st * 33 + g * SEG + l];
         const int ri = st < 4 ? st : 4 + o.nat2ring[st - 4];
-        tot[ri] = t;
-        if (a.stats) {
-          if (a.accumulate) a.stats[job * 88 + comp * 44 + ri] += t;
-          else a.stats[job * 88 + comp * 44 + ri] = t;
+        tot[g * 44 + ri] = t;
+        bool og = on_s[0];
+        int64_t jg = job_s[0];
+#pragma unroll
+        for (int h = 1; h < WPW; ++h)
+          if (g == h) {
+            og = on_s[h];
+            jg = job_s[h];
+          }
+        if (og && a.stats) {
+          if (a.accumulate) a.stats[jg * 88 + comp * 44 + ri] += t;
+          else a.stats[jg * 88 + comp * 44 + ri] = t;
         }
       }
       __syncwarp();
-      if (lane == 0 && a.unc_u) (comp == 0 ? a.unc_u : a.unc_v)[gid] = uq_finalize(tot, o);
+      if (c == 0 && on && a.unc_u) (comp == 0 ? a.unc_u : a.unc_v)[gid] = uq_finalize(tot + seg * 44, o);
     }
     __syncthreads();  // the window buffers are reused by the next iteration
   }
@@ -461,7 +504,7 @@ template <int W> static cudaError_t launch_uq_warp(const UQArgs& a, cudaStream_t
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   int64_t grid = (int64_t)per_sm * num_sms;
-  const int64_t units = (a.njobs + UQW_WINDOWS - 1) / UQW_WINDOWS;
+  const int64_t units = (a.njobs + C::NWIN - 1) / C::NWIN;
   if (grid > units) grid = units;
   uq_warp_kernel<W><<<(unsigned)grid, UQW_THREADS, sm, s>>>(a, offs);
   return cudaGetLastError();
