@@ -68,6 +68,10 @@ hh_status run_schedule(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr
   HH_TRY(buf(ctx, "outl2", Gmax, &outl2));
   HH_TRY(buf(ctx, "gmask", Gmax, &gm));
   HH_TRY(buf(ctx, "jobs", 4 * Jmax, &djobs));
+  size_t recw = 0;
+  for (int k = 0; k < np; ++k) recw = std::max(recw, hh::correlate_record_words(passes[k].n_peaks));
+  float* prec;
+  HH_TRY(buf(ctx, "peakrec", (size_t)Jmax * recw, &prec));
 
   // events for per-pass device time
   while ((int)ctx->events.size() < np + 1) {
@@ -182,6 +186,7 @@ hh_status run_schedule(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr
       ca.alt_u = nalt > 0 ? altu : nullptr;
       ca.alt_v = nalt > 0 ? altv : nullptr;
       ca.nalt = nalt;
+      ca.rec = prec;
       HH_K(HH_K_CORRELATE, 1, corr_flops(N, njobs), corr_bytes(W, nalt, njobs), njobs, hh::launch_correlate(ca, N, W, s, ctx->num_sms));
       if (fused_unc) {
         hh::UQArgs ua{srcA, srcB, dmask, nr, djobs, njobs, ny, W, tb.apod, nullptr, uncu, uncv};
@@ -655,6 +660,8 @@ static hh_status hook_correlate(hh_ctx* ctx, const hh_pass_desc* p, const int32_
   if (out) HH_TRY(buf(ctx, "hook_packed", (size_t)(5 + 2 * (K - 1)) * njobs, &dpk));
   if (locs) HH_TRY(buf(ctx, "hook_locs", (size_t)2 * K * njobs, &dlc));
   if (planes) HH_TRY(buf(ctx, "hook_planes", (size_t)N * N * njobs, &dpl));
+  float* drec;
+  HH_TRY(buf(ctx, "hook_rec", hh::correlate_record_words(p->n_peaks) * njobs, &drec));
   CorrArgs ca{};
   ca.A = ctx->curA;
   ca.B = ctx->curB;
@@ -675,6 +682,7 @@ static hh_status hook_correlate(hh_ctx* ctx, const hh_pass_desc* p, const int32_
   ca.packed = dpk;
   ca.locs = dlc;
   ca.planes = dpl;
+  ca.rec = drec;
   HH_K(HH_K_CORRELATE, 1, 0, 0, 0, hh::launch_correlate(ca, N, W, s, ctx->num_sms));
   if (uq) {
     HH_TRY(buf(ctx, "hook_uq", (size_t)88 * njobs, &duq));

@@ -52,6 +52,7 @@ struct BPlan {
   int32_t* d_sweeps = nullptr;
   uint8_t* d_gmask = nullptr;
   float *warpA = nullptr, *warpB = nullptr, *coefA = nullptr, *coefB = nullptr, *dbuf = nullptr;
+  float* rec = nullptr;  // peak records of a correlation launch
   float *stageA = nullptr, *stageB = nullptr;
   uint16_t *stage16A = nullptr, *stage16B = nullptr;  // host UInt16 frames before conversion
   uint8_t* stageM = nullptr;
@@ -374,6 +375,12 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
       c.hjobs.shrink_to_fit();
     }
   }
+  // peak records of the largest correlation launch (launches of a sweep run
+  // one after another on the stream, so they share it)
+  size_t recw = 0;
+  for (const auto& S : P.slots)
+    for (const auto& c : S.classes) recw = std::max(recw, (size_t)c.njobs * hh::correlate_record_words(c.npeaks));
+  HH_TRY(plan_alloc(ctx, P, recw, &P.rec));
   return HH_OK;
 }
 
@@ -423,6 +430,7 @@ static hh_status issue(hh_ctx* ctx, BPlan& P) {
         ca.bp = T;
         ca.done = P.d_done;
         ca.it = it;
+        ca.rec = P.rec;
         HH_K(HH_K_CORRELATE, 1, corr_flops(c.N, c.njobs), corr_bytes(c.W, c.npeaks - 1, c.njobs), c.njobs,
              hh::launch_correlate(ca, c.N, c.W, s, ctx->num_sms));
       }

@@ -46,11 +46,16 @@ struct CorrArgs {
   // fftshifted rows/columns [box_lo, box_hi] outside which the overlap gain
   // is zero (box_hi == 0: the whole plane)
   int32_t box_lo, box_hi;
+  // peak records (correlate_record_words(npeaks) x njobs floats) or nullptr:
+  // with regional maxima the per-window outputs are then formed by a
+  // one-thread-per-window epilogue kernel after the correlation kernel
+  float* rec;
 };
 
 // Launch the correlation kernel for FFT size N (square) and window W.
 cudaError_t launch_correlate(const CorrArgs& a, int N, int W, cudaStream_t s, int num_sms);
 bool correlate_supported(int N, int W);
+size_t correlate_record_words(int npeaks);  // per job
 size_t correlate_smem_bytes(int N, int W);
 
 // Device peak analysis of caller-supplied planes.

@@ -176,6 +176,27 @@ __device__ __forceinline__ int warp_topk(TopK& tk, int K, int lane, uint32_t& mh
   return n;
 }
 
+// Plane access for the subpixel and moment arithmetic: value at (row i,
+// column j), 0-based. PlaneAcc reads a column-major plane with leading
+// dimension ld; RecAcc reads a w x w patch around a peak kept in a peak
+// record (column-major, `stride` words between consecutive cells).
+struct PlaneAcc {
+  const float* p;
+  int ld;
+  __device__ __forceinline__ float operator()(int i, int j) const { return p[j * ld + i]; }
+};
+struct RecAcc {
+  const float* p;
+  int64_t stride;
+  int i0, j0, w;  // patch origin and size
+  __device__ __forceinline__ float operator()(int i, int j) const {
+    // cells the arithmetic reads lie inside the patch; the clamp only keeps
+    // every read inside the record
+    const int di = min(max(i - i0, 0), w - 1), dj = min(max(j - j0, 0), w - 1);
+    return __ldg(p + (int64_t)(dj * w + di) * stride);
+  }
+};
+
 // subpixel_gauss3 (src/correlators.jl:499-520) with FP64 logarithms.
 // (i, j) 0-based; returns 1-based refined (row, col).
 // One axis: (ln Im - ln Ip) / (2 (ln Im - 2 ln I0 + ln Ip)), formed as
@@ -188,23 +209,23 @@ __device__ __forceinline__ double gauss3_axis(float Im, float I0, float Ip) {
   return den != 0.0 ? log(m / p) / (2.0 * den) : 0.0;
 }
 
-__device__ __forceinline__ void gauss3_fp64(const float* R, int nr, int nc, int ldr, int i, int j, float* out) {
+template <class Acc> __device__ __forceinline__ void gauss3_fp64(const Acc& R, int nr, int nc, int i, int j, float* out) {
   double di = 0.0, dj = 0.0;
-  const float I0 = R[j * ldr + i];
-  if (i > 0 && i < nr - 1) di = gauss3_axis(R[j * ldr + i - 1], I0, R[j * ldr + i + 1]);
-  if (j > 0 && j < nc - 1) dj = gauss3_axis(R[(j - 1) * ldr + i], I0, R[(j + 1) * ldr + i]);
+  const float I0 = R(i, j);
+  if (i > 0 && i < nr - 1) di = gauss3_axis(R(i - 1, j), I0, R(i + 1, j));
+  if (j > 0 && j < nc - 1) dj = gauss3_axis(R(i, j - 1), I0, R(i, j + 1));
   out[0] = (float)((double)(i + 1) + di);
   out[1] = (float)((double)(j + 1) + dj);
 }
 
 // subpixel_gauss9 (src/correlators.jl:534-564) with FP64 logarithms.
-__device__ __forceinline__ void gauss9_fp64(const float* R, int nr, int nc, int ldr, int pr, int pc, float* out) {
-  if (!(pr > 0 && pr < nr - 1 && pc > 0 && pc < nc - 1)) return gauss3_fp64(R, nr, nc, ldr, pr, pc, out);
+template <class Acc> __device__ __forceinline__ void gauss9_fp64(const Acc& R, int nr, int nc, int pr, int pc, float* out) {
+  if (!(pr > 0 && pr < nr - 1 && pc > 0 && pc < nc - 1)) return gauss3_fp64(R, nr, nc, pr, pc, out);
   double sL = 0, sxL = 0, syL = 0, sxxL = 0, syyL = 0, sxyL = 0;
   for (int dj = -1; dj <= 1; ++dj)
     for (int di = -1; di <= 1; ++di) {
-      float val = R[(pc + dj) * ldr + pr + di];
-      if (!(val > 0.f)) return gauss3_fp64(R, nr, nc, ldr, pr, pc, out);
+      float val = R(pr + di, pc + dj);
+      if (!(val > 0.f)) return gauss3_fp64(R, nr, nc, pr, pc, out);
       double L = log((double)val);
       sL += L;
       sxL += dj * L;
@@ -215,17 +236,17 @@ __device__ __forceinline__ void gauss9_fp64(const float* R, int nr, int nc, int 
     }
   double a1 = sxL / 6, a2 = syL / 6, a3 = sxxL / 2 - sL / 3, a4 = sxyL / 4, a5 = syyL / 2 - sL / 3;
   double D = 4 * a3 * a5 - a4 * a4;
-  if (!(a3 < 0 && D > 0)) return gauss3_fp64(R, nr, nc, ldr, pr, pc, out);
+  if (!(a3 < 0 && D > 0)) return gauss3_fp64(R, nr, nc, pr, pc, out);
   double dx = (a4 * a2 - 2 * a5 * a1) / D;
   double dy = (a4 * a1 - 2 * a3 * a2) / D;
-  if (!(fabs(dx) <= 1 && fabs(dy) <= 1)) return gauss3_fp64(R, nr, nc, ldr, pr, pc, out);
+  if (!(fabs(dx) <= 1 && fabs(dy) <= 1)) return gauss3_fp64(R, nr, nc, pr, pc, out);
   out[0] = (float)((double)(pr + 1) + dy);
   out[1] = (float)((double)(pc + 1) + dx);
 }
 
 // calculate_correlation_moment (src/quality.jl:49-74, neighbourhood 3):
 // (c - pc)^2 in float like the Float32 reference, sums in FP64.
-__device__ __forceinline__ float moment_fp64(const float* R, int nr, int nc, int ldr, float pr, float pc) {
+template <class Acc> __device__ __forceinline__ float moment_fp64(const Acc& R, int nr, int nc, float pr, float pc) {
   if (!(isfinite(pr) && isfinite(pc))) return __int_as_float(0x7fc00000);
   int r0 = (int)rintf(pr), c0 = (int)rintf(pc);  // 1-based, ties to even
   int rlo = max(1, r0 - 1), rhi = min(nr, r0 + 1), clo = max(1, c0 - 1), chi = min(nc, c0 + 1);
@@ -239,7 +260,7 @@ __device__ __forceinline__ float moment_fp64(const float* R, int nr, int nc, int
     for (int dr = -1; dr <= 1; ++dr) {
       const int c = c0 + dc, r = r0 + dr;
       if (c < clo || c > chi || r < rlo || r > rhi) continue;
-      double w = fmax((double)R[(c - 1) * ldr + (r - 1)], 0.0);
+      double w = fmax((double)R(r - 1, c - 1), 0.0);
       float dx = __fsub_rn((float)c, pc), dy = __fsub_rn((float)r, pr);
       sumC += w;
       sdx += (double)__fmul_rn(dx, dx) * w;
@@ -261,6 +282,104 @@ struct PeakOut {
   float* packed;
   int32_t* locs;
 };
+
+// Peak record of one window (regional maxima), written by the correlation
+// kernel in place of its epilogue and read by peak_epilogue_kernel: word w
+// of job j at rec[w * njobs + j]. Words: 0 the number of peaks found (-1:
+// window skipped), 1..K their values, then (row, col) per peak, then the
+// 5 x 5 plane patch around the primary and a 3 x 3 patch around each
+// alternative (column-major, cells outside the plane 0). A regional maximum
+// is >= its neighbours, so its gauss3 offsets stay within 1/2 px and its
+// gauss9 offsets within 1 px; the fits and the 3 x 3 moment around the
+// refined primary therefore read only cells inside these patches.
+__host__ __device__ constexpr int rec_words(int K) { return 17 + 12 * K; }
+__device__ __forceinline__ int rec_patch(int K, int m) { return m == 0 ? 1 + 3 * K : 1 + 3 * K + 25 + 9 * (m - 1); }
+
+// where the epilogue reads peak m's neighbourhood: the plane itself ...
+struct PlaneSrc {
+  const float* R;
+  int ld;
+  __device__ __forceinline__ PlaneAcc at(int, int, int) const { return PlaneAcc{R, ld}; }
+};
+// ... or the patches of a peak record
+struct RecSrc {
+  const float* rec;  // rec + job
+  int64_t stride;
+  int K;
+  __device__ __forceinline__ RecAcc at(int m, int pr, int pc) const {
+    const int h = m == 0 ? 2 : 1;
+    return RecAcc{rec + (int64_t)rec_patch(K, m) * stride, stride, pr - h, pc - h, 2 * h + 1};
+  }
+};
+
+// The per-window outputs from the peaks found (analyze_plane!'s tail,
+// src/correlators.jl:459-468): the primary refined by the chosen subpixel
+// method, displacement from the plane centre, peak ratio and moment; the
+// alternatives 1..npeaks-1 refined by gauss3; 1-based peak locations.
+template <class Src>
+__device__ void peak_outputs(const Src& src, int nr, int nc, int K, int npeaks, int subpixel, int nfound,
+                             const float* vals, const int* locs, int64_t grid_id, int64_t job, const PeakOut& o) {
+  int found = 0;
+  if (nfound > 0) {
+    found = 1;
+    while (found < nfound && vals[found] > 0.f) ++found;
+  }
+  const float NaN = __int_as_float(0x7fc00000);
+  const int cr = nr / 2 + 1, cc = nc / 2 + 1;
+  const int mmax = found < npeaks ? found : npeaks;  // peaks 1..mmax carry results
+  float* pk = o.packed ? o.packed + job * (int64_t)(5 + 2 * (K - 1)) : nullptr;
+  for (int m = 0; m < K; ++m) {
+    float ref[2] = {NaN, NaN};
+    if (m < found && (m == 0 || m < mmax)) {
+      const int pr = locs[2 * m], pc = locs[2 * m + 1];
+      const auto R = src.at(m, pr, pc);
+      if (m == 0 && subpixel == 1) gauss9_fp64(R, nr, nc, pr, pc, ref);
+      else if (m == 0 && subpixel == 3) {
+        ref[0] = (float)(pr + 1);
+        ref[1] = (float)(pc + 1);
+      } else gauss3_fp64(R, nr, nc, pr, pc, ref);
+    }
+    const float d_col = ref[1] - (float)cc, d_row = ref[0] - (float)cr;
+    if (m == 0) {
+      float ratio = NaN, mom = NaN;
+      if (found > 0) {
+        const float v1 = vals[0];
+        ratio = found >= 2 ? v1 / vals[1] : (v1 > 0.f ? INFINITY : NaN);
+        mom = moment_fp64(src.at(0, locs[0], locs[1]), nr, nc, ref[0], ref[1]);
+      }
+      if (grid_id >= 0 && o.du) {
+        o.du[grid_id] = d_col;
+        o.dv[grid_id] = d_row;
+        o.ratio[grid_id] = ratio;
+        o.moment[grid_id] = mom;
+      }
+      if (pk) {
+        pk[0] = d_col;
+        pk[1] = d_row;
+        pk[2] = ratio;
+        pk[3] = mom;
+        pk[4] = (float)found;
+      }
+    } else {
+      // alternative peak m (0-based): result only while m < min(found, npeaks)
+      const bool has = m < mmax;
+      const float au = has ? d_col : NaN, av = has ? d_row : NaN;
+      if (grid_id >= 0 && o.alt_u && m - 1 < o.nalt) {
+        o.alt_u[grid_id + (int64_t)(m - 1) * o.G] = au;
+        o.alt_v[grid_id + (int64_t)(m - 1) * o.G] = av;
+      }
+      if (pk) {
+        pk[5 + (m - 1)] = au;
+        pk[5 + (K - 1) + (m - 1)] = av;
+      }
+    }
+    if (o.locs) {
+      int32_t* lc = o.locs + job * (int64_t)(2 * K);
+      lc[2 * m] = m < found ? locs[2 * m] + 1 : 0;
+      lc[2 * m + 1] = m < found ? locs[2 * m + 1] + 1 : 0;
+    }
+  }
+}
 
 // Peak analysis of one plane by a group of threads (tid in [0, gsize)).
 // Every thread of the group must call this (uniform K and finder), because
@@ -296,7 +415,8 @@ __device__ __forceinline__ ScanPlan scan_plan(int gtid, int gsize, int rlo, int 
 __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
                                              int subpixel, int gtid, int gsize, uint32_t* red, bool active,
                                              float* s_vals, int* s_locs, int64_t grid_id, int64_t job,
-                                             const PeakOut& o, bool poison, int bar, const ScanPlan sp) {
+                                             const PeakOut& o, bool poison, int bar, const ScanPlan sp,
+                                             float* rec, int64_t rec_stride) {
   const int rlo = sp.rlo, rhi = sp.rhi, clo = sp.clo, chi = sp.chi;
   // a poisoned plane (non-finite window data: the reference's plane is all
   // NaN there) yields no peak, so every output is NaN
@@ -450,100 +570,32 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
       grp_sync(bar, gsize);  // s_locs visible to the next round's exclusion test
     }
   }
-  // Epilogue on the group's first warp: lane 0 refines the primary and forms
-  // ratio and moment, lanes 1..K-1 refine the alternatives in parallel.
+  // Epilogue on the group's first warp, after the last merge step wrote
+  // s_vals / s_locs: with a record buffer (regional maxima) the lanes of the
+  // peaks store the peak record and peak_epilogue_kernel forms the outputs;
+  // otherwise lane 0 forms them here.
   if (gtid >= 32 || !active) return;
-  __syncwarp();  // s_vals / s_locs written by lane 0 after the last merge round
-  const int lane = gtid;
-  int found = 0;
-  if (nfound > 0) {
-    found = 1;
-    while (found < nfound && s_vals[found] > 0.f) ++found;
-  }
-  const float NaN = __int_as_float(0x7fc00000);
-  const int cr = nr / 2 + 1, cc = nc / 2 + 1;
-  const int mmax = found < npeaks ? found : npeaks;  // peaks 1..mmax carry results
-  // The gauss3 logarithms of every peak refined by gauss3, one per lane:
-  // lane 4m + q takes peak m, q = 0 / 1: ln(Im/Ip), ln(Im Ip / I0^2) along
-  // the rows, q = 2 / 3 along the columns (gauss3_axis, spread over lanes so
-  // the warp evaluates one logarithm instead of four in a row).
-  double lg = 0.0;
-  int lv = 0;
-  {
-    const int m = lane >> 2, q = lane & 3;
-    const bool fit3 = m < K && m < found && (m == 0 ? (subpixel != 1 && subpixel != 3) : m < mmax);
-    if (fit3) {
-      const int i = s_locs[2 * m], j = s_locs[2 * m + 1];
-      const bool rows = q < 2;
-      if (rows ? (i > 0 && i < nr - 1) : (j > 0 && j < nc - 1)) {
-        const float I0 = R[j * ldr + i];
-        const float Im = rows ? R[j * ldr + i - 1] : R[(j - 1) * ldr + i];
-        const float Ip = rows ? R[j * ldr + i + 1] : R[(j + 1) * ldr + i];
-        if (Im > 0.f && I0 > 0.f && Ip > 0.f) {
-          const double dm = (double)Im, dz = (double)I0, dp = (double)Ip;
-          lg = log((q & 1) ? (dm * dp) / (dz * dz) : dm / dp);
-          lv = 1;
+  __syncwarp();
+  if (rec && finder == 0) {
+    const int lane = gtid;
+    if (lane == 0) rec[job] = __int_as_float(nfound);
+    if (lane < nfound) {
+      const int pr = s_locs[2 * lane], pc = s_locs[2 * lane + 1];
+      rec[(int64_t)(1 + lane) * rec_stride + job] = s_vals[lane];
+      rec[(int64_t)(1 + K + 2 * lane) * rec_stride + job] = __int_as_float(pr);
+      rec[(int64_t)(2 + K + 2 * lane) * rec_stride + job] = __int_as_float(pc);
+      const int h = lane == 0 ? 2 : 1, w = 2 * h + 1;
+      float* P = rec + (int64_t)rec_patch(K, lane) * rec_stride + job;
+      for (int dc = -h; dc <= h; ++dc)
+        for (int dr = -h; dr <= h; ++dr) {
+          const int i = pr + dr, j = pc + dc;
+          P[(int64_t)((dc + h) * w + (dr + h)) * rec_stride] =
+              (i >= 0 && i < nr && j >= 0 && j < nc) ? R[j * ldr + i] : 0.f;
         }
-      }
     }
+    return;
   }
-  const double g0 = __shfl_sync(0xffffffffu, lg, (4 * lane) & 31), g1 = __shfl_sync(0xffffffffu, lg, (4 * lane + 1) & 31);
-  const double g2 = __shfl_sync(0xffffffffu, lg, (4 * lane + 2) & 31), g3 = __shfl_sync(0xffffffffu, lg, (4 * lane + 3) & 31);
-  const int v0 = __shfl_sync(0xffffffffu, lv, (4 * lane) & 31), v2 = __shfl_sync(0xffffffffu, lv, (4 * lane + 2) & 31);
-  if (lane >= K) return;
-  float ref[2] = {NaN, NaN};
-  if (lane < found && (lane == 0 || lane < mmax)) {
-    const int pr = s_locs[2 * lane], pc = s_locs[2 * lane + 1];
-    if (lane == 0 && subpixel == 1) gauss9_fp64(R, nr, nc, ldr, pr, pc, ref);
-    else if (lane == 0 && subpixel == 3) { ref[0] = (float)(pr + 1); ref[1] = (float)(pc + 1); }
-    else {  // gauss3 from the lanes' logarithms (gauss3_fp64)
-      const double di = v0 ? (g1 != 0.0 ? g0 / (2.0 * g1) : 0.0) : 0.0;
-      const double dj = v2 ? (g3 != 0.0 ? g2 / (2.0 * g3) : 0.0) : 0.0;
-      ref[0] = (float)((double)(pr + 1) + di);
-      ref[1] = (float)((double)(pc + 1) + dj);
-    }
-  }
-  const float d_col = ref[1] - (float)cc, d_row = ref[0] - (float)cr;
-  if (lane == 0) {
-    float ratio = NaN, mom = NaN;
-    if (found > 0) {
-      const float v1 = s_vals[0];
-      ratio = found >= 2 ? v1 / s_vals[1] : (v1 > 0.f ? INFINITY : NaN);
-      mom = moment_fp64(R, nr, nc, ldr, ref[0], ref[1]);
-    }
-    if (grid_id >= 0 && o.du) {
-      o.du[grid_id] = d_col;
-      o.dv[grid_id] = d_row;
-      o.ratio[grid_id] = ratio;
-      o.moment[grid_id] = mom;
-    }
-    if (o.packed) {
-      float* pk = o.packed + job * (int64_t)(5 + 2 * (K - 1));
-      pk[0] = d_col;
-      pk[1] = d_row;
-      pk[2] = ratio;
-      pk[3] = mom;
-      pk[4] = (float)found;
-    }
-  } else {
-    // alternative peak `lane` (0-based): result only while lane < min(found, npeaks)
-    const bool has = lane < mmax;
-    const float au = has ? d_col : NaN, av = has ? d_row : NaN;
-    if (grid_id >= 0 && o.alt_u && lane - 1 < o.nalt) {
-      o.alt_u[grid_id + (int64_t)(lane - 1) * o.G] = au;
-      o.alt_v[grid_id + (int64_t)(lane - 1) * o.G] = av;
-    }
-    if (o.packed) {
-      float* pk = o.packed + job * (int64_t)(5 + 2 * (K - 1));
-      pk[5 + (lane - 1)] = au;
-      pk[5 + (K - 1) + (lane - 1)] = av;
-    }
-  }
-  if (o.locs) {
-    int32_t* lc = o.locs + job * (int64_t)(2 * K);
-    lc[2 * lane] = lane < found ? s_locs[2 * lane] + 1 : 0;
-    lc[2 * lane + 1] = lane < found ? s_locs[2 * lane + 1] + 1 : 0;
-  }
+  if (gtid == 0) peak_outputs(PlaneSrc{R, ldr}, nr, nc, K, npeaks, subpixel, nfound, s_vals, s_locs, grid_id, job, o);
 }
 
 // The analysis as a call: small planes keep it out of line (the kernel's
@@ -551,9 +603,10 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
 __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
                                            int subpixel, int gtid, int gsize, uint32_t* red, bool active,
                                            float* s_vals, int* s_locs, int64_t grid_id, int64_t job,
-                                           const PeakOut& o, bool poison, int bar, const ScanPlan sp) {
+                                           const PeakOut& o, bool poison, int bar, const ScanPlan sp,
+                                           float* rec, int64_t rec_stride) {
   analyze_body(R, nr, nc, ldr, K, npeaks, finder, subpixel, gtid, gsize, red, active, s_vals, s_locs, grid_id, job, o,
-               poison, bar, sp);
+               poison, bar, sp, rec, rec_stride);
 }
 
 // S(k) = conj(FA(k)) FB(k) of the packed transform Z = F(a + i b), from
@@ -672,7 +725,10 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
       const int gij = a.jobs[4 * job + 1];
       const int64_t cell = (int64_t)(gij & 0xFFFF) + (int64_t)(gij >> 16) * b.ny;
       // pairs that converged or have no further sweep, and masked cells, are skipped
-      if (!bp_live(b, a.it, a.done, p) || (b.gmask && b.gmask[cell])) continue;
+      if (!bp_live(b, a.it, a.done, p) || (b.gmask && b.gmask[cell])) {
+        if (a.rec && a.finder == 0 && gt == 0) a.rec[job] = __int_as_float(-1);  // no record for the epilogue
+        continue;
+      }
       rs = a.jobs[4 * job + 2];
       cs = a.jobs[4 * job + 3];
       const bool warped = a.it > 1 || b.has_pred0;
@@ -1005,10 +1061,10 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
     uint32_t* gred = red + w * (G / 32) * 2 * KMAX;
     if (C::INLINE_ANALYSIS)
       analyze_body(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
-                   s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, sp);
+                   s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, sp, a.rec, a.njobs);
     else
       analyze_group(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
-                    s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, sp);
+                    s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, sp, a.rec, a.njobs);
     grp_sync(bar, G);  // the plane is reused by the group's next window
   }
 }
@@ -1029,10 +1085,48 @@ __global__ void __launch_bounds__(128) analyze_planes_kernel(const AnalyzeArgs a
     __syncthreads();
     const int64_t gid = a.jobs ? (int64_t)a.jobs[4 * pl] + (int64_t)a.jobs[4 * pl + 1] * a.ny : -1;
     analyze_group(R, a.nr, a.nc, a.nr, K, a.npeaks, a.finder, a.subpixel, threadIdx.x, 128, red, true, s_vals,
-                  s_locs, gid, pl, po, false, 0, sp);
+                  s_locs, gid, pl, po, false, 0, sp, nullptr, 0);
     __syncthreads();
   }
 }
+
+// The per-window outputs from the peak records (one thread per window):
+// the same arithmetic as the in-kernel epilogue, with every lane on its own
+// window instead of one lane per window holding up the window's warp.
+__global__ void __launch_bounds__(128) peak_epilogue_kernel(const CorrArgs a, int N) {
+  const int K = a.npeaks > 2 ? a.npeaks : 2;
+  const int64_t S = a.njobs;
+  const PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
+  for (int64_t job = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; job < a.njobs;
+       job += (int64_t)gridDim.x * blockDim.x) {
+    const int nf = __float_as_int(__ldg(a.rec + job));
+    if (nf < 0) continue;  // skipped by the correlation kernel
+    int64_t gid;
+    PeakOut pw = po;
+    if (a.bp) {  // the correlation kernel's addressing of the window's grid cell
+      const int p = a.jobs[4 * job];
+      const BPair& b = a.bp[p];
+      const int gij = a.jobs[4 * job + 1];
+      gid = b.goff + (int64_t)(gij & 0xFFFF) + (int64_t)(gij >> 16) * b.ny;
+      pw.G = (int64_t)b.ny * b.nx;
+      pw.nalt = b.nalt;
+      pw.alt_u = a.alt_u ? a.alt_u + b.aoff - b.goff : nullptr;
+      pw.alt_v = a.alt_v ? a.alt_v + b.aoff - b.goff : nullptr;
+    } else {
+      gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
+    }
+    float vals[KMAX];
+    int locs[2 * KMAX];
+    for (int m = 0; m < nf; ++m) {
+      vals[m] = __ldg(a.rec + (int64_t)(1 + m) * S + job);
+      locs[2 * m] = __float_as_int(__ldg(a.rec + (int64_t)(1 + K + 2 * m) * S + job));
+      locs[2 * m + 1] = __float_as_int(__ldg(a.rec + (int64_t)(2 + K + 2 * m) * S + job));
+    }
+    peak_outputs(RecSrc{a.rec + job, S, K}, N, N, K, a.npeaks, a.subpixel, nf, vals, locs, gid, job, pw);
+  }
+}
+
+size_t correlate_record_words(int npeaks) { return (size_t)rec_words(npeaks > 2 ? npeaks : 2); }
 
 // ---------------------------------------------------------------------------
 template <int N, int W> static cudaError_t launch_nw(const CorrArgs& a, cudaStream_t s, int num_sms) {
@@ -1058,6 +1152,11 @@ template <int N, int W> static cudaError_t launch_nw(const CorrArgs& a, cudaStre
   if (grid > units) grid = units;
   if (grid < 1) grid = 1;
   correlate_kernel<N, W><<<(unsigned)grid, C::NT, sm, s>>>(a);
+  if (a.rec && a.finder == 0 && !a.accumulate) {
+    int64_t eb = (a.njobs + 127) / 128;
+    if (eb > (int64_t)num_sms * 16) eb = (int64_t)num_sms * 16;
+    peak_epilogue_kernel<<<(unsigned)eb, 128, 0, s>>>(a, N);
+  }
   return cudaGetLastError();
 }
 
