@@ -47,11 +47,116 @@ __device__ __forceinline__ double median_d(double* a, int n) {
 constexpr int UOD_MAXN = 80;  // neighbourhood <= 4 layers
 
 
+// Neighbourhoods of 1 and 2 layers in registers: the S = (2nb+1)^2 - 1
+// neighbour slots hold +inf where a neighbour is missing (edge or excluded),
+// so sorting the slots with a fixed comparator network puts the n present
+// values first, in order, and no array needs dynamic indexing. The networks
+// are Batcher's odd-even merge sort (19 comparators for 8 inputs; the
+// 32-input network without the comparators that reach slots 24..31, which
+// hold +inf throughout, for 24); both sort every 0/1 input (checked
+// exhaustively), hence every input. The medians equal median_f's up to the
+// sign of a zero, which only ever enters through |x - m|.
+__device__ __forceinline__ void cas_f(float& a, float& b) {
+  const float lo = fminf(a, b), hi = fmaxf(a, b);
+  a = lo;
+  b = hi;
+}
+template <int S> __device__ __forceinline__ void sort_net_f(float (&a)[S]);
+template <> __device__ __forceinline__ void sort_net_f<8>(float (&a)[8]) {
+  cas_f(a[0], a[1]); cas_f(a[2], a[3]); cas_f(a[4], a[5]); cas_f(a[6], a[7]); cas_f(a[0], a[2]); cas_f(a[1], a[3]);
+  cas_f(a[4], a[6]); cas_f(a[5], a[7]); cas_f(a[1], a[2]); cas_f(a[5], a[6]); cas_f(a[0], a[4]); cas_f(a[3], a[7]);
+  cas_f(a[1], a[5]); cas_f(a[2], a[6]); cas_f(a[1], a[4]); cas_f(a[3], a[6]); cas_f(a[2], a[4]); cas_f(a[3], a[5]);
+  cas_f(a[3], a[4]);
+}
+template <> __device__ __forceinline__ void sort_net_f<24>(float (&a)[24]) {
+  cas_f(a[0], a[1]); cas_f(a[2], a[3]); cas_f(a[0], a[2]); cas_f(a[1], a[3]); cas_f(a[1], a[2]); cas_f(a[4], a[5]);
+  cas_f(a[6], a[7]); cas_f(a[4], a[6]); cas_f(a[5], a[7]); cas_f(a[5], a[6]); cas_f(a[0], a[4]); cas_f(a[2], a[6]);
+  cas_f(a[2], a[4]); cas_f(a[1], a[5]); cas_f(a[3], a[7]); cas_f(a[3], a[5]); cas_f(a[1], a[2]); cas_f(a[3], a[4]);
+  cas_f(a[5], a[6]); cas_f(a[8], a[9]); cas_f(a[10], a[11]); cas_f(a[8], a[10]); cas_f(a[9], a[11]); cas_f(a[9], a[10]);
+  cas_f(a[12], a[13]); cas_f(a[14], a[15]); cas_f(a[12], a[14]); cas_f(a[13], a[15]); cas_f(a[13], a[14]); cas_f(a[8], a[12]);
+  cas_f(a[10], a[14]); cas_f(a[10], a[12]); cas_f(a[9], a[13]); cas_f(a[11], a[15]); cas_f(a[11], a[13]); cas_f(a[9], a[10]);
+  cas_f(a[11], a[12]); cas_f(a[13], a[14]); cas_f(a[0], a[8]); cas_f(a[4], a[12]); cas_f(a[4], a[8]); cas_f(a[2], a[10]);
+  cas_f(a[6], a[14]); cas_f(a[6], a[10]); cas_f(a[2], a[4]); cas_f(a[6], a[8]); cas_f(a[10], a[12]); cas_f(a[1], a[9]);
+  cas_f(a[5], a[13]); cas_f(a[5], a[9]); cas_f(a[3], a[11]); cas_f(a[7], a[15]); cas_f(a[7], a[11]); cas_f(a[3], a[5]);
+  cas_f(a[7], a[9]); cas_f(a[11], a[13]); cas_f(a[1], a[2]); cas_f(a[3], a[4]); cas_f(a[5], a[6]); cas_f(a[7], a[8]);
+  cas_f(a[9], a[10]); cas_f(a[11], a[12]); cas_f(a[13], a[14]); cas_f(a[16], a[17]); cas_f(a[18], a[19]); cas_f(a[16], a[18]);
+  cas_f(a[17], a[19]); cas_f(a[17], a[18]); cas_f(a[20], a[21]); cas_f(a[22], a[23]); cas_f(a[20], a[22]); cas_f(a[21], a[23]);
+  cas_f(a[21], a[22]); cas_f(a[16], a[20]); cas_f(a[18], a[22]); cas_f(a[18], a[20]); cas_f(a[17], a[21]); cas_f(a[19], a[23]);
+  cas_f(a[19], a[21]); cas_f(a[17], a[18]); cas_f(a[19], a[20]); cas_f(a[21], a[22]); cas_f(a[18], a[20]); cas_f(a[19], a[21]);
+  cas_f(a[17], a[18]); cas_f(a[19], a[20]); cas_f(a[21], a[22]); cas_f(a[0], a[16]); cas_f(a[8], a[16]); cas_f(a[4], a[20]);
+  cas_f(a[12], a[20]); cas_f(a[4], a[8]); cas_f(a[12], a[16]); cas_f(a[2], a[18]); cas_f(a[10], a[18]); cas_f(a[6], a[22]);
+  cas_f(a[14], a[22]); cas_f(a[6], a[10]); cas_f(a[14], a[18]); cas_f(a[2], a[4]); cas_f(a[6], a[8]); cas_f(a[10], a[12]);
+  cas_f(a[14], a[16]); cas_f(a[18], a[20]); cas_f(a[1], a[17]); cas_f(a[9], a[17]); cas_f(a[5], a[21]); cas_f(a[13], a[21]);
+  cas_f(a[5], a[9]); cas_f(a[13], a[17]); cas_f(a[3], a[19]); cas_f(a[11], a[19]); cas_f(a[7], a[23]); cas_f(a[15], a[23]);
+  cas_f(a[7], a[11]); cas_f(a[15], a[19]); cas_f(a[3], a[5]); cas_f(a[7], a[9]); cas_f(a[11], a[13]); cas_f(a[15], a[17]);
+  cas_f(a[19], a[21]); cas_f(a[1], a[2]); cas_f(a[3], a[4]); cas_f(a[5], a[6]); cas_f(a[7], a[8]); cas_f(a[9], a[10]);
+  cas_f(a[11], a[12]); cas_f(a[13], a[14]); cas_f(a[15], a[16]); cas_f(a[17], a[18]); cas_f(a[19], a[20]); cas_f(a[21], a[22]);
+}
+
+// median of the n (1..S) present slots; NaN when one of them is NaN
+template <int S> __device__ __forceinline__ float median_net_f(float (&a)[S], int n) {
+  bool nan = false;
+#pragma unroll
+  for (int i = 0; i < S; ++i) nan |= isnan(a[i]);
+  if (nan) return f_nan();
+  sort_net_f<S>(a);
+  const int h = n / 2;
+  float lo = a[0], hi = a[0];  // a[h - 1], a[h]
+#pragma unroll
+  for (int i = 1; i < S; ++i) {
+    if (i == h) hi = a[i];
+    if (i == h - 1) lo = a[i];
+  }
+  if (n & 1) return hi;
+  return FADD(lo / 2.0f, hi / 2.0f);
+}
+
+template <int NB>
+__device__ __forceinline__ uint8_t uod_cell_net(const float* u, const float* v, int ny, int nx, int r, int c, double thr,
+                                                double eps, const uint8_t* exclude) {
+  constexpr int D = 2 * NB + 1, S = D * D - 1;
+  const int64_t k = r + (int64_t)c * ny;
+  const float INF = __int_as_float(0x7f800000);
+  float nu[S], nv[S];
+  uint32_t present = 0;
+  int n = 0;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int d = s < S / 2 ? s : s + 1;  // skip the centre of the D x D block
+    const int r2 = r + d % D - NB, c2 = c + d / D - NB;
+    const int64_t q = r2 + (int64_t)c2 * ny;
+    const bool ok = r2 >= 0 && r2 < ny && c2 >= 0 && c2 < nx && !(exclude && exclude[q]);
+    nu[s] = ok ? u[q] : INF;
+    nv[s] = ok ? v[q] : INF;
+    present |= ok ? 1u << s : 0u;
+    n += ok;
+  }
+  if (n == 0) return 0;
+  float ru[S], rv[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    ru[s] = nu[s];
+    rv[s] = nv[s];
+  }
+  const float um = median_net_f<S>(ru, n), vm = median_net_f<S>(rv, n);
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const bool ok = (present >> s) & 1u;
+    ru[s] = ok ? fabsf(FSUB(nu[s], um)) : INF;
+    rv[s] = ok ? fabsf(FSUB(nv[s], vm)) : INF;
+  }
+  const double un = (double)fabsf(FSUB(u[k], um)) / __dadd_rn((double)median_net_f<S>(ru, n), eps);
+  const double vn = (double)fabsf(FSUB(v[k], vm)) / __dadd_rn((double)median_net_f<S>(rv, n), eps);
+  return (un > thr || vn > thr) ? 1 : 0;
+}
+
 // universal_outlier_detection (src/quality.jl:244-293) at cell (r, c).
 __device__ __forceinline__ uint8_t uod_cell(const float* u, const float* v, int ny, int nx, int r, int c, double thr,
                                             int nb, double eps, const uint8_t* exclude) {
   const int64_t k = r + (int64_t)c * ny;
   if (exclude && exclude[k]) return 0;
+  if (nb == 1) return uod_cell_net<1>(u, v, ny, nx, r, c, thr, eps, exclude);
+  if (nb == 2) return uod_cell_net<2>(u, v, ny, nx, r, c, thr, eps, exclude);
   float nu[UOD_MAXN], nv[UOD_MAXN], ru[UOD_MAXN], rv[UOD_MAXN];
   int n = 0;
   for (int c2 = max(0, c - nb); c2 <= min(nx - 1, c + nb); ++c2)

@@ -98,6 +98,11 @@ CORR_CASES = [
     dict(window_size=16, overlap=8),
     dict(window_size=32, overlap=16, correlation_method="phase", padding=True, apodization="gauss"),
     dict(window_size=32, overlap=16, peak_finder="exclusion", n_peaks=4),
+    # 16 px padded windows run two per warp: the exclusion finder and the
+    # other options through the half-warp groups as well
+    dict(window_size=16, overlap=8, padding=True, peak_finder="exclusion", n_peaks=3),
+    dict(window_size=16, overlap=8, padding=True, correlation_method="phase", n_peaks=3,
+         subpixel_method="gauss9"),
 ]
 
 
@@ -189,10 +194,20 @@ def _noisy_field(rng, ny, nx, nspikes=6):
     return u, v
 
 
+@pytest.mark.parametrize("nans", [False, True])
 @pytest.mark.parametrize("nb", [1, 2, 3])
-def test_uod_bit_exact(ws, orc, hooks, nb):
-    rng = np.random.default_rng(nb)
+def test_uod_bit_exact(ws, orc, hooks, nb, nans):
+    """Neighbourhoods of 1 and 2 layers take the sorting-network path, 3 the
+    general one; NaN neighbours make the median NaN (never flagged), zeros of
+    either sign and ties exercise the median's order rules."""
+    rng = np.random.default_rng(nb + 10 * nans)
     u, v = _noisy_field(rng, 41, 37)
+    u[::7, ::5] = 0.0
+    v[3::7, ::5] = -0.0
+    u[10, 4:9] = u[10, 3]  # ties
+    if nans:
+        u[rng.uniform(size=u.shape) < 0.02] = np.nan
+        v[rng.uniform(size=v.shape) < 0.02] = np.nan
     ex = rng.uniform(size=u.shape) < 0.05
     f = hooks.universal_outlier_detection(ws, u, v, 2.0, nb, 0.1, ex)
     g = orc.uod(u, v, 2.0, nb, 0.1, ex, dtype=np.float32)
