@@ -118,22 +118,30 @@ __device__ __forceinline__ bool is_local_max(const float* R, int nr, int nc, int
   return true;
 }
 
-// Barrier of one thread group: a warp (count 32), the whole CTA (bar 0), or
-// the named barrier `bar` shared by `count` threads (whole warps).
+// Lanes of the calling thread's group within its warp: the whole warp for
+// groups of 32 threads or more, else the aligned block of `count` lanes
+// (count a power of two below 32: two or more groups share a warp).
+__device__ __forceinline__ unsigned grp_mask(int count) {
+  return count >= 32 ? 0xffffffffu : (((1u << count) - 1u) << ((threadIdx.x & 31) & ~(count - 1)));
+}
+
+// Barrier of one thread group: lanes of a warp (count <= 32), the whole CTA
+// (bar 0), or the named barrier `bar` shared by `count` threads (whole warps).
 __device__ __forceinline__ void grp_sync(int bar, int count) {
-  if (count == 32) __syncwarp();
+  if (count <= 32) __syncwarp(grp_mask(count));
   else if (bar == 0) __syncthreads();
   else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(count) : "memory");
 }
 
 // Group-wide argmax of (hi, lo) keys. Every thread of the group calls it (it
 // synchronises the group); each group has its own reduction slots.
-__device__ __forceinline__ void group_argmax(uint32_t hi, uint32_t lo, uint32_t* red, int gwarp, int nwarps,
+__device__ __forceinline__ void group_argmax(uint32_t hi, uint32_t lo, uint32_t* red, int gwarp, int gsize,
                                              uint32_t& whi, uint32_t& wlo, int bar) {
-  const int lane = threadIdx.x & 31;
-  uint32_t mhi = __reduce_max_sync(0xffffffffu, hi);
-  uint32_t mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
-  if (nwarps == 1) {  // one warp: the shuffle reduction is the answer
+  const int lane = threadIdx.x & 31, nwarps = gsize >> 5;
+  const unsigned m = grp_mask(gsize);
+  uint32_t mhi = __reduce_max_sync(m, hi);
+  uint32_t mlo = __reduce_max_sync(m, hi == mhi ? lo : 0u);
+  if (nwarps <= 1) {  // one warp or part of one: the shuffle reduction is the answer
     whi = mhi;
     wlo = mlo;
     return;
@@ -155,17 +163,18 @@ __device__ __forceinline__ void group_argmax(uint32_t hi, uint32_t lo, uint32_t*
   grp_sync(bar, nwarps * 32);
 }
 
-// The warp's K best keys over its lanes' lists, by K shuffle rounds (keys
-// are unique, so exactly one lane pops each winner): lane m receives the
-// m-th best in (mh, ml); returns how many exist (the same in every lane).
-__device__ __forceinline__ int warp_topk(TopK& tk, int K, int lane, uint32_t& mh, uint32_t& ml) {
+// The K best keys over the lists of the lanes in `mask` (a warp or the
+// group's part of one), by K shuffle rounds (keys are unique, so exactly one
+// lane pops each winner): lane m receives the m-th best in (mh, ml);
+// returns how many exist (the same in every lane).
+__device__ __forceinline__ int warp_topk(TopK& tk, int K, int lane, uint32_t& mh, uint32_t& ml, unsigned mask) {
   int n = 0;
   mh = ml = 0u;
   for (int round = 0; round < K; ++round) {
     const uint32_t h = tk.hi[0], l = tk.lo[0];  // empty slots hold 0
-    const uint32_t wh = __reduce_max_sync(0xffffffffu, h);
+    const uint32_t wh = __reduce_max_sync(mask, h);
     if (wh == 0u) break;
-    const uint32_t wl = __reduce_max_sync(0xffffffffu, h == wh ? l : 0u);
+    const uint32_t wl = __reduce_max_sync(mask, h == wh ? l : 0u);
     if (h == wh && l == wl) tk.pop();
     if (lane == round) {
       mh = wh;
@@ -498,7 +507,7 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
     // K best from them the same way.
     const int lane = gtid & 31;
     uint32_t mh = 0u, ml = 0u;
-    int nw = warp_topk(tk, K, lane, mh, ml);
+    int nw = warp_topk(tk, K, lane, mh, ml, grp_mask(gsize));
     if (nwarps > 1) {
       if (lane < K) {
         red[2 * (gwarp * K + lane)] = mh;
@@ -512,7 +521,7 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
           const uint32_t h = red[2 * e], l = red[2 * e + 1];
           if (h != 0u) tg.insert(h, l, K);
         }
-        nw = warp_topk(tg, K, lane, mh, ml);
+        nw = warp_topk(tg, K, lane, mh, ml, 0xffffffffu);
       }
     }
     if (gwarp == 0) {
@@ -548,7 +557,7 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
             if (h > bh || (h == bh && l > bl)) { bh = h; bl = l; }
           }
         }
-        group_argmax(bh, bl, red, gwarp, nwarps, whi, wlo, bar);
+        group_argmax(bh, bl, red, gwarp, gsize, whi, wlo, bar);
         if (whi > fkey(0.f) || (rlo == 0 && clo == 0 && rhi == nr - 1 && chi == nc - 1)) break;  // positive, or the box is the plane
       }
       if (!done && whi != 0u) {
@@ -575,7 +584,7 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
   // peaks store the peak record and peak_epilogue_kernel forms the outputs;
   // otherwise lane 0 forms them here.
   if (gtid >= 32 || !active) return;
-  __syncwarp();
+  __syncwarp(grp_mask(gsize));
   if (rec && finder == 0) {
     const int lane = gtid;
     if (lane == 0) rec[job] = __int_as_float(nfound);
@@ -628,12 +637,16 @@ __device__ __forceinline__ float2 cross_spectrum(float2 X, float2 Zm, int method
 // ---------------------------------------------------------------------------
 template <int N, int W> struct CorrCfg {
   static constexpr int N1 = AxisSplit<N>::N1, N2 = AxisSplit<N>::N2;
-  static constexpr int WPC = N <= 32 ? 4 : (N <= 64 ? 2 : 1);    // windows per CTA
+  // 16 x 16 windows padded to 32: every stage of the plane has at most 16
+  // lines (16 data columns, 16 canonical column items, 16 row pairs), so
+  // half a warp serves a window and each warp carries two
+  static constexpr bool HALF = N == 32 && W == 16;
+  static constexpr int WPC = HALF ? 8 : (N <= 32 ? 4 : (N <= 64 ? 2 : 1));  // windows per CTA
   static constexpr int NT = N <= 48 ? 128 : (N <= 96 ? 256 : 512);
-  static constexpr int G = NT / WPC;  // threads per window in the analysis
+  static constexpr int G = NT / WPC;  // threads per window
   // CTAs per SM the register budget is sized for (the shared-memory limit
   // allows at least this many)
-  static constexpr int MINB = N <= 48 ? 4 : (N <= 64 ? 3 : (N <= 96 ? 2 : 1));
+  static constexpr int MINB = HALF ? 3 : (N <= 48 ? 4 : (N <= 64 ? 3 : (N <= 96 ? 2 : 1)));
   // the peak analysis inline (one window per CTA: its latency is the CTA's)
   static constexpr bool INLINE_ANALYSIS = N >= 96;
   // The spectrum is Hermitian, so the inverse transforms only the N/2 + 1
@@ -655,7 +668,7 @@ template <int N, int W> struct CorrCfg {
            WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int)) + 3 * N * sizeof(int) + 64;
   }
   static_assert(W == N || 2 * W == N, "window must equal the FFT size or half of it");
-  static_assert(G >= 32 && G % 32 == 0, "analysis group must be whole warps");
+  static_assert((G >= 32 && G % 32 == 0) || G == 16, "a window group is whole warps or half a warp");
   static_assert(N * LDR <= 2 * N * LD, "real plane must fit in the complex plane");
 };
 
@@ -774,11 +787,12 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
           }
         }
       }
+      const unsigned gm = grp_mask(G);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        sa += __shfl_xor_sync(0xffffffffu, sa, o);
-        sb += __shfl_xor_sync(0xffffffffu, sb, o);
-        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+      for (int o = (G < 32 ? G : 32) / 2; o > 0; o >>= 1) {
+        sa += __shfl_xor_sync(gm, sa, o);
+        sb += __shfl_xor_sync(gm, sb, o);
+        cnt += __shfl_xor_sync(gm, cnt, o);
       }
       double ta = sa, tb = sb, tn = cnt;
       if (G > 32) {
@@ -930,20 +944,37 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
       grp_sync(bar, G);
     }
 #pragma unroll 1
-    for (int it = gt; it < NC * N2; it += G) {
-      const int c = it % NC, n2 = it / NC;
+    //      With N2 = 1 the two self-paired columns kq = 0 and N/2, whose
+    //      results are real, share one transform as col0 + i col(N/2) (real
+    //      part: column 0, imaginary part: column N/2): H items in all.
+    for (int it = gt; it < (N2 == 1 ? H : NC * N2); it += G) {
+      const bool pk = N2 == 1 && it == 0;
+      const int c = N2 == 1 ? it : it % NC, n2 = N2 == 1 ? 0 : it / NC;
       const int aq = N2 == 1 ? c : s_canon[c];
-      const int bq = N2 == 1 ? (N - c) % N : s_neg[aq];
+      const int bq = pk ? H : (N2 == 1 ? N - c : s_neg[aq]);
       float2* L = P + aq * LD;
       float2* Lb = P + bq * LD;
       float2 x[N1];
 #pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) x[k1] = L[N2 * k1 + n2];
+      for (int k1 = 0; k1 < N1; ++k1) {
+        const float2 u = L[N2 * k1 + n2];
+        if (pk) {
+          const float2 v = Lb[k1];
+          x[k1] = make_float2(u.x - v.y, u.y + v.x);
+        } else {
+          x[k1] = u;
+        }
+      }
       RDFT<N1, true>::run(x, N1);
 #pragma unroll
       for (int n1 = 0; n1 < N1; ++n1) {
-        L[N2 * n1 + n2] = x[n1];
-        if (bq != aq) Lb[N2 * n1 + n2] = make_float2(x[n1].x, -x[n1].y);
+        if (pk) {
+          L[n1] = make_float2(x[n1].x, 0.f);
+          Lb[n1] = make_float2(x[n1].y, 0.f);
+        } else {
+          L[N2 * n1 + n2] = x[n1];
+          if (bq != aq) Lb[N2 * n1 + n2] = make_float2(x[n1].x, -x[n1].y);
+        }
       }
     }
     grp_sync(bar, G);

@@ -126,12 +126,17 @@ def test_correlation_planes_and_peaks(ws, orc, hb, hooks, pair256, kw):
     w = p.window_size[0]
     K = max(p.n_peaks, 2)
     near_ties = 0
+    # the phase method divides every bin by its magnitude, so FFT round-off in
+    # bins of small magnitude reaches the plane at full weight: 2.9e-5 of the
+    # peak is seen for unapodized 16 px windows, against ~3e-7 for the cross
+    # method
+    ptol = 1e-4 if p.correlation_method == "phase" else 2e-5
     for q, (gi, gj, rs, cs) in enumerate(jobs):
         sa = A[rs - 1:rs - 1 + w, cs - 1:cs - 1 + w]
         sb = B[rs - 1:rs - 1 + w, cs - 1:cs - 1 + w]
         R = orc.correlation_plane(sa, sb, p)
         scale = np.abs(R).max()
-        assert np.abs(planes[q] - R).max() <= 2e-5 * scale + 1e-12
+        assert np.abs(planes[q] - R).max() <= ptol * scale + 1e-12
         ref, rl = orc.analyze_plane(R, p.n_peaks, p.peak_finder, p.subpixel_method)
         f = int(ref[4])
         if int(out[q, 4]) != f or not np.array_equal(locs[q, :2 * f], rl[:2 * f]):
