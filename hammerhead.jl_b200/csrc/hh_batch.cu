@@ -194,7 +194,7 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
     wcol[p] = WC;
     wrow[p] = WR;
     if (deforms[p]) {
-      Wt += nr * nc;
+      Wt += (nr * nc + 3) / 4 * 4;  // 16-byte aligned per pair: the deformation stores pixel quads
       Q += (nr + 2) * (nc + 2);
       WC += (nc + 31) / 32 * nseg_host(nr + 2);  // column tiles x segments
       WR += (nr + 2) * nseg_host(nc + 2);
@@ -326,7 +326,7 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
       b.tol = pd.convergence_tol;
       const int64_t Gk = (int64_t)gr.ny * gr.nx;
       coff += Gk;
-      if (deforms[p]) pcoff += q.nr * q.nc;
+      if (deforms[p]) pcoff += (q.nr * q.nc + 3) / 4 * 4;  // quads of pixels never straddle two pairs
       S.max_maxit = std::max(S.max_maxit, (int)pd.max_iterations);
       S.any_nalt |= b.nalt > 0;
       S.any_replace |= b.replace != 0;

@@ -40,14 +40,14 @@ struct BPair {
   const float* cpr;  // ... and of the row length nc + 2
   const float* ivr;
   int64_t nr, nc;
-  int64_t poff;   // warped-pixel storage offset
+  int64_t poff;   // warped-pixel storage offset (a multiple of 4)
   int64_t qoff;   // padded-pixel (coefficient) storage offset, compact over deforming pairs
   int64_t wcol;   // prefilter work offsets (32-column tiles x segments, row segments)
   int64_t wrow;
   int64_t goff;   // cell storage offset
   int64_t aoff;   // alternatives storage offset (nalt planes of ny*nx cells)
   int64_t coff;   // slot-compact cell offset
-  int64_t pcoff;  // slot-compact pixel offset
+  int64_t pcoff;  // slot-compact pixel offset (a multiple of 4)
   int64_t roff;   // offset of the pair's final-pass result
   int32_t ny, nx;      // this slot's grid (0 when the slot does not exist)
   int32_t pgny, pgnx;  // previous slot's grid (predictor of sweep 1)

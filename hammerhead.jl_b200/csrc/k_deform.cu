@@ -198,6 +198,16 @@ __device__ __forceinline__ void lin_axis(float q, float q0, float step, int n, i
   d = FD(FS(q, k0), FS(k1, k0));
 }
 
+// the bilinear combination at cell (iy, ix) with fractions (dy, dx)
+__device__ __forceinline__ float bilinear_at(const float* f, const PredGrid& g, int iy, float dy, int ix, float dx) {
+  const int iy2 = g.gny == 1 ? iy : iy + 1, ix2 = g.gnx == 1 ? ix : ix + 1;
+  const float f00 = f[iy + ix * g.gny], f01 = f[iy + ix2 * g.gny], f10 = f[iy2 + ix * g.gny],
+              f11 = f[iy2 + ix2 * g.gny];
+  const float a = FA(FM(FS(1.f, dx), f00), FM(dx, f01));
+  const float b = FA(FM(FS(1.f, dx), f10), FM(dx, f11));
+  return FA(FM(FS(1.f, dy), a), FM(dy, b));
+}
+
 __device__ __forceinline__ float bilinear(const float* f, const PredGrid& g, float qy, float qx) {
   int iy, ix;
   float dy, dx;
@@ -318,6 +328,49 @@ constexpr int BS_TLD = BS_TILE + 1;        // odd stride: conflict-free by lane 
 constexpr int BSC_WARPS = 4;
 constexpr size_t BSC_SMEM = (size_t)BSC_WARPS * 32 * BS_TLD * sizeof(float);
 
+// Rows [0, cnt) (cnt <= 96) of `ncol` columns between global memory (column
+// c at g + c * gld) and a staged tile (column c at T + c * BS_TLD). The
+// lanes walk down the columns; eight columns per batch keep 24 loads of a
+// lane in flight instead of waiting on each column in turn.
+__device__ __forceinline__ void tile_load(float* T, const float* g, int64_t gld, int ncol, int cnt, int lane) {
+  for (int c0 = 0; c0 < ncol; c0 += 8) {
+    float v[8][3];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const int c = c0 + u, r = lane + 32 * j;
+        v[u][j] = (c < ncol && r < cnt) ? __ldg(g + c * gld + r) : 0.f;
+      }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const int c = c0 + u, r = lane + 32 * j;
+        if (c < ncol && r < cnt) T[c * BS_TLD + r] = v[u][j];
+      }
+  }
+}
+__device__ __forceinline__ void tile_store(const float* T, float* g, int64_t gld, int ncol, int cnt, int lane) {
+  for (int c0 = 0; c0 < ncol; c0 += 8) {
+    float v[8][3];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const int c = c0 + u, r = lane + 32 * j;
+        v[u][j] = (c < ncol && r < cnt) ? T[c * BS_TLD + r] : 0.f;
+      }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const int c = c0 + u, r = lane + 32 * j;
+        if (c < ncol && r < cnt) g[c * gld + r] = v[u][j];
+      }
+  }
+}
+
 template <int PASS>
 __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPair* __restrict__ bp, int npairs,
                                                                       int64_t witems, float* dbuf, int64_t qtot) {
@@ -359,8 +412,7 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
       const int64_t ks = max((int64_t)0, k0 - BS_WARM);
       const int cnt = (int)(k1 - ks);
       // stage the right-hand sides: unknown k is padded element k + 2 = image row k + 1
-      for (int c = 0; c < ncol; ++c)
-        for (int r = lane; r < cnt; r += 32) T[c * BS_TLD + r] = __ldg(im + c * nr + ks + 1 + r);
+      tile_load(T, im + ks + 1, nr, ncol, cnt, lane);
       __syncwarp();
       if (mine) {
         const float* ic = im + lane * nr;
@@ -368,6 +420,7 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
         const float c2 = __ldg(ic), cn1 = __ldg(ic + nr - 1);  // padded elements 1 and n - 2
         float* x = T + lane * BS_TLD;
         float dv = 0.f;
+#pragma unroll 4
         for (int64_t k = ks; k < k1; ++k) {
           float rhs = x[k - ks];
           if (k == 0) rhs = FS(rhs, FM(sixth, c2));
@@ -378,18 +431,17 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
       }
       __syncwarp();
       const int nout = (int)(k1 - k0), o = (int)(k0 - ks);
-      for (int c = 0; c < ncol; ++c)
-        for (int r = lane; r < nout; r += 32) d[c * n + k0 + 2 + r] = T[c * BS_TLD + o + r];
+      tile_store(T + o, d + k0 + 2, n, ncol, nout, lane);
       __syncwarp();  // the tile is restaged by the next item
     } else {
       const int64_t ke = min(m - 1, k1 - 1 + BS_WARM);
       const int cnt = (int)(ke - k0 + 1);
-      for (int c = 0; c < ncol; ++c)
-        for (int r = lane; r < cnt; r += 32) T[c * BS_TLD + r] = d[c * n + k0 + 2 + r];
+      tile_load(T, d + k0 + 2, n, ncol, cnt, lane);
       __syncwarp();
       if (mine) {
         float* x = T + lane * BS_TLD;
         float xv = 0.f, xlast = 0.f;
+#pragma unroll 4
         for (int64_t k = ke; k >= k0; --k) {
           const float dk = x[k - k0];
           xv = k == ke ? dk : FS(dk, FM(__ldg(b.cpc + k), xv));
@@ -411,8 +463,7 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
       }
       __syncwarp();
       const int nout = (int)(k1 - k0);
-      for (int c = 0; c < ncol; ++c)
-        for (int r = lane; r < nout; r += 32) coef[c * n + k0 + 2 + r] = T[c * BS_TLD + r];
+      tile_store(T, coef + k0 + 2, n, ncol, nout, lane);
       __syncwarp();
     }
   }
@@ -531,35 +582,77 @@ cudaError_t launch_b_sweep_begin(const BPair* bp, int npairs, const int32_t* don
   return cudaGetLastError();
 }
 
+// Four consecutive pixels (a quad; pairs start on multiples of 4 in the
+// slot-compact index and in the warped arrays) per thread: the pair lookup,
+// the pair's fields, the pixel index division and the predictor's column
+// interpolation are done once per quad (again only where the quad wraps to
+// the next column), and a full quad is stored as one 16-byte vector.
 __global__ void __launch_bounds__(256) b_deform_kernel(const BPair* __restrict__ bp, int npairs,
                                                        const int32_t* __restrict__ done, int it, int64_t ptot,
                                                        const float* __restrict__ pu, const float* __restrict__ pv) {
-  B_STRIDE(k, ptot) {
+  B_STRIDE(t, (ptot + 3) / 4) {
+    const int64_t k = 4 * t;
     const int p = bp_find<&BPair::pcoff>(bp, npairs, k);
     const BPair& b = bp[p];
-    const int64_t l = k - b.pcoff;
-    if (!bp_live(b, it, done, p) || !(it > 1 || b.has_pred0) || !b.deforms || l >= b.nr * b.nc) continue;
+    const int64_t l0 = k - b.pcoff, npx = b.nr * b.nc;
+    if (!bp_live(b, it, done, p) || !(it > 1 || b.has_pred0) || !b.deforms || l0 >= npx) continue;
     const PredGrid g = b_pred_grid(b, it);
+    const float* fu = pu + b.goff;
+    const float* fv = pv + b.goff;
+    const int64_t nr = b.nr, nc = b.nc;
     int64_t r, c;
-    if (b.nr * b.nc <= 0x7fffffff) {  // 32-bit division when the pair's pixel index fits
-      r = (uint32_t)l % (uint32_t)b.nr;
-      c = (uint32_t)l / (uint32_t)b.nr;
+    if (npx <= 0x7fffffff) {  // 32-bit division when the pair's pixel index fits
+      r = (uint32_t)l0 % (uint32_t)nr;
+      c = (uint32_t)l0 / (uint32_t)nr;
     } else {
-      r = l % b.nr;
-      c = l / b.nr;
+      r = l0 % nr;
+      c = l0 / nr;
     }
-    const float R = (float)(r + 1), Cc = (float)(c + 1);
-    const float du2 = FM(bilinear(pu + b.goff, g, R, Cc), 0.5f);
-    const float dv2 = FM(bilinear(pv + b.goff, g, R, Cc), 0.5f);
-    b.warpA[l] = bspline_eval(b.coefA, b.nr, b.nc, FS(R, dv2), FS(Cc, du2));
-    b.warpB[l] = bspline_eval(b.coefB, b.nr, b.nc, FA(R, dv2), FA(Cc, du2));
+    float wa[4], wb[4];
+    int ix = 0;
+    float dx = 0.f;
+    int64_t cx = -1;  // column whose x interpolation (ix, dx) is held
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      wa[j] = wb[j] = 0.f;
+      if (l0 + j < npx) {
+        int64_t rj = r + j, cj = c;
+        while (rj >= nr) {  // the quad wraps to the next column
+          rj -= nr;
+          ++cj;
+        }
+        const float R = (float)(rj + 1), Cc = (float)(cj + 1);
+        if (cj != cx) {
+          lin_axis(Cc, g.x0, g.xsp, g.gnx, ix, dx);
+          cx = cj;
+        }
+        int iy;
+        float dy;
+        lin_axis(R, g.y0, g.ysp, g.gny, iy, dy);
+        const float du2 = FM(bilinear_at(fu, g, iy, dy, ix, dx), 0.5f);
+        const float dv2 = FM(bilinear_at(fv, g, iy, dy, ix, dx), 0.5f);
+        wa[j] = bspline_eval(b.coefA, nr, nc, FS(R, dv2), FS(Cc, du2));
+        wb[j] = bspline_eval(b.coefB, nr, nc, FA(R, dv2), FA(Cc, du2));
+      }
+    }
+    if (l0 + 3 < npx) {
+      *reinterpret_cast<float4*>(b.warpA + l0) = make_float4(wa[0], wa[1], wa[2], wa[3]);
+      *reinterpret_cast<float4*>(b.warpB + l0) = make_float4(wb[0], wb[1], wb[2], wb[3]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (l0 + j < npx) {
+          b.warpA[l0 + j] = wa[j];
+          b.warpB[l0 + j] = wb[j];
+        }
+    }
   }
 }
 
 cudaError_t launch_b_deform(const BPair* bp, int npairs, const int32_t* done, int it, int64_t ptot, const float* pu,
                             const float* pv, cudaStream_t s) {
   if (ptot <= 0) return cudaSuccess;
-  b_deform_kernel<<<b_blocks(ptot, 32), 256, 0, s>>>(bp, npairs, done, it, ptot, pu, pv);
+  b_deform_kernel<<<b_blocks((ptot + 3) / 4, 32), 256, 0, s>>>(bp, npairs, done, it, ptot, pu, pv);
   return cudaGetLastError();
 }
 

@@ -262,7 +262,7 @@ template <int W> struct UQWCfg {
   static constexpr size_t win_bytes = 2 * (size_t)LD * W * sizeof(float) + (size_t)W * W;
   static constexpr size_t part_bytes = (44 * 33 + 44 * WPW) * sizeof(double);  // per warp: partials + totals
   static constexpr size_t smem() { return NWIN * win_bytes + 4 * part_bytes + 16; }
-  static constexpr int MINB = W <= 16 ? 3 : 2;  // CTAs per SM the register budget is sized for
+  static constexpr int MINB = 3;  // CTAs per SM the register budget is sized for
 };
 
 // sum over the lanes of one SEG-lane segment
