@@ -649,6 +649,13 @@ template <int N, int W> struct CorrCfg {
   static constexpr int MINB = HALF ? 3 : (N <= 48 ? 4 : (N <= 64 ? 3 : (N <= 96 ? 2 : 1)));
   // the peak analysis inline (one window per CTA: its latency is the CTA's)
   static constexpr bool INLINE_ANALYSIS = N >= 96;
+  // Canonical column c sits at storage column N2 (c % N1) + c / N1, and with
+  // LD = N + 1 a 64-bit element's bank pair is (column + row) mod 16, so at
+  // N = 128 consecutive canonical columns (8 storage columns apart) share two
+  // bank pairs. The first inverse pass then walks c = N1 u + v with u
+  // fastest, which halves its conflicts there (a model of the pass's
+  // addresses gives 1088 wavefronts instead of 2112 for 520 ideal).
+  static constexpr bool SPREAD7 = N == 128;
   // The spectrum is Hermitian, so the inverse transforms only the N/2 + 1
   // canonical columns along p and then rows p and p + N/2 together along q
   // (their outputs are real: one lands in the real part, one in the
@@ -661,7 +668,11 @@ template <int N, int W> struct CorrCfg {
   static constexpr int NZ1 = PADDED ? (W / N2) : N1;  // nonzero inputs of a forward pass-A line
 
   static constexpr int EPT = (W * W + G - 1) / G;             // window pixels per thread
-  static constexpr size_t PLANE_B = (size_t)N * LD * sizeof(float2);
+  // plane stride in float2; the two windows of a half-warp pair start 16
+  // banks apart, so their 32-bit plane accesses (peak scan, real-plane
+  // writes) do not meet in one bank
+  static constexpr int PS = N * LD + (HALF ? 8 : 0);
+  static constexpr size_t PLANE_B = (size_t)PS * sizeof(float2);
   static constexpr size_t smem() {
     return WPC * PLANE_B + WPC * (G / 32) * 3 * sizeof(double) + N * sizeof(float2) +
            WPC * (G / 32) * 2 * KMAX * sizeof(uint32_t) +
@@ -677,7 +688,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
   using C = CorrCfg<N, W>;
   constexpr int WPC = C::WPC, NT = C::NT, LD = C::LD, LDR = C::LDR, N1 = C::N1, N2 = C::N2, IPT = C::IPT;
   constexpr int G = C::G, EPT = C::EPT, NC = C::NC, H = N / 2;
-  constexpr int PS = N * LD;
+  constexpr int PS = C::PS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* planes = reinterpret_cast<float2*>(smem_raw);
   double* s_part = reinterpret_cast<double*>(smem_raw + WPC * C::PLANE_B);  // 3 per warp: sum A, sum B, count
@@ -918,7 +929,21 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
     if (N2 > 1) {
 #pragma unroll 1
       for (int it = gt; it < NC * N1; it += G) {
-        const int c = it % NC, k1 = it / NC;
+        int c, k1;
+        if (C::SPREAD7) {  // c = N1 u + v with u fastest, then v, then k1; c = N/2 last
+          if (it < H * N1) {
+            constexpr int U = N2 / 2 > 0 ? N2 / 2 : 1;
+            const int u = it % U, w = it / U;
+            c = N1 * u + w % N1;
+            k1 = w / N1;
+          } else {
+            c = H;
+            k1 = it - H * N1;
+          }
+        } else {
+          c = it % NC;
+          k1 = it / NC;
+        }
         const int aq = s_canon[c], bq = s_neg[aq];
         float2* L = P + aq * LD + N2 * k1;
         const float2* Lb = P + bq * LD;
@@ -947,9 +972,12 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
     //      With N2 = 1 the two self-paired columns kq = 0 and N/2, whose
     //      results are real, share one transform as col0 + i col(N/2) (real
     //      part: column 0, imaginary part: column N/2): H items in all.
+    //      With N2 > 1 consecutive threads take consecutive n2 of one column
+    //      (the canonical columns sit N2 storage columns apart, which alias
+    //      to two banks; rows n2 of one column do not).
     for (int it = gt; it < (N2 == 1 ? H : NC * N2); it += G) {
       const bool pk = N2 == 1 && it == 0;
-      const int c = N2 == 1 ? it : it % NC, n2 = N2 == 1 ? 0 : it / NC;
+      const int c = N2 == 1 ? it : it / N2, n2 = N2 == 1 ? 0 : it % N2;
       const int aq = N2 == 1 ? c : s_canon[c];
       const int bq = pk ? H : (N2 == 1 ? N - c : s_neg[aq]);
       float2* L = P + aq * LD;
