@@ -259,9 +259,12 @@ template <int W> struct UQWCfg {
   static constexpr int WPW = M <= 16 ? 2 : 1;  // windows per warp
   static constexpr int SEG = 32 / WPW;         // lanes per window
   static constexpr int NWIN = 2 * WPW;         // windows per CTA
-  static constexpr size_t win_bytes = 2 * (size_t)LD * W * sizeof(float) + (size_t)W * W;
+  // window buffers of consecutive slots start 16 banks apart (64 bytes mod
+  // 128), so the two windows of a warp do not meet in one bank
+  static constexpr size_t win_raw = 2 * (size_t)LD * W * sizeof(float) + (size_t)W * W;
+  static constexpr size_t win_bytes = (win_raw + 127) / 128 * 128 + 64;
   static constexpr size_t part_bytes = (44 * 33 + 44 * WPW) * sizeof(double);  // per warp: partials + totals
-  static constexpr size_t smem() { return NWIN * win_bytes + 4 * part_bytes + 16; }
+  static constexpr size_t smem() { return NWIN * win_bytes + 4 * part_bytes + sizeof(UQOffsets) + 16; }
   static constexpr int MINB = 3;  // CTAs per SM the register budget is sized for
 };
 
@@ -280,7 +283,12 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* part_all = reinterpret_cast<double*>(smem_raw);  // [warp][44][33] + totals
   unsigned char* wbase = smem_raw + 4 * C::part_bytes;
+  // the offset tables in shared memory (indexed at run time; a parameter
+  // struct indexed that way would be copied to local memory)
+  UQOffsets& so = *reinterpret_cast<UQOffsets*>(wbase + NWIN * C::win_bytes);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) so = o;
+  __syncthreads();
   const int comp = warp & 1, seg = lane / SEG, c = lane % SEG;
   const int slot = (warp >> 1) * WPW + seg;  // window of this lane
   const int ts = comp * SEG + c;             // this lane among the 2*SEG threads of its window
@@ -462,7 +470,7 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
         const int g = j / 44, st = j % 44;
         double t = 0.0;
         for (int l = 0; l < (WPW == 1 ? 32 : M); ++l) t += part[st * 33 + g * SEG + l];
-        const int ri = st < 4 ? st : 4 + o.nat2ring[st - 4];
+        const int ri = st < 4 ? st : 4 + so.nat2ring[st - 4];
         tot[g * 44 + ri] = t;
         bool og = on_s[0];
         int64_t jg = job_s[0];
@@ -478,7 +486,7 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
         }
       }
       __syncwarp();
-      if (c == 0 && on && a.unc_u) (comp == 0 ? a.unc_u : a.unc_v)[gid] = uq_finalize(tot + seg * 44, o);
+      if (c == 0 && on && a.unc_u) (comp == 0 ? a.unc_u : a.unc_v)[gid] = uq_finalize(tot + seg * 44, so);
     }
     __syncthreads();  // the window buffers are reused by the next iteration
   }
