@@ -586,21 +586,28 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
   if (gtid >= 32 || !active) return;
   __syncwarp(grp_mask(gsize));
   if (rec && finder == 0) {
-    const int lane = gtid;
-    if (lane == 0) rec[job] = __int_as_float(nfound);
-    if (lane < nfound) {
-      const int pr = s_locs[2 * lane], pc = s_locs[2 * lane + 1];
-      rec[(int64_t)(1 + lane) * rec_stride + job] = s_vals[lane];
-      rec[(int64_t)(1 + K + 2 * lane) * rec_stride + job] = __int_as_float(pr);
-      rec[(int64_t)(2 + K + 2 * lane) * rec_stride + job] = __int_as_float(pc);
-      const int h = lane == 0 ? 2 : 1, w = 2 * h + 1;
-      float* P = rec + (int64_t)rec_patch(K, lane) * rec_stride + job;
-      for (int dc = -h; dc <= h; ++dc)
-        for (int dr = -h; dr <= h; ++dr) {
-          const int i = pr + dr, j = pc + dc;
-          P[(int64_t)((dc + h) * w + (dr + h)) * rec_stride] =
-              (i >= 0 && i < nr && j >= 0 && j < nc) ? R[j * ldr + i] : 0.f;
+    // the record's words spread over the lanes (a few each), so its shared
+    // loads and global stores overlap instead of one lane walking the patches
+    const int lanes = gsize < 32 ? gsize : 32, base0 = 1 + 3 * K, nw = rec_words(K);
+    for (int wd = gtid; wd < nw; wd += lanes) {
+      float val = 0.f;
+      if (wd == 0) {
+        val = __int_as_float(nfound);
+      } else if (wd <= K) {
+        val = wd - 1 < nfound ? s_vals[wd - 1] : 0.f;
+      } else if (wd < base0) {
+        const int m = (wd - 1 - K) >> 1;
+        val = m < nfound ? __int_as_float(s_locs[wd - 1 - K]) : 0.f;
+      } else {
+        const int e = wd - base0;  // primary: 25 cells; alternative m: 9 cells
+        const int m = e < 25 ? 0 : 1 + (e - 25) / 9, cell = e < 25 ? e : (e - 25) % 9;
+        const int h = m == 0 ? 2 : 1, w = 2 * h + 1;
+        if (m < nfound) {
+          const int i = s_locs[2 * m] + cell % w - h, j = s_locs[2 * m + 1] + cell / w - h;
+          val = (i >= 0 && i < nr && j >= 0 && j < nc) ? R[j * ldr + i] : 0.f;
         }
+      }
+      rec[(int64_t)wd * rec_stride + job] = val;
     }
     return;
   }
