@@ -134,9 +134,9 @@ template <int N> struct AxisSplit;
 template <> struct AxisSplit<16> { static constexpr int N1 = 16, N2 = 1; };
 template <> struct AxisSplit<24> { static constexpr int N1 = 24, N2 = 1; };
 template <> struct AxisSplit<32> { static constexpr int N1 = 32, N2 = 1; };
-template <> struct AxisSplit<48> { static constexpr int N1 = 16, N2 = 3; };
-template <> struct AxisSplit<64> { static constexpr int N1 = 8, N2 = 8; };
-template <> struct AxisSplit<96> { static constexpr int N1 = 16, N2 = 6; };
+template <> struct AxisSplit<48> { static constexpr int N1 = 8, N2 = 6; };
+template <> struct AxisSplit<64> { static constexpr int N1 = 16, N2 = 4; };
+template <> struct AxisSplit<96> { static constexpr int N1 = 12, N2 = 8; };
 template <> struct AxisSplit<128> { static constexpr int N1 = 16, N2 = 8; };
 
 }  // namespace hh

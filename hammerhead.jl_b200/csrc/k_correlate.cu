@@ -424,7 +424,7 @@ __device__ __forceinline__ ScanPlan scan_plan(int gtid, int gsize, int rlo, int 
 __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
                                              int subpixel, int gtid, int gsize, uint32_t* red, bool active,
                                              float* s_vals, int* s_locs, int64_t grid_id, int64_t job,
-                                             const PeakOut& o, bool poison, int bar, const ScanPlan sp,
+                                             const PeakOut* o, bool poison, int bar, const ScanPlan sp,
                                              float* rec, int64_t rec_stride) {
   const int rlo = sp.rlo, rhi = sp.rhi, clo = sp.clo, chi = sp.chi;
   // a poisoned plane (non-finite window data: the reference's plane is all
@@ -611,7 +611,7 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
     }
     return;
   }
-  if (gtid == 0) peak_outputs(PlaneSrc{R, ldr}, nr, nc, K, npeaks, subpixel, nfound, s_vals, s_locs, grid_id, job, o);
+  if (gtid == 0) peak_outputs(PlaneSrc{R, ldr}, nr, nc, K, npeaks, subpixel, nfound, s_vals, s_locs, grid_id, job, *o);
 }
 
 // The analysis as a call: small planes keep it out of line (the kernel's
@@ -619,7 +619,7 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
 __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
                                            int subpixel, int gtid, int gsize, uint32_t* red, bool active,
                                            float* s_vals, int* s_locs, int64_t grid_id, int64_t job,
-                                           const PeakOut& o, bool poison, int bar, const ScanPlan sp,
+                                           const PeakOut* o, bool poison, int bar, const ScanPlan sp,
                                            float* rec, int64_t rec_stride) {
   analyze_body(R, nr, nc, ldr, K, npeaks, finder, subpixel, gtid, gsize, red, active, s_vals, s_locs, grid_id, job, o,
                poison, bar, sp, rec, rec_stride);
@@ -657,12 +657,12 @@ template <int N, int W> struct CorrCfg {
   // the peak analysis inline (one window per CTA: its latency is the CTA's)
   static constexpr bool INLINE_ANALYSIS = N >= 96;
   // Canonical column c sits at storage column N2 (c % N1) + c / N1, and with
-  // LD = N + 1 a 64-bit element's bank pair is (column + row) mod 16, so at
-  // N = 128 consecutive canonical columns (8 storage columns apart) share two
+  // LD = N + 1 a 64-bit element's bank pair is (column + row) mod 16, so with
+  // N2 = 8 consecutive canonical columns (8 storage columns apart) share two
   // bank pairs. The first inverse pass then walks c = N1 u + v with u
-  // fastest, which halves its conflicts there (a model of the pass's
-  // addresses gives 1088 wavefronts instead of 2112 for 520 ideal).
-  static constexpr bool SPREAD7 = N == 128;
+  // fastest (a model of the pass's addresses: 1088 wavefronts instead of
+  // 2112 for 520 ideal at N = 128, 624 instead of 912 for 296 at N = 96).
+  static constexpr bool SPREAD7 = N2 == 8;
   // The spectrum is Hermitian, so the inverse transforms only the N/2 + 1
   // canonical columns along p and then rows p and p + N/2 together along q
   // (their outputs are real: one lands in the real part, one in the
@@ -1123,14 +1123,16 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
         continue;
       }
     }
-    // ---- stage 9: peak analysis by the group
+    // ---- stage 9: peak analysis by the group (the output pointers are
+    //      needed only when the outputs are formed here, not from a record)
+    const bool defer = a.rec && a.finder == 0;
     uint32_t* gred = red + w * (G / 32) * 2 * KMAX;
     if (C::INLINE_ANALYSIS)
       analyze_body(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
-                   s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, sp, a.rec, a.njobs);
+                   s_locs + w * 2 * KMAX, gid, job, defer ? nullptr : &pw, bad, bar, sp, a.rec, a.njobs);
     else
       analyze_group(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
-                    s_locs + w * 2 * KMAX, gid, job, pw, bad, bar, sp, a.rec, a.njobs);
+                    s_locs + w * 2 * KMAX, gid, job, defer ? nullptr : &pw, bad, bar, sp, a.rec, a.njobs);
     grp_sync(bar, G);  // the plane is reused by the group's next window
   }
 }
@@ -1151,7 +1153,7 @@ __global__ void __launch_bounds__(128) analyze_planes_kernel(const AnalyzeArgs a
     __syncthreads();
     const int64_t gid = a.jobs ? (int64_t)a.jobs[4 * pl] + (int64_t)a.jobs[4 * pl + 1] * a.ny : -1;
     analyze_group(R, a.nr, a.nc, a.nr, K, a.npeaks, a.finder, a.subpixel, threadIdx.x, 128, red, true, s_vals,
-                  s_locs, gid, pl, po, false, 0, sp, nullptr, 0);
+                  s_locs, gid, pl, &po, false, 0, sp, nullptr, 0);
     __syncthreads();
   }
 }
