@@ -264,7 +264,12 @@ template <int W> struct UQWCfg {
   static constexpr size_t win_raw = 2 * (size_t)LD * W * sizeof(float) + (size_t)W * W;
   static constexpr size_t win_bytes = (win_raw + 127) / 128 * 128 + 64;
   static constexpr size_t part_bytes = (44 * 33 + 44 * WPW) * sizeof(double);  // per warp: partials + totals
-  static constexpr size_t smem() { return NWIN * win_bytes + 4 * part_bytes + sizeof(UQOffsets) + 16; }
+  // the next windows are copied in (cp.async) while the current ones are
+  // reduced, into a second set of buffers (timed: faster up to 16 px, no
+  // gain at 24 px, and at 32 px the buffers would cost a CTA per SM)
+  static constexpr bool PREFETCH = W <= 16;
+  static constexpr int NBUF = PREFETCH ? 2 : 1;
+  static constexpr size_t smem() { return NBUF * NWIN * win_bytes + 4 * part_bytes + sizeof(UQOffsets) + 16; }
   static constexpr int MINB = 3;  // CTAs per SM the register budget is sized for
 };
 
@@ -274,6 +279,48 @@ template <int SEG> __device__ __forceinline__ double seg_sum(double v) {
   for (int o = SEG / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+
+// Where window `job` comes from: on = the window is estimated in this launch.
+struct UQSrc {
+  bool on;
+  const float* A;
+  const float* B;
+  const uint8_t* M;
+  int64_t ld, gid;
+  int rs, cs;
+};
+__device__ __forceinline__ UQSrc uq_src(const UQArgs& a, int64_t job) {
+  UQSrc r{job < a.njobs, a.A, a.B, a.mask, a.ld, -1, 0, 0};
+  if (r.on) {
+    r.rs = a.jobs[4 * job + 2];
+    r.cs = a.jobs[4 * job + 3];
+    if (a.bp) {
+      const int p = a.jobs[4 * job];
+      const BPair& b = a.bp[p];
+      const int gij = a.jobs[4 * job + 1];
+      const int64_t cell = (int64_t)(gij & 0xFFFF) + (int64_t)(gij >> 16) * b.ny;
+      r.on = a.mode == 0 ? (b.unc_fused && bp_live(b, 1, a.done, p)) : (b.unc_post && b.live);
+      r.on = r.on && !(b.gmask && b.gmask[cell]);
+      const bool warped = a.mode == 1 || b.has_pred0;
+      r.A = warped ? b.warpA : b.A;
+      r.B = warped ? b.warpB : b.B;
+      r.M = b.mask;
+      r.ld = b.nr;
+      r.gid = b.goff + cell;
+    } else {
+      r.gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
+    }
+  }
+  return r;
+}
+
+// 4-byte asynchronous global -> shared copy and its group operations
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 template <int W>
 __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(const UQArgs a, const UQOffsets o) {
@@ -285,52 +332,72 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
   unsigned char* wbase = smem_raw + 4 * C::part_bytes;
   // the offset tables in shared memory (indexed at run time; a parameter
   // struct indexed that way would be copied to local memory)
-  UQOffsets& so = *reinterpret_cast<UQOffsets*>(wbase + NWIN * C::win_bytes);
+  UQOffsets& so = *reinterpret_cast<UQOffsets*>(wbase + C::NBUF * NWIN * C::win_bytes);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) so = o;
   __syncthreads();
   const int comp = warp & 1, seg = lane / SEG, c = lane % SEG;
   const int slot = (warp >> 1) * WPW + seg;  // window of this lane
   const int ts = comp * SEG + c;             // this lane among the 2*SEG threads of its window
-  float* wa = reinterpret_cast<float*>(wbase + slot * C::win_bytes);  // W x W, column stride LD
-  float* wb = wa + LD * W;
-  uint8_t* mf = reinterpret_cast<uint8_t*>(wb + LD * W);
   double* part = part_all + warp * (C::part_bytes / sizeof(double));
-  for (int64_t base = (int64_t)blockIdx.x * NWIN; base < a.njobs; base += (int64_t)gridDim.x * NWIN) {
-    const int64_t job = base + slot;
-    // ---- the window's source (uniform within the window's lanes)
-    bool on = job < a.njobs;
-    const float* A = a.A;
-    const float* B = a.B;
-    const uint8_t* Mk = a.mask;
-    int64_t ld = a.ld, gid = -1;
-    int rs = 0, cs = 0;
-    if (on) {
-      rs = a.jobs[4 * job + 2];
-      cs = a.jobs[4 * job + 3];
-      if (a.bp) {
-        const int p = a.jobs[4 * job];
-        const BPair& b = a.bp[p];
-        const int gij = a.jobs[4 * job + 1];
-        const int64_t cell = (int64_t)(gij & 0xFFFF) + (int64_t)(gij >> 16) * b.ny;
-        on = a.mode == 0 ? (b.unc_fused && bp_live(b, 1, a.done, p)) : (b.unc_post && b.live);
-        on = on && !(b.gmask && b.gmask[cell]);
-        const bool warped = a.mode == 1 || b.has_pred0;
-        A = warped ? b.warpA : b.A;
-        B = warped ? b.warpB : b.B;
-        Mk = b.mask;
-        ld = b.nr;
-        gid = b.goff + cell;
-      } else {
-        gid = (int64_t)a.jobs[4 * job] + (int64_t)a.jobs[4 * job + 1] * a.ny;
+  const int64_t stride = (int64_t)gridDim.x * NWIN;
+  // copies the window's pixels into buffer set `ph` asynchronously
+  auto prefetch = [&](const UQSrc& q0, int ph) {
+    float* pa = reinterpret_cast<float*>(wbase + (ph * NWIN + slot) * C::win_bytes);
+    float* pb = pa + LD * W;
+    if (q0.on)
+      for (int k = ts; k < W * W; k += 2 * SEG) {
+        const int p = k % W, q = k / W;
+        const int64_t off = (int64_t)(q0.rs + p) + (int64_t)(q0.cs + q) * q0.ld;
+        cp_async4(pa + p + q * LD, q0.A + off);
+        cp_async4(pb + p + q * LD, q0.B + off);
       }
-    }
+  };
+  int iter = 0;
+  if (C::PREFETCH) {
+    const int64_t base0 = (int64_t)blockIdx.x * NWIN;
+    if (base0 < a.njobs) prefetch(uq_src(a, base0 + slot), 0);
+    cp_async_commit();
+  }
+  for (int64_t base = (int64_t)blockIdx.x * NWIN; base < a.njobs; base += stride, ++iter) {
+    const int64_t job = base + slot;
+    const int ph = C::PREFETCH ? (iter & 1) : 0;
+    float* wa = reinterpret_cast<float*>(wbase + (ph * NWIN + slot) * C::win_bytes);  // W x W, column stride LD
+    float* wb = wa + LD * W;
+    uint8_t* mf = reinterpret_cast<uint8_t*>(wb + LD * W);
+    // ---- the window's source (uniform within the window's lanes)
+    const UQSrc src = uq_src(a, job);
+    const bool on = src.on;
+    const float* A = src.A;
+    const float* B = src.B;
+    const uint8_t* Mk = src.M;
+    const int64_t ld = src.ld, gid = src.gid;
+    const int rs = src.rs, cs = src.cs;
     // with two windows per warp every lane runs the arithmetic below (the
     // shuffles span the warp, whose windows may differ in `on`); a window
     // that is off computes on zeros and writes nothing. With one window per
     // warp `on` is uniform and an idle warp pair skips the work.
     const bool run = WPW == 1 ? on : true;
-    if (run)
+    if (C::PREFETCH) {
+      // the next windows go to the other buffer set while these are reduced
+      // (that set was last read in the previous iteration, before its final
+      // barrier); then wait for this set's copies, issued one group earlier
+      if (base + stride < a.njobs) prefetch(uq_src(a, base + stride + slot), ph ^ 1);
+      cp_async_commit();
+      cp_async_wait_prev();
+      if (run)
+        for (int k = ts; k < W * W; k += 2 * SEG) {
+          const int p = k % W, q = k / W;
+          uint8_t mk = 1;
+          if (on) {
+            mk = Mk ? __ldg(Mk + (int64_t)(rs + p) + (int64_t)(cs + q) * ld) : 0;
+          } else {
+            wa[p + q * LD] = 0.f;
+            wb[p + q * LD] = 0.f;
+          }
+          mf[k] = mk;
+        }
+    } else if (run) {
       for (int k = ts; k < W * W; k += 2 * SEG) {
         const int p = k % W, q = k / W;
         float va = 0.f, vb = 0.f;
@@ -345,6 +412,7 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
         wb[p + q * LD] = vb;
         mf[k] = mk;
       }
+    }
     __syncthreads();
     // ---- window means (load_uncertainty_windows!), FP64, computed by each warp
     float ma = 0.f, mb = 0.f;
