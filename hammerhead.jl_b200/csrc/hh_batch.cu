@@ -591,10 +591,12 @@ static hh_status stage_inputs(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs,
       }
     }
   }
+  // the tables and grid masks are read from their page-locked staging by a
+  // kernel: an upload through the copy engine would queue behind frame
+  // copies that a caller streams in on another stream meanwhile
   memcpy(P.h_tables, P.tables.data(), sizeof(BPair) * P.tables.size());
-  HH_CK(cudaMemcpyAsync(P.d_tables, P.h_tables, sizeof(BPair) * P.tables.size(), cudaMemcpyHostToDevice, s));
-  if (any_mask)
-    HH_CK(cudaMemcpyAsync(P.d_gmask, P.h_gmask, (size_t)P.nslots * P.gcap, cudaMemcpyHostToDevice, s));
+  HH_CK(hh::launch_host_read_copy(P.d_tables, P.h_tables, sizeof(BPair) * P.tables.size(), s));
+  if (any_mask) HH_CK(hh::launch_host_read_copy(P.d_gmask, P.h_gmask, (size_t)P.nslots * P.gcap, s));
   return HH_OK;
 }
 

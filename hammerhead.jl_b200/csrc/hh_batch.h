@@ -95,6 +95,11 @@ __device__ __forceinline__ int bp_find(const BPair* bp, int npairs, int64_t k) {
 // --- batched launches (k_batch.cu, k_deform.cu) --------------------------------
 // Totals of the index spaces a launch covers are passed by the host; the
 // kernels stop at them and skip pairs that are not live.
+// Copy `bytes` from page-locked host memory (addressable from the device
+// under unified addressing) to device memory with a kernel, not a copy-engine
+// transfer: the small per-call uploads then never wait behind large frame
+// copies that other streams have queued on the host-to-device copy engine.
+cudaError_t launch_host_read_copy(void* dst, const void* host_src, size_t bytes, cudaStream_t s);
 cudaError_t launch_b_prefilter(const BPair* bp, int npairs, int64_t qtot, int64_t wcol_tot, int64_t wrow_tot,
                                float* dbuf, cudaStream_t s);
 cudaError_t launch_b_sweep_begin(const BPair* bp, int npairs, const int32_t* done, int it, int64_t gtot,

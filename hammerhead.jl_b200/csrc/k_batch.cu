@@ -284,4 +284,23 @@ cudaError_t launch_b_gather(const BPair* bp, int npairs, int64_t rtot, const BGr
   return cudaGetLastError();
 }
 
+// 16-byte words while both addresses and the length allow, then the tail by
+// bytes; the source is page-locked host memory read over the bus
+__global__ void host_read_copy_kernel(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, size_t bytes) {
+  const size_t n16 = ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 15) ? 0 : bytes / 16;
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x, nt = (size_t)gridDim.x * blockDim.x;
+  for (size_t k = t; k < n16; k += nt) reinterpret_cast<uint4*>(dst)[k] = reinterpret_cast<const uint4*>(src)[k];
+  for (size_t k = n16 * 16 + t; k < bytes; k += nt) dst[k] = src[k];
+}
+
+cudaError_t launch_host_read_copy(void* dst, const void* host_src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return cudaSuccess;
+  size_t blocks = (bytes / 16 + 255) / 256;
+  if (blocks < 1) blocks = 1;
+  if (blocks > 148 * 4) blocks = 148 * 4;
+  host_read_copy_kernel<<<(unsigned)blocks, 256, 0, s>>>(static_cast<uint8_t*>(dst), static_cast<const uint8_t*>(host_src),
+                                                         bytes);
+  return cudaGetLastError();
+}
+
 }  // namespace hh

@@ -23,7 +23,7 @@ from .pipeline import (PhysicalScale, PIVResult, PIVWorkspace, check_backend_par
                        with_scale)
 from . import adjoint
 from .adjoint import NCCLoss
-from .batch import BatchRunner, run_piv_batch, run_piv_sequence
+from .batch import BatchRunner, run_piv_batch, run_piv_batch_stream, run_piv_sequence
 from .ensemble import run_piv_ensemble
 from .statistics import error_statistics, rms_error
 from . import synthetic
@@ -33,6 +33,6 @@ __all__ = [
     "effort_schedule", "parse_validator", "PeakRatioValidator", "CorrelationMomentValidator",
     "VelocityMagnitudeValidator", "UniversalOutlierValidator", "PIVResult", "PIVWorkspace", "PhysicalScale",
     "piv_workspace", "run_piv", "pass_grid", "check_backend_params", "with_scale", "error_statistics", "rms_error",
-    "synthetic", "BatchRunner", "run_piv_batch", "run_piv_sequence", "NCCLoss", "adjoint",
+    "synthetic", "BatchRunner", "run_piv_batch", "run_piv_batch_stream", "run_piv_sequence", "NCCLoss", "adjoint",
     "run_piv_ensemble",
 ]

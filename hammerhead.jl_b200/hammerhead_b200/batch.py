@@ -347,6 +347,121 @@ def _sequence_pipelined(pairs, params, on_result, progress, batch_size, smoothin
     return out
 
 
+def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_threshold=0.5, workspace=None,
+                         u16="normalised", on_batch=None):
+    """A stream of batches of the same composition (for example every camera
+    of a rig at each time step): batch k+1's frames are copied to the device
+    on a copy stream while batch k is analysed, so the host-to-device copies
+    overlap the analysis. Returns one list of PIVResult per batch (in order),
+    equal to run_piv_batch on that batch; `on_batch(k, results)` is called as
+    each batch completes (0-based k).
+
+    Every batch holds the same number of pairs, and pair j has the same
+    shape and pixel type (float32 or UInt16) in every batch. Frames in
+    page-locked memory (for example numpy views of pinned torch tensors,
+    column-major) are copied directly; others go through page-locked
+    staging buffers first. Needs a CUDA device visible to torch; masks are
+    not supported on this path (use run_piv_batch)."""
+    import concurrent.futures as cf
+
+    import torch
+
+    it = iter(batches)
+    try:
+        first = list(next(it))
+    except StopIteration:
+        return []
+    if not first:
+        raise ArgumentError("batches must not be empty")
+    n = len(first)
+    spec = []
+    for a, b in first:
+        if tuple(a.shape) != tuple(b.shape) or len(a.shape) != 2:
+            raise DimensionMismatch("each pair's frames must be matrices of one size")
+        tdt = torch.uint16 if _is_u16(a) else torch.float32
+        spec.append((int(a.shape[0]), int(a.shape[1]), tdt))
+    own = workspace is None
+    ws = workspace if workspace is not None else PIVWorkspace()
+    copy_stream = torch.cuda.Stream()
+    # two sets of device frames (column-major: tensors (nc, nr) seen through .T)
+    dev = [[(torch.empty((nc, nr), dtype=t, device="cuda"), torch.empty((nc, nr), dtype=t, device="cuda"))
+            for nr, nc, t in spec] for _ in range(2)]
+    stage_host = {}  # page-locked staging for frames that are not page-locked already
+    events = [torch.cuda.Event(), torch.cuda.Event()]
+
+    def host_tensor(x, j, which, slot):
+        nr, nc, t = spec[j]
+        if tuple(x.shape) != (nr, nc):
+            raise DimensionMismatch(f"pair {j} changed size in the stream: {tuple(x.shape)} vs {(nr, nc)}")
+        nd = np.uint16 if t == torch.uint16 else np.float32
+        xt = np.asarray(x).T  # (nc, nr); C-contiguous when x is column-major
+        if xt.dtype == nd and xt.flags["C_CONTIGUOUS"]:
+            h = torch.from_numpy(xt)
+            if h.is_pinned():
+                return h
+        key = (slot, j, which)
+        if key not in stage_host:
+            stage_host[key] = torch.empty((nc, nr), dtype=t, pin_memory=True)
+        stage_host[key].numpy()[...] = xt.astype(nd, copy=False)
+        return stage_host[key]
+
+    def stage(batch, slot):
+        batch = list(batch)
+        if len(batch) != n:
+            raise DimensionMismatch(f"every batch must hold {n} pairs, got {len(batch)}")
+        srcs = [(host_tensor(a, j, 0, slot), host_tensor(b, j, 1, slot)) for j, (a, b) in enumerate(batch)]
+        with torch.cuda.stream(copy_stream):
+            for (da, db), (ha, hb_) in zip(dev[slot], srcs):
+                da.copy_(ha, non_blocking=True)
+                db.copy_(hb_, non_blocking=True)
+            events[slot].record(copy_stream)
+        return srcs  # kept alive until the copies are done
+
+    runners = [BatchRunner([(a.T, b.T) for a, b in dev[s]], passes, predictor_smoothing=predictor_smoothing,
+                           mask_threshold=mask_threshold, workspace=ws, u16=u16) for s in range(2)]
+    out = []
+    conv = [None, None]  # result conversion of the batch last analysed by each runner
+
+    def collect(k, slot):
+        res = runners[slot].results(copy=True)
+        if on_batch is not None:
+            on_batch(k, res)
+        return res
+
+    try:
+        with cf.ThreadPoolExecutor(max_workers=1) as pool, cf.ThreadPoolExecutor(max_workers=1) as post:
+            fut = pool.submit(stage, first, 0)
+            k = 0
+            while fut is not None:
+                slot = k % 2
+                fut.result()
+                try:
+                    nxt = next(it)
+                except StopIteration:
+                    nxt = None
+                # batch k+1 streams into the other set while batch k is analysed
+                # (that set's previous batch, k-1, finished before this point)
+                fut = pool.submit(stage, nxt, 1 - slot) if nxt is not None else None
+                events[slot].synchronize()
+                if conv[slot] is not None:  # this runner's buffers still hold batch k-2
+                    out.append(conv[slot].result())
+                    conv[slot] = None
+                runners[slot].run()
+                # the results of batch k become PIVResults while batch k+1 runs
+                conv[slot] = post.submit(collect, k, slot)
+                k += 1
+            for j in range(k - 2, k):
+                if j >= 0 and conv[j % 2] is not None:
+                    out.append(conv[j % 2].result())
+                    conv[j % 2] = None
+    finally:
+        for r in runners:
+            r.close()
+        if own:
+            ws.close()
+    return out
+
+
 class _Done:
     """A finished future (the staged size of the next batch)."""
 

@@ -212,3 +212,28 @@ def test_sequence_pipelined_equals_batch(hb, ws):
     unpiped = hb.run_piv_sequence(pairs, s1, batch_size=3, workspace=ws, pipeline=False)
     for a, b in zip(unpiped, ref):
         _same(a, b)
+
+
+def test_batch_stream_equals_batch(hb, ws):
+    # a stream of three batches of the same composition (mixed sizes and
+    # schedules); batch k+1 is copied in while batch k is analysed. Frames
+    # of the second batch sit in page-locked memory (copied directly), the
+    # others in pageable numpy arrays (staged)
+    import torch
+
+    s1, s2 = _schedules(hb)
+    sched = [s1, s2, s2, s1]
+    batches = [_mixed(hb, n=4, seed=600 + 10 * k)[0] for k in range(3)]
+    pinned = []
+    for A, B in batches[1]:
+        pa = torch.from_numpy(np.ascontiguousarray(A.T)).pin_memory().numpy().T
+        pb = torch.from_numpy(np.ascontiguousarray(B.T)).pin_memory().numpy().T
+        pinned.append((pa, pb))
+    seen = []
+    out = hb.run_piv_batch_stream([batches[0], pinned, batches[2]], sched, workspace=ws,
+                                  on_batch=lambda k, r: seen.append(k))
+    assert seen == [0, 1, 2] and len(out) == 3
+    for k in range(3):
+        ref = hb.run_piv_batch(batches[k], sched, workspace=ws)
+        for a, b in zip(out[k], ref):
+            _same(a, b)
