@@ -237,3 +237,21 @@ def test_batch_stream_equals_batch(hb, ws):
         ref = hb.run_piv_batch(batches[k], sched, workspace=ws)
         for a, b in zip(out[k], ref):
             _same(a, b)
+
+
+def test_batch_stream_uint16(hb, ws):
+    # UInt16 frames keep their pixel type on the device and are converted
+    # there, in a stream exactly as in one batch call
+    syn = hb.synthetic
+    s1, s2 = _schedules(hb)
+    batches = []
+    for k in range(2):
+        b = []
+        for i, shape in enumerate([(256, 256), (192, 320)]):
+            A, B = syn.particle_pair(shape, syn.uniform_flow(1.3 + k, -0.7), seed=900 + 10 * k + i)
+            b.append((syn.to_uint16_12bit(A), syn.to_uint16_12bit(B)))
+        batches.append(b)
+    out = hb.run_piv_batch_stream(batches, [s1, s2], workspace=ws)
+    for k in range(2):
+        for a, b in zip(out[k], hb.run_piv_batch(batches[k], [s1, s2], workspace=ws)):
+            _same(a, b)
