@@ -75,6 +75,9 @@ struct hh_ctx {
   // batched-schedule plans by batch shape (hh_batch.cu), most recent last
   std::vector<std::pair<std::string, void*>> bplans;
   void (*bplan_free)(void*) = nullptr;
+  // cross-process reduction of the ensemble sums (hh_set_ensemble_reducer)
+  hh_ensemble_reducer ens_reduce = nullptr;
+  void* ens_reduce_user = nullptr;
 };
 
 namespace hhd {

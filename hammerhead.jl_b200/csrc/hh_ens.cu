@@ -4,7 +4,9 @@
 // device-resident accumulator (and the Wieneke statistics to FP64 sums), and
 // after the last pair the summed planes are analysed once, combined with the
 // predictor and validated exactly like a WIDIM sweep. Only the final vector
-// grid returns to the host.
+// grid returns to the host. With the pairs split over processes, the context
+// reducer (hh_set_ensemble_reducer) turns each pass's partial sums into the
+// sums over all processes before the analysis.
 #include "hh_ctx.h"
 
 using namespace hhd;
@@ -225,6 +227,12 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
         }
       }
     }
+    // partial sums of this process's pairs -> sums over all processes
+    if (ctx->ens_reduce && njobs > 0) {
+      const int64_t nst = unc ? njobs * 88 : 0;
+      if (ctx->ens_reduce(ctx->ens_reduce_user, k, acc, njobs * N * N, unc ? stats : nullptr, nst, (void*)s) != 0)
+        return fail(ctx, HH_ERR_STATE, "ensemble reducer failed in pass " + std::to_string(k + 1));
+    }
     // ensemble_analyze! (src/ensemble.jl:273-305): one analysis of every summed plane
     HH_K(HH_K_VECTOR, 1, 0, 4 * G, G, hh::launch_fill(uncu, NaN, G, s));
     HH_K(HH_K_VECTOR, 1, 0, 4 * G, G, hh::launch_fill(uncv, NaN, G, s));
@@ -281,4 +289,11 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
   HH_CK(cudaStreamSynchronize(s));
   for (int k = 0; k < np; ++k) HH_CK(cudaEventElapsedTime(&ctx->pass_ms[k], ctx->events[k], ctx->events[k + 1]));
   return flush_profile(ctx);
+}
+
+extern "C" hh_status hh_set_ensemble_reducer(hh_ctx* ctx, hh_ensemble_reducer fn, void* user) {
+  if (!ctx) return fail(nullptr, HH_ERR_ARG, "context is NULL");
+  ctx->ens_reduce = fn;
+  ctx->ens_reduce_user = fn ? user : nullptr;
+  return HH_OK;
 }

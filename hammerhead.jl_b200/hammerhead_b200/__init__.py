@@ -24,7 +24,7 @@ from .pipeline import (PhysicalScale, PIVResult, PIVWorkspace, check_backend_par
 from . import adjoint
 from .adjoint import NCCLoss
 from .batch import BatchRunner, run_piv_batch, run_piv_batch_stream, run_piv_sequence
-from .ensemble import run_piv_ensemble
+from .ensemble import collective_reducer, run_piv_ensemble, shard_pairs
 from .statistics import error_statistics, rms_error
 from . import synthetic
 
@@ -35,4 +35,6 @@ __all__ = [
     "piv_workspace", "run_piv", "pass_grid", "check_backend_params", "with_scale", "error_statistics", "rms_error",
     "synthetic", "BatchRunner", "run_piv_batch", "run_piv_batch_stream", "run_piv_sequence", "NCCLoss", "adjoint",
     "run_piv_ensemble",
+    "shard_pairs",
+    "collective_reducer",
 ]

@@ -22,6 +22,10 @@ HH_ERR_STATE = 6
 
 MAX_VALIDATORS = 8
 
+# int32_t (*)(void* user, int32_t pass, float* planes, int64_t nplanes, double* stats, int64_t nstats, void* stream)
+ENSEMBLE_REDUCER = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
+                                    ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p)
+
 
 class hh_validator(ctypes.Structure):
     _fields_ = [
@@ -172,6 +176,7 @@ SIGNATURES = [
     ("hh_run_ensemble", ctypes.c_int32,
      [_CTX, ctypes.POINTER(hh_batch_pair), ctypes.c_int32, _PASS, ctypes.c_int32, _U8, ctypes.c_double,
       ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(hh_result)]),
+    ("hh_set_ensemble_reducer", ctypes.c_int32, [_CTX, ctypes.c_void_p, ctypes.c_void_p]),
     ("hh_ncc_loss_grad", ctypes.c_int32,
      [_CTX, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
       ctypes.c_float, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),

@@ -208,6 +208,27 @@ hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npair
                           int32_t npasses, const uint8_t* mask, double mask_threshold,
                           int32_t predictor_smoothing, int32_t flags, hh_result* out);
 
+/* Cross-process reduction of the ensemble sums (multi-GPU ensemble: each
+ * process holds a share of the pairs). The reference sums every plane on one
+ * host (accum[j] .+= plane, src/ensemble.jl:170-171; the uncertainty sums,
+ * :182-183); with the pairs split over processes each hh_run_ensemble call
+ * sums its own pairs and the reducer turns the partial sums into the sums
+ * over all processes before the planes are analysed. It is called once per
+ * pass that has windows, after the last local pair, with
+ *   planes : nplanes device floats (njobs x N x N, window-major),
+ *   stats  : nstats device doubles (njobs x 88), or NULL / 0 when the pass
+ *            carries no uncertainty,
+ *   stream : the context stream (cudaStream_t) the sums were produced on,
+ * and must leave in both arrays their element-wise sum over the processes,
+ * ordered on that stream (an in-place all-reduce, e.g. NCCL). Every process
+ * makes the same calls in the same order: the grids depend only on the image
+ * size, mask and passes, which must agree. A nonzero return fails the call
+ * with HH_ERR_STATE. fn == NULL removes the reducer. No counterpart in the
+ * reference (single-process only). */
+typedef int32_t (*hh_ensemble_reducer)(void* user, int32_t pass, float* planes, int64_t nplanes, double* stats,
+                                       int64_t nstats, void* stream);
+hh_status hh_set_ensemble_reducer(hh_ctx* ctx, hh_ensemble_reducer fn, void* user);
+
 /* ---- Differentiation: adjoint of deformation + correlation -------------
  *
  * No counterpart in the reference: a correlation loss of the predictor
