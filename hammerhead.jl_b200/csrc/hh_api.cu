@@ -187,7 +187,9 @@ hh_status run_schedule(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr
       ca.alt_v = nalt > 0 ? altv : nullptr;
       ca.nalt = nalt;
       ca.rec = prec;
-      HH_K(HH_K_CORRELATE, 1, corr_flops(N, njobs), corr_bytes(W, nalt, njobs), njobs, hh::launch_correlate(ca, N, W, s, ctx->num_sms));
+      ca.win = p.search[0] != W ? W : 0;
+      HH_K(HH_K_CORRELATE, 1, corr_flops(N, njobs), corr_bytes(p.search[0], nalt, njobs), njobs,
+           hh::launch_correlate(ca, N, p.search[0], s, ctx->num_sms));
       if (fused_unc) {
         hh::UQArgs ua{srcA, srcB, dmask, nr, djobs, njobs, ny, W, tb.apod, nullptr, uncu, uncv};
         HH_K(HH_K_UQ, 1, uq_flops(W, njobs), 8.0 * W * W * njobs, njobs, hh::launch_uq(ua, s, ctx->num_sms));
@@ -325,9 +327,6 @@ hh_status hh_check_backend_params(const hh_pass_desc* passes, int32_t npasses) {
   hh_ctx* ctx = nullptr;
   for (int k = 0; k < npasses; ++k) {
     const hh_pass_desc& p = passes[k];
-    if (p.search[0] != p.window[0] || p.search[1] != p.window[1])
-      return fail(ctx, HH_ERR_UNSUPPORTED,
-                  "backend :b200 does not support enlarged search_area_size yet; use backend = :cpu");
     if (!(p.subpixel == HH_GAUSS3 || p.subpixel == HH_GAUSS9 || p.subpixel == HH_SUBPIXEL_NONE))
       return fail(ctx, HH_ERR_UNSUPPORTED,
                   "backend :b200 supports subpixel_method :gauss3, :gauss9 or :none only (got :gauss2d); use backend = :cpu");
@@ -336,8 +335,16 @@ hh_status hh_check_backend_params(const hh_pass_desc* passes, int32_t npasses) {
                   "backend :b200 does not support keep_correlation_planes yet; use backend = :cpu");
     if (p.window[0] != p.window[1])
       return fail(ctx, HH_ERR_UNSUPPORTED, "backend :b200 supports square windows only, got window_size=" + tup(p.window));
-    const int N = fft_size(p), W = p.window[0];
-    if (!hh::correlate_supported(N, W))
+    if (p.search[0] != p.search[1])
+      return fail(ctx, HH_ERR_UNSUPPORTED,
+                  "backend :b200 supports square search areas only, got search_area_size=" + tup(p.search));
+    const int N = fft_size(p), W = p.window[0], S = p.search[0];
+    if (S != W && !hh::correlate_supported(N, S))
+      return fail(ctx, HH_ERR_UNSUPPORTED,
+                  "backend :b200 has no correlation kernel for search area " + std::to_string(S) +
+                      (p.padding ? " padded" : "") + " (FFT size " + std::to_string(N) +
+                      "); supported search areas: 16, 24, 32, 48, 64 (padded), 16, 24, 32, 48, 64, 96, 128 (unpadded)");
+    if (S == W && !hh::correlate_supported(N, W))
       return fail(ctx, HH_ERR_UNSUPPORTED,
                   "backend :b200 has no correlation kernel for window " + std::to_string(W) +
                       (p.padding ? " padded" : "") + " (FFT size " + std::to_string(N) +
@@ -618,13 +625,16 @@ hh_status hh_apply_predictor(hh_ctx* ctx, const float* pu, const float* pv, int3
   return HH_OK;
 }
 
+// Jobs of a hook call (1-based, from the caller) checked and copied to the
+// device 0-based; m is the margin of an enlarged search area around each
+// window.
 static hh_status hook_jobs(hh_ctx* ctx, const int32_t* jobs, int64_t njobs, int64_t nr, int64_t nc, int W,
-                           int32_t** djobs_out, int32_t* ny_out) {
+                           int32_t** djobs_out, int32_t* ny_out, int m = 0) {
   std::vector<int32_t> hj((size_t)4 * njobs);
   int32_t ny = 1;
   for (int64_t k = 0; k < njobs; ++k) {
     const int32_t gi = jobs[4 * k] - 1, gj = jobs[4 * k + 1] - 1, rs = jobs[4 * k + 2] - 1, cs = jobs[4 * k + 3] - 1;
-    if (rs < 0 || cs < 0 || rs + W > nr || cs + W > nc || gi < 0 || gj < 0)
+    if (rs - m < 0 || cs - m < 0 || rs + W + m > nr || cs + W + m > nc || gi < 0 || gj < 0)
       return fail(ctx, HH_ERR_ARG, "job " + std::to_string(k + 1) + " lies outside the image");
     hj[4 * k] = gi;
     hj[4 * k + 1] = gj;
@@ -651,7 +661,7 @@ static hh_status hook_correlate(hh_ctx* ctx, const hh_pass_desc* p, const int32_
   const int W = p->window[0], N = fft_size(*p), K = std::max(p->n_peaks, 2);
   int32_t* dj;
   int32_t ny;
-  HH_TRY(hook_jobs(ctx, jobs, njobs, ctx->nr, ctx->nc, W, &dj, &ny));
+  HH_TRY(hook_jobs(ctx, jobs, njobs, ctx->nr, ctx->nc, W, &dj, &ny, (p->search[0] - W) / 2));
   Tables tb;
   HH_TRY(get_tables(ctx, *p, tb));
   float *dpk = nullptr, *dpl = nullptr;
@@ -683,7 +693,8 @@ static hh_status hook_correlate(hh_ctx* ctx, const hh_pass_desc* p, const int32_
   ca.locs = dlc;
   ca.planes = dpl;
   ca.rec = drec;
-  HH_K(HH_K_CORRELATE, 1, 0, 0, 0, hh::launch_correlate(ca, N, W, s, ctx->num_sms));
+  ca.win = p->search[0] != W ? W : 0;
+  HH_K(HH_K_CORRELATE, 1, 0, 0, 0, hh::launch_correlate(ca, N, p->search[0], s, ctx->num_sms));
   if (uq) {
     HH_TRY(buf(ctx, "hook_uq", (size_t)88 * njobs, &duq));
     hh::UQArgs ua{ctx->curA, ctx->curB, nullptr, ctx->nr, dj, njobs, ny, W, tb.apod, duq, nullptr, nullptr};

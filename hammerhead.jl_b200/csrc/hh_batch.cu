@@ -18,7 +18,7 @@ using hh::BPair;
 namespace hhd {
 
 struct BClass {
-  int N = 0, W = 0, method = 0, npeaks = 1, finder = 0, subpixel = 0, apod = 0, padding = 0;
+  int N = 0, W = 0, S = 0, method = 0, npeaks = 1, finder = 0, subpixel = 0, apod = 0, padding = 0;  // S: search area
   Tables tb;
   std::vector<int32_t> hjobs;
   int32_t* jobs = nullptr;
@@ -344,6 +344,7 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
         BClass c;
         c.N = fft_size(pd);
         c.W = pd.window[0];
+        c.S = pd.search[0];
         c.method = pd.method;
         c.npeaks = pd.n_peaks;
         c.finder = pd.peak_finder;
@@ -431,8 +432,9 @@ static hh_status issue(hh_ctx* ctx, BPlan& P) {
         ca.done = P.d_done;
         ca.it = it;
         ca.rec = P.rec;
-        HH_K(HH_K_CORRELATE, 1, corr_flops(c.N, c.njobs), corr_bytes(c.W, c.npeaks - 1, c.njobs), c.njobs,
-             hh::launch_correlate(ca, c.N, c.W, s, ctx->num_sms));
+        ca.win = c.S != c.W ? c.W : 0;
+        HH_K(HH_K_CORRELATE, 1, corr_flops(c.N, c.njobs), corr_bytes(c.S, c.npeaks - 1, c.njobs), c.njobs,
+             hh::launch_correlate(ca, c.N, c.S, s, ctx->num_sms));
       }
       if (it == 1)
         for (const BClass& c : S.classes)

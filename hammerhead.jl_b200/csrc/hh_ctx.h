@@ -28,16 +28,17 @@ struct DevBuf {
 };
 
 struct TableKey {
-  int W, N, apod, method, padded;
+  int W, S, N, apod, method, padded;
   bool operator<(const TableKey& o) const {
-    return std::tie(W, N, apod, method, padded) < std::tie(o.W, o.N, o.apod, o.method, o.padded);
+    return std::tie(W, S, N, apod, method, padded) < std::tie(o.W, o.S, o.N, o.apod, o.method, o.padded);
   }
 };
 struct Tables {
   float* apod = nullptr;
   float* gain = nullptr;
   float* phasew = nullptr;
-  int box_lo = 0, box_hi = 0;  // support of the gain in fftshifted rows/columns (0, 0: whole plane)
+  // support of the gain, or the kept search lags, in fftshifted rows/columns (0, 0: whole plane)
+  int box_lo = 0, box_hi = 0;
 };
 
 }  // namespace hhd
@@ -236,8 +237,8 @@ inline void phase_table(int N, std::vector<float>& out) {
 }
 
 inline hh_status get_tables(hh_ctx* ctx, const hh_pass_desc& p, Tables& t) {
-  const int W = p.window[0], N = fft_size(p);
-  TableKey key{W, N, p.apodization, p.method, p.padding};
+  const int W = p.window[0], S = p.search[0], N = fft_size(p);
+  TableKey key{W, S, N, p.apodization, p.method, p.padding};
   auto it = ctx->tables.find(key);
   if (it != ctx->tables.end()) {
     t = it->second;
@@ -248,7 +249,13 @@ inline hh_status get_tables(hh_ctx* ctx, const hh_pass_desc& p, Tables& t) {
   Tables nt;
   HH_CK(cudaMalloc(&nt.apod, ap.size() * sizeof(float)));
   HH_CK(cudaMemcpy(nt.apod, ap.data(), ap.size() * sizeof(float), cudaMemcpyHostToDevice));
-  if (p.padding) {
+  if (S != W) {
+    // enlarged search area: no overlap gain (CrossCorrelator, src/correlators.jl:73);
+    // only lags with |lag| <= (S - W) / 2 are kept (restrict_search_lags!, :347-355)
+    const int m = (S - W) / 2;
+    nt.box_lo = N / 2 - m;
+    nt.box_hi = N / 2 + m;
+  } else if (p.padding) {
     gain_table(W, ap, gn);
     // bounding box of the nonzero gain (square and centred, by symmetry)
     int lo = N, hi = -1;

@@ -44,15 +44,21 @@ struct CorrArgs {
   // ensemble mode: planes += R (planes != nullptr) and no peak analysis
   int32_t accumulate;
   // fftshifted rows/columns [box_lo, box_hi] outside which the overlap gain
-  // is zero (box_hi == 0: the whole plane)
+  // is zero (box_hi == 0: the whole plane); with an enlarged search area the
+  // lags kept by restrict_search_lags! (src/correlators.jl:347-355)
   int32_t box_lo, box_hi;
+  // enlarged search area: the launch's W is the frame-B search area and win
+  // the frame-A window centred in it (jobs give the window's origin); 0 when
+  // the two are equal
+  int32_t win;
   // peak records (correlate_record_words(npeaks) x njobs floats) or nullptr:
   // with regional maxima the per-window outputs are then formed by a
   // one-thread-per-window epilogue kernel after the correlation kernel
   float* rec;
 };
 
-// Launch the correlation kernel for FFT size N (square) and window W.
+// Launch the correlation kernel for FFT size N (square) and window W (the
+// search area when a.win is set).
 cudaError_t launch_correlate(const CorrArgs& a, int N, int W, cudaStream_t s, int num_sms);
 bool correlate_supported(int N, int W);
 size_t correlate_record_words(int npeaks);  // per job

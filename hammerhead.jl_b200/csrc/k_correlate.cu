@@ -642,7 +642,9 @@ __device__ __forceinline__ float2 cross_spectrum(float2 X, float2 Zm, int method
 }
 
 // ---------------------------------------------------------------------------
-template <int N, int W> struct CorrCfg {
+// W is the extent of the data: the window, or with SRCH the frame-B search
+// area that holds the (runtime) frame-A window at its centre.
+template <int N, int W, bool SRCH = false> struct CorrCfg {
   static constexpr int N1 = AxisSplit<N>::N1, N2 = AxisSplit<N>::N2;
   // 16 x 16 windows padded to 32: every stage of the plane has at most 16
   // lines (16 data columns, 16 canonical column items, 16 row pairs), so
@@ -675,13 +677,14 @@ template <int N, int W> struct CorrCfg {
   static constexpr int NZ1 = PADDED ? (W / N2) : N1;  // nonzero inputs of a forward pass-A line
 
   static constexpr int EPT = (W * W + G - 1) / G;             // window pixels per thread
+  static constexpr int NPART = SRCH ? 4 : 3;  // FP64 partial sums per warp: A, B, count (and count of B)
   // plane stride in float2; the two windows of a half-warp pair start 16
   // banks apart, so their 32-bit plane accesses (peak scan, real-plane
   // writes) do not meet in one bank
   static constexpr int PS = N * LD + (HALF ? 8 : 0);
   static constexpr size_t PLANE_B = (size_t)PS * sizeof(float2);
   static constexpr size_t smem() {
-    return WPC * PLANE_B + WPC * (G / 32) * 3 * sizeof(double) + N * sizeof(float2) +
+    return WPC * PLANE_B + WPC * (G / 32) * NPART * sizeof(double) + N * sizeof(float2) +
            WPC * (G / 32) * 2 * KMAX * sizeof(uint32_t) +
            WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int)) + 3 * N * sizeof(int) + 64;
   }
@@ -690,16 +693,17 @@ template <int N, int W> struct CorrCfg {
   static_assert(N * LDR <= 2 * N * LD, "real plane must fit in the complex plane");
 };
 
-template <int N, int W>
-__global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correlate_kernel(const CorrArgs a) {
-  using C = CorrCfg<N, W>;
+template <int N, int W, bool SRCH>
+__global__ void __launch_bounds__(CorrCfg<N, W, SRCH>::NT, CorrCfg<N, W, SRCH>::MINB)
+    correlate_kernel(const CorrArgs a) {
+  using C = CorrCfg<N, W, SRCH>;
   constexpr int WPC = C::WPC, NT = C::NT, LD = C::LD, LDR = C::LDR, N1 = C::N1, N2 = C::N2, IPT = C::IPT;
   constexpr int G = C::G, EPT = C::EPT, NC = C::NC, H = N / 2;
   constexpr int PS = C::PS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* planes = reinterpret_cast<float2*>(smem_raw);
-  double* s_part = reinterpret_cast<double*>(smem_raw + WPC * C::PLANE_B);  // 3 per warp: sum A, sum B, count
-  float2* tw = reinterpret_cast<float2*>(s_part + WPC * (G / 32) * 3);
+  double* s_part = reinterpret_cast<double*>(smem_raw + WPC * C::PLANE_B);  // NPART per warp
+  float2* tw = reinterpret_cast<float2*>(s_part + WPC * (G / 32) * C::NPART);
   uint32_t* red = reinterpret_cast<uint32_t*>(tw + N);
   float* s_vals = reinterpret_cast<float*>(red + WPC * (G / 32) * 2 * KMAX);
   int* s_locs = reinterpret_cast<int*>(s_vals + WPC * KMAX);
@@ -733,7 +737,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
   const int bar = WPC == 1 ? 0 : w + 1;
   float2* P = planes + w * PS;
   float* Rw = reinterpret_cast<float*>(P);  // real plane, overlays the complex one after stage 8
-  double* part = s_part + w * (G / 32) * 3;
+  double* part = s_part + w * (G / 32) * C::NPART;
   const float scale = 1.0f / (float)(N * N);
   // fftshifted rows / columns that can hold a nonzero correlation value (the
   // support of the overlap gain; the whole plane without padding)
@@ -784,7 +788,80 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
     //      mean is the exact sum over n rounded once, where the reference
     //      folds in Float32 left to right; the two differ by a few ulp.
     bool bad;
-    {
+    if constexpr (SRCH) {
+      // enlarged search area (load_windows!, src/correlators.jl:229-262):
+      // the W x W frame-B area starts (W - win) / 2 before the window on
+      // both axes; frame A enters only inside the centred window, apodized
+      // and less its own mean, frame B everywhere, less its mean, without
+      // apodization; a masked pixel is zero in both and leaves both means
+      const int wa = a.win, oa = (W - wa) / 2;
+      const int64_t r0 = rs - oa, c0 = cs - oa;
+      float2 z[EPT];
+      bool mk[EPT];
+      double sa = 0.0, sb = 0.0, na = 0.0, nb = 0.0;
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int e = gt + i * G;
+        z[i] = make_float2(0.f, 0.f);
+        mk[i] = true;
+        if (e < W * W) {
+          const int p = e % W, q = e / W;
+          const bool ina = (unsigned)(p - oa) < (unsigned)wa && (unsigned)(q - oa) < (unsigned)wa;
+          const int64_t off = (r0 + p) + (c0 + q) * ld;
+          z[i] = make_float2(ina ? __ldg(A + off) : 0.f, __ldg(B + off));
+          mk[i] = M ? __ldg(M + off) != 0 : false;
+          if (!mk[i]) {
+            sb += (double)z[i].y;
+            nb += 1.0;
+            if (ina) {
+              sa += (double)z[i].x;
+              na += 1.0;
+            }
+          }
+        }
+      }
+      const unsigned gm = grp_mask(G);
+#pragma unroll
+      for (int o = (G < 32 ? G : 32) / 2; o > 0; o >>= 1) {
+        sa += __shfl_xor_sync(gm, sa, o);
+        sb += __shfl_xor_sync(gm, sb, o);
+        na += __shfl_xor_sync(gm, na, o);
+        nb += __shfl_xor_sync(gm, nb, o);
+      }
+      double ta = sa, tb = sb, tna = na, tnb = nb;
+      if (G > 32) {
+        if (lane == 0) {
+          part[4 * gw] = sa;
+          part[4 * gw + 1] = sb;
+          part[4 * gw + 2] = na;
+          part[4 * gw + 3] = nb;
+        }
+        grp_sync(bar, G);
+        ta = tb = tna = tnb = 0.0;
+        for (int k = 0; k < G / 32; ++k) {
+          ta += part[4 * k];
+          tb += part[4 * k + 1];
+          tna += part[4 * k + 2];
+          tnb += part[4 * k + 3];
+        }
+      }
+      const float ma = tna > 0 ? (float)(ta / tna) : 0.f, mb = tnb > 0 ? (float)(tb / tnb) : 0.f;
+      bad = !(isfinite(ta) && isfinite(tb));
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int e = gt + i * G;
+        if (e < W * W) {
+          const int p = e % W, q = e / W;
+          const bool ina = (unsigned)(p - oa) < (unsigned)wa && (unsigned)(q - oa) < (unsigned)wa;
+          float2 v = make_float2(0.f, 0.f);
+          if (!(mk[i] || bad)) {
+            v.y = z[i].y - mb;
+            if (ina) v.x = __ldg(a.apod + (p - oa) + (q - oa) * wa) * (z[i].x - ma);
+          }
+          P[q * LD + p] = v;
+        }
+      }
+    } else {
       float2 z[EPT];
       bool mk[EPT];
       double sa = 0.0, sb = 0.0, cnt = 0.0;
@@ -1079,6 +1156,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W>::NT, CorrCfg<N, W>::MINB) correl
               r0 *= __ldg(a.gain + qs * N + ps0);
               r1 *= hasb ? __ldg(a.gain + qs * N + ps1) : 0.f;
             }
+            if (SRCH && (qs < blo || qs > bhi)) r0 = r1 = 0.f;  // lags outside the search range
             rv[i][0][n1] = r0;
             rv[i][1][n1] = r1;
           }
@@ -1197,29 +1275,29 @@ __global__ void __launch_bounds__(128) peak_epilogue_kernel(const CorrArgs a, in
 size_t correlate_record_words(int npeaks) { return (size_t)rec_words(npeaks > 2 ? npeaks : 2); }
 
 // ---------------------------------------------------------------------------
-template <int N, int W> static cudaError_t launch_nw(const CorrArgs& a, cudaStream_t s, int num_sms) {
-  using C = CorrCfg<N, W>;
+template <int N, int W, bool SRCH> static cudaError_t launch_nw(const CorrArgs& a, cudaStream_t s, int num_sms) {
+  using C = CorrCfg<N, W, SRCH>;
   const size_t sm = C::smem();
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(correlate_kernel<N, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = cudaFuncSetAttribute(correlate_kernel<N, W, SRCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     // the planes live in shared memory: ask for the largest carveout so the
     // register budget, not the L1 split, sets the CTAs per SM
-    e = cudaFuncSetAttribute(correlate_kernel<N, W>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    e = cudaFuncSetAttribute(correlate_kernel<N, W, SRCH>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, correlate_kernel<N, W>, C::NT, sm);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, correlate_kernel<N, W, SRCH>, C::NT, sm);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   const int64_t units = (a.njobs + C::WPC - 1) / C::WPC;
   int64_t grid = (int64_t)per_sm * num_sms;
   if (grid > units) grid = units;
   if (grid < 1) grid = 1;
-  correlate_kernel<N, W><<<(unsigned)grid, C::NT, sm, s>>>(a);
+  correlate_kernel<N, W, SRCH><<<(unsigned)grid, C::NT, sm, s>>>(a);
   if (a.rec && a.finder == 0 && !a.accumulate) {
     int64_t eb = (a.njobs + 127) / 128;
     if (eb > (int64_t)num_sms * 16) eb = (int64_t)num_sms * 16;
@@ -1248,7 +1326,9 @@ size_t correlate_smem_bytes(int N, int W) {
 
 cudaError_t launch_correlate(const CorrArgs& a, int N, int W, cudaStream_t s, int num_sms) {
   if (a.njobs <= 0) return cudaSuccess;
-#define X(n, w) if (N == n && W == w) return launch_nw<n, w>(a, s, num_sms);
+#define X(n, w)                                                                                       \
+  if (N == n && W == w)                                                                              \
+    return a.win > 0 && a.win < w ? launch_nw<n, w, true>(a, s, num_sms) : launch_nw<n, w, false>(a, s, num_sms);
   HH_CORR_CASES(X)
 #undef X
   return cudaErrorInvalidValue;

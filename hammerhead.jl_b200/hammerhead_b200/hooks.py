@@ -81,7 +81,7 @@ class DeviceSession:
     def correlation_planes(self, params: PIVParameters, jobs):
         jobs = np.ascontiguousarray(jobs, np.int32)
         nj = jobs.shape[0]
-        n = 2 * params.window_size[0] if params.padding else params.window_size[0]
+        n = 2 * params.search_area_size[0] if params.padding else params.search_area_size[0]
         planes = np.empty((nj, n * n), np.float32)
         d = params.to_desc()
         _lib.check(_lib.lib().hh_correlation_planes(self.ws.ctx, ctypes.byref(d), _lib.i32ptr(jobs), nj,

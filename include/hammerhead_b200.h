@@ -108,7 +108,8 @@ const char* hh_last_error(const hh_ctx* ctx);
 hh_status hh_pass_validate(const hh_pass_desc* p);
 
 /* Reject options the device path does not implement, before any work:
- * replaces _check_backend_params / _ka_scope_check (src/ka_backend.jl:13-29). */
+ * replaces _check_backend_params / _ka_scope_check (src/ka_backend.jl:13-29),
+ * except that enlarged (square) search areas are accepted. */
 hh_status hh_check_backend_params(const hh_pass_desc* passes, int32_t npasses);
 
 /* Interrogation grid of one pass: replaces pass_grid (src/pipeline.jl:529-555).

@@ -277,13 +277,27 @@ def fft2(z, inverse=False, dtype=np.float64):
 
 
 def correlation_plane(subA, subB, params, dtype=np.float32):
+    """correlation_plane! (src/correlators.jl:326-341) of the frame-A window
+    subA and the frame-B search area subB (the window itself unless
+    search_area_size is larger)."""
     T, ct, suf = _T(dtype)
-    A = np.asfortranarray(subA, T)
     B = np.asfortranarray(subB, T)
+    if subA.shape == subB.shape:
+        A = np.asfortranarray(subA, T)
+        pa = _p(A, ct)
+    else:
+        # the C restatement reads both frames with one leading dimension:
+        # place the window at its offset inside a search-area-sized array
+        sr, sc = B.shape
+        wr, wc = subA.shape
+        orr, oc = (sr - wr) // 2, (sc - wc) // 2
+        A = np.zeros((sr, sc), T, order="F")
+        A[orr:orr + wr, oc:oc + wc] = subA
+        pa = ctypes.cast(A.ctypes.data + (orr + oc * sr) * A.itemsize, ctypes.POINTER(ct))
     n = 2 * params.search_area_size[0] if params.padding else params.search_area_size[0]
     R = np.empty((n, n), T, order="F")
     d = to_pass(params)
-    _fn("correlation_plane", suf)(_p(A, ct), _p(B, ct), ctypes.c_int64(A.shape[0]), ctypes.byref(d), _p(R, ct))
+    _fn("correlation_plane", suf)(pa, _p(B, ct), ctypes.c_int64(B.shape[0]), ctypes.byref(d), _p(R, ct))
     return R
 
 

@@ -1,0 +1,166 @@
+"""Enlarged search areas on the device against the CPU restatement.
+
+The frame-B search area is larger than the frame-A window and centred on it
+(load_windows!, src/correlators.jl:229-262); only lags for which the window
+stays inside the search area are kept (restrict_search_lags!, :347-355), and
+the grid margins grow by half the difference (pass_grid, src/pipeline.jl:
+529-555). The reference's device backends reject these passes; the CPU path
+is the parity target, with the tolerances of the equal-area parity tests.
+"""
+import numpy as np
+import pytest
+
+from helpers import shear_pair
+
+pytestmark = pytest.mark.gpu
+
+TOL_PX = 1e-3
+
+SEARCH_CASES = [
+    dict(window_size=16, search_area_size=32, overlap=8),
+    dict(window_size=16, search_area_size=32, overlap=8, padding=True, apodization="gauss"),
+    # padded 8 px windows in 16 px areas run two windows per warp
+    dict(window_size=8, search_area_size=16, overlap=4, padding=True, n_peaks=3),
+    dict(window_size=32, search_area_size=48, overlap=16),
+    dict(window_size=32, search_area_size=64, overlap=16, correlation_method="phase"),
+    dict(window_size=16, search_area_size=48, overlap=8, peak_finder="exclusion", n_peaks=3),
+    dict(window_size=64, search_area_size=96, overlap=32, subpixel_method="gauss9"),
+    dict(window_size=32, search_area_size=64, overlap=16, padding=True),
+]
+
+
+@pytest.fixture(scope="module")
+def hooks():
+    from hammerhead_b200 import hooks
+
+    return hooks
+
+
+@pytest.fixture(scope="module")
+def far_pair(hb):
+    # 6.3 px right, 5.4 px up: beyond a quarter of a 16 px window, inside the
+    # lags a 32 px search area keeps
+    syn = hb.synthetic
+    return syn.particle_pair((256, 256), syn.uniform_flow(6.3, -5.4), seed=91)
+
+
+@pytest.mark.parametrize("kw", SEARCH_CASES, ids=lambda k: "-".join(f"{a}={b}" for a, b in k.items()))
+def test_search_planes_and_peaks(ws, orc, hb, hooks, far_pair, kw):
+    A, B = far_pair
+    p = hb.PIVParameters(**kw)
+    sess = hooks.DeviceSession(ws)
+    sess.stage_pair(A, B)
+    x, y, _, jobs = hb.pass_grid(A.shape, p)
+    jobs = jobs[:: max(1, len(jobs) // 60)]
+    planes = sess.correlation_planes(p, jobs)
+    out, locs, _ = sess.process_windows(p, jobs, want_locs=True)
+    w, s = p.window_size[0], p.search_area_size[0]
+    m = (s - w) // 2
+    n = planes.shape[1]
+    assert n == (2 * s if p.padding else s)
+    phase = p.correlation_method == "phase"
+    near_ties = 0
+    for q, (gi, gj, rs, cs) in enumerate(jobs):
+        sa = A[rs - 1:rs - 1 + w, cs - 1:cs - 1 + w]
+        sb = B[rs - 1 - m:rs - 1 + w + m, cs - 1 - m:cs - 1 + w + m]
+        R = orc.correlation_plane(sa, sb, p)
+        scale = np.abs(R).max()
+        if phase:
+            # the phase method weights every bin by the inverse of its
+            # magnitude, so round-off in small bins reaches the plane at full
+            # weight: over an unapodized 64 px search area the Float32 oracle
+            # itself strays up to 1.8e-3 of the peak from its Float64 form.
+            # The device must stay as close to the Float64 plane as that.
+            R64 = orc.correlation_plane(sa, sb, p, dtype=np.float64)
+            own = np.abs(R - R64).max()
+            assert np.abs(planes[q] - R64).max() <= max(2 * own, 2e-5 * scale)
+        else:
+            assert np.abs(planes[q] - R).max() <= 2e-5 * scale + 1e-12
+        c = n // 2
+        keep = np.zeros((n, n), bool)
+        keep[c - m:c + m + 1, c - m:c + m + 1] = True
+        assert not planes[q][~keep].any()                     # lags outside the search range are zero
+        ref, rl = orc.analyze_plane(R, p.n_peaks, p.peak_finder, p.subpixel_method)
+        f = int(ref[4])
+        if int(out[q, 4]) != f or not np.array_equal(locs[q, :2 * f], rl[:2 * f]):
+            vals = np.sort(R.ravel())[::-1]
+            assert abs(vals[0] - vals[1]) < (4e-3 if phase else 1e-4) * scale or f > 1, (q, out[q], ref)
+            near_ties += 1
+            continue
+        np.testing.assert_allclose(out[q, :2], ref[:2], atol=TOL_PX)
+        np.testing.assert_allclose(out[q, 3], ref[3], rtol=1e-3, atol=1e-6, equal_nan=True)
+    # phase planes carry round-off of 1e-3 of the peak, so more candidate
+    # peaks are tied within it
+    assert near_ties <= max(1, len(jobs) // (20 if phase else 50))
+
+
+def _compare(r, o, tol=TOL_PX, max_flag_diff=0):
+    assert np.array_equal(r.mask, o["mask"])
+    valid = ~(o["outliers"] | o["mask"]) & ~(r.outliers | r.mask)
+    assert np.abs(r.u - o["u"])[valid].max() <= tol and np.abs(r.v - o["v"])[valid].max() <= tol
+    assert int((r.outliers != o["outliers"]).sum()) <= max_flag_diff
+
+
+def test_search_run_piv_large_shift(hb, orc, ws, far_pair):
+    A, B = far_pair
+    p = hb.PIVParameters(window_size=16, search_area_size=32, overlap=8)
+    r = hb.run_piv(A, B, p, workspace=ws)
+    o = orc.run_piv(A, B, p)
+    assert r.u.shape == o["u"].shape
+    _compare(r, o)
+    ok = ~r.outliers
+    assert np.median(np.abs(r.u[ok] - 6.3)) < 0.1 and np.median(np.abs(r.v[ok] + 5.4)) < 0.1
+
+
+def test_search_multipass_mask_and_uncertainty(hb, orc, ws):
+    A, B = shear_pair(23)
+    mask = np.zeros(A.shape, bool)
+    mask[:40, 70:] = True
+    passes = [hb.PIVParameters(window_size=32, search_area_size=64, overlap=16, padding=True, apodization="gauss"),
+              hb.PIVParameters(window_size=16, search_area_size=32, overlap=8, padding=True, apodization="gauss",
+                               uncertainty=True, max_iterations=2)]
+    r = hb.run_piv(A, B, passes, mask=mask, workspace=ws)
+    o = orc.run_piv(A, B, passes, mask=mask)
+    _compare(r, o, max_flag_diff=1)
+    assert r.mask.any()
+    both = np.isfinite(r.uncertainty_u) & np.isfinite(o["uncertainty_u"])
+    assert both.any()
+    assert np.quantile(np.abs(r.uncertainty_u - o["uncertainty_u"])[both], 0.99) < 1e-3
+
+
+def test_search_batch_equals_single(hb, ws, far_pair):
+    A, B = far_pair
+    syn = hb.synthetic
+    C, D = syn.particle_pair((192, 224), syn.sine_shear_flow(3.0, 120.0), seed=5)
+    sched = hb.multipass_parameters([32, 16], search_area_size=32)
+    plain = [hb.PIVParameters(window_size=32, overlap=16)]
+    res = hb.run_piv_batch([(A, B), (C, D), (C, D)], [sched, sched, plain], workspace=ws)
+    for (a, b), sc, got in zip([(A, B), (C, D), (C, D)], [sched, sched, plain], res):
+        ref = hb.run_piv(a, b, sc, workspace=ws)
+        for k in ("u", "v", "peak_ratio", "correlation_moment"):
+            assert np.array_equal(getattr(got, k), getattr(ref, k), equal_nan=True), k
+        assert np.array_equal(got.outliers, ref.outliers)
+
+
+def test_search_ensemble(hb, orc, ws):
+    syn = hb.synthetic
+    flow = syn.uniform_flow(5.7, 4.9)
+    pairs = [syn.particle_pair((128, 160), flow, seed=300 + i, ppp=0.004, noise=0.04) for i in range(8)]
+    p = hb.PIVParameters(window_size=16, search_area_size=32, overlap=8)
+    e = hb.run_piv_ensemble(pairs, p, workspace=ws)
+    o = orc.run_ensemble(pairs, [p], nthreads=8)
+    both = ~(e.outliers | o["outliers"])
+    assert np.quantile(np.abs(e.u - o["u"])[both], 0.99) <= TOL_PX
+    assert np.quantile(np.abs(e.v - o["v"])[both], 0.99) <= TOL_PX
+    assert np.quantile(np.hypot(e.u - 5.7, e.v - 4.9)[both], 0.95) < 0.15
+
+
+def test_search_hook_bounds(ws, hb, hooks, far_pair):
+    A, B = far_pair
+    p = hb.PIVParameters(window_size=16, search_area_size=32, overlap=8)
+    sess = hooks.DeviceSession(ws)
+    sess.stage_pair(A, B)
+    with pytest.raises(hb.ArgumentError, match="outside the image"):
+        sess.correlation_planes(p, np.array([[1, 1, 1, 1]], np.int32))   # the search area starts 8 px before
+    x, y, _, jobs = hb.pass_grid(A.shape, p)
+    assert jobs[0][2] == 9 and jobs[0][3] == 9                            # 1-based origin after the margin

@@ -99,8 +99,10 @@ def test_effort_schedule(hb):
 def test_backend_scope_check(hb):
     ok = hb.multipass_parameters([64, 32, 16], padding=True, apodization="gauss", final=dict(uncertainty=True))
     hb.check_backend_params(ok)
+    hb.check_backend_params([hb.PIVParameters(window_size=16, search_area_size=48, overlap=8)])
     for kw, msg in [(dict(subpixel_method="gauss2d"), "gauss2d"),
-                    (dict(window_size=16, search_area_size=48, overlap=8), "search_area_size"),
+                    (dict(window_size=16, search_area_size=40, overlap=8), "search area 40"),
+                    (dict(window_size=16, search_area_size=(48, 32), overlap=8), "square search areas"),
                     (dict(keep_correlation_planes=True), "keep_correlation_planes"),
                     (dict(window_size=(32, 16), overlap=(8, 8)), "square"),
                     (dict(window_size=20, overlap=10), "no correlation kernel"),

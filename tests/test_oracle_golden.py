@@ -246,6 +246,22 @@ def test_extended_search_known_shift(orc, hb):
     assert np.median(r["u"]) == 10 and np.median(r["v"]) == 3
 
 
+def test_extended_search_plane(orc, hb):
+    # a single window of the known shift: the frame-A window sits at the
+    # centre of the frame-B search area, so the peak is at the centre plus
+    # the shift, and lags beyond (48 - 16) / 2 = 16 are zero
+    rng = np.random.default_rng(71)
+    A = rng.uniform(size=(128, 128))
+    B = np.zeros((128, 128))
+    B[3:, 10:] = A[:-3, :-10]
+    p = hb.PIVParameters(window_size=16, search_area_size=48, overlap=8)
+    rs, cs = 40, 50                                   # 0-based window origin
+    R = orc.correlation_plane(A[rs:rs + 16, cs:cs + 16], B[rs - 16:rs + 32, cs - 16:cs + 32], p, dtype=np.float64)
+    assert R.shape == (48, 48)
+    assert np.unravel_index(np.argmax(R), R.shape) == (24 + 3, 24 + 10)
+    assert R[:8].max() == 0 and R[41:].max() == 0 and R[:, :8].max() == 0 and R[:, 41:].max() == 0
+
+
 # --- end-to-end behaviour (test/runtests.jl:164-460) ---------------------------------
 
 def test_uniform_displacement(orc, hb):
