@@ -361,7 +361,9 @@ def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_thre
     page-locked memory (for example numpy views of pinned torch tensors,
     column-major) are copied directly; others go through page-locked
     staging buffers first. Needs a CUDA device visible to torch; masks are
-    not supported on this path (use run_piv_batch)."""
+    not supported on this path (use run_piv_batch). With a caller's
+    workspace, the device frames and prepared runners of a composition are
+    kept in it for the next call of the same composition."""
     import concurrent.futures as cf
 
     import torch
@@ -382,12 +384,19 @@ def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_thre
         spec.append((int(a.shape[0]), int(a.shape[1]), tdt))
     own = workspace is None
     ws = workspace if workspace is not None else PIVWorkspace()
-    copy_stream = torch.cuda.Stream()
-    # two sets of device frames (column-major: tensors (nc, nr) seen through .T)
-    dev = [[(torch.empty((nc, nr), dtype=t, device="cuda"), torch.empty((nc, nr), dtype=t, device="cuda"))
-            for nr, nc, t in spec] for _ in range(2)]
-    stage_host = {}  # page-locked staging for frames that are not page-locked already
-    events = [torch.cuda.Event(), torch.cuda.Event()]
+    scheds, index = _schedules(passes, n)
+    key = (tuple(spec), tuple(index), b"".join(bytes(q.to_desc()) for sc in scheds for q in sc),
+           bool(predictor_smoothing), float(mask_threshold), u16)
+    cache = None if own else ws.__dict__.setdefault("_stream_sessions", {})
+    sess = None if cache is None else cache.get(key)
+    if sess is None:
+        sess = dict(copy_stream=torch.cuda.Stream(),
+                    # two sets of device frames (column-major: tensors (nc, nr) seen through .T)
+                    dev=[[(torch.empty((nc, nr), dtype=t, device="cuda"), torch.empty((nc, nr), dtype=t, device="cuda"))
+                          for nr, nc, t in spec] for _ in range(2)],
+                    stage_host={},  # page-locked staging for frames that are not page-locked already
+                    events=[torch.cuda.Event(), torch.cuda.Event()], runners=None)
+    copy_stream, dev, stage_host, events = sess["copy_stream"], sess["dev"], sess["stage_host"], sess["events"]
 
     def host_tensor(x, j, which, slot):
         nr, nc, t = spec[j]
@@ -417,10 +426,9 @@ def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_thre
             events[slot].record(copy_stream)
         return srcs  # kept alive until the copies are done
 
-    runners = [BatchRunner([(a.T, b.T) for a, b in dev[s]], passes, predictor_smoothing=predictor_smoothing,
-                           mask_threshold=mask_threshold, workspace=ws, u16=u16) for s in range(2)]
     out = []
     conv = [None, None]  # result conversion of the batch last analysed by each runner
+    runners = sess["runners"]
 
     def collect(k, slot):
         res = runners[slot].results(copy=True)
@@ -431,6 +439,13 @@ def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_thre
     try:
         with cf.ThreadPoolExecutor(max_workers=1) as pool, cf.ThreadPoolExecutor(max_workers=1) as post:
             fut = pool.submit(stage, first, 0)
+            if runners is None:  # prepared while the first batch is copied in
+                runners = [BatchRunner([(a.T, b.T) for a, b in dev[s]], passes,
+                                       predictor_smoothing=predictor_smoothing, mask_threshold=mask_threshold,
+                                       workspace=ws, u16=u16) for s in range(2)]
+                if cache is not None:
+                    sess["runners"] = runners
+                    cache[key] = sess
             k = 0
             while fut is not None:
                 slot = k % 2
@@ -455,9 +470,9 @@ def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_thre
                     out.append(conv[j % 2].result())
                     conv[j % 2] = None
     finally:
-        for r in runners:
-            r.close()
         if own:
+            for r in runners or ():
+                r.close()
             ws.close()
     return out
 

@@ -87,6 +87,7 @@ class PIVWorkspace:
         return _lib.lib().hh_ctx_stream(self.ctx)
 
     def close(self):
+        self.__dict__.pop("_stream_sessions", None)  # device frames and runners of run_piv_batch_stream
         if getattr(self, "_ctx", None) is not None:
             _lib.lib().hh_ctx_destroy(self._ctx)
             self._ctx = None

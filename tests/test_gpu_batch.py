@@ -255,3 +255,23 @@ def test_batch_stream_uint16(hb, ws):
     for k in range(2):
         for a, b in zip(out[k], hb.run_piv_batch(batches[k], [s1, s2], workspace=ws)):
             _same(a, b)
+
+
+def test_batch_stream_session_reused(hb, ws):
+    # a second stream of the same composition on the same workspace reuses
+    # the first call's device frames and prepared runners, with the same
+    # results; another composition gets its own session
+    s1, s2 = _schedules(hb)
+    sched = [s1, s2, s2, s1]
+    batches = [_mixed(hb, n=4, seed=700 + 10 * k)[0] for k in range(2)]
+    ws.__dict__.pop("_stream_sessions", None)
+    a = hb.run_piv_batch_stream(batches, sched, workspace=ws)
+    assert len(ws._stream_sessions) == 1
+    runners = next(iter(ws._stream_sessions.values()))["runners"]
+    b = hb.run_piv_batch_stream(batches[::-1], sched, workspace=ws)
+    assert next(iter(ws._stream_sessions.values()))["runners"] is runners
+    for k in range(2):
+        for x, y in zip(a[k], b[1 - k]):
+            _same(x, y)
+    hb.run_piv_batch_stream([batches[0][:3]], sched[:3], workspace=ws)
+    assert len(ws._stream_sessions) == 2
