@@ -5,7 +5,7 @@ sums, :182-183) are reduced across the processes before the analysis.
 One GPU only: the two-process case runs both ranks on cuda:0 over a gloo
 process group (gloo reduces CUDA tensors through host memory), so neither
 rank's kernels wait on the other's; the NCCL path differs only in the
-transport. Sums over processes follow another order than the single-process
+transport, which a group of one rank exercises on the library stream. Sums over processes follow another order than the single-process
 pair order, so the fields agree within float rounding, not bit for bit.
 """
 import os
@@ -156,3 +156,43 @@ def test_two_processes_match_one(hb, ws):
     for k, v in got[0].items():
         setattr(r0, k, v)
     _close(r0, whole)
+
+
+def _nccl_rank(port, q):
+    sys.path.insert(0, os.path.join(ROOT, "hammerhead.jl_b200"))
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import hammerhead_b200 as hb
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", 0))
+    try:
+        pairs = _pairs(hb, 4)
+        passes = hb.multipass_parameters([32, 16], padding=True, uncertainty=True)
+        e = hb.run_piv_ensemble(pairs, passes, process_group=True)
+        p = hb.run_piv_ensemble(pairs, passes)
+        q.put({k: bool(np.array_equal(getattr(e, k), getattr(p, k), equal_nan=True)) for k in FIELDS})
+    except BaseException as ex:  # noqa: BLE001 - reported to the parent
+        q.put(repr(ex))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_nccl_group_of_one(hb):
+    # the NCCL transport on the library stream: a group of one rank leaves
+    # every sum as it is, so the result is the plain ensemble's bit for bit
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_nccl_rank, args=(_free_port(), q))
+    p.start()
+    got = q.get(timeout=600)
+    p.join(timeout=60)
+    assert p.exitcode == 0
+    assert isinstance(got, dict) and all(got.values()), got
