@@ -447,24 +447,33 @@ def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_thre
                     sess["runners"] = runners
                     cache[key] = sess
             k = 0
+            pend = None  # the batch analysed last, not yet handed to the post thread
             while fut is not None:
                 slot = k % 2
                 fut.result()
-                try:
-                    nxt = next(it)
-                except StopIteration:
-                    nxt = None
-                # batch k+1 streams into the other set while batch k is analysed
-                # (that set's previous batch, k-1, finished before this point)
-                fut = pool.submit(stage, nxt, 1 - slot) if nxt is not None else None
                 events[slot].synchronize()
                 if conv[slot] is not None:  # this runner's buffers still hold batch k-2
                     out.append(conv[slot].result())
                     conv[slot] = None
+                try:
+                    nxt = next(it)
+                except StopIteration:
+                    nxt = None
+                # batch k+1 streams into the other set while batch k is
+                # analysed (that set's previous batch, k-1, finished before
+                # this point), and the results of batch k-1 become PIVResults.
+                # Both are handed over just before the library call, which
+                # releases the interpreter lock: the helper threads then do
+                # their Python work while the device runs, instead of holding
+                # the lock while this thread prepares the call
+                fut = pool.submit(stage, nxt, 1 - slot) if nxt is not None else None
+                if pend is not None:
+                    conv[pend[1]] = post.submit(collect, *pend)
                 runners[slot].run()
-                # the results of batch k become PIVResults while batch k+1 runs
-                conv[slot] = post.submit(collect, k, slot)
+                pend = (k, slot)
                 k += 1
+            if pend is not None:
+                conv[pend[1]] = post.submit(collect, *pend)
             for j in range(k - 2, k):
                 if j >= 0 and conv[j % 2] is not None:
                     out.append(conv[j % 2].result())
