@@ -170,7 +170,15 @@ class BatchRunner:
         return self
 
     def results(self, copy=True):
-        """PIVResult per pair (views into the runner's buffers unless copy)."""
+        """PIVResult per pair (views into the runner's buffers unless copy;
+        with copy, views into one private copy of each buffer)."""
+        R = int(self.offsets[-1])
+        if copy:
+            fields = {k: self.out[k][:R].copy() for k in _FIELDS}
+            outl, gmask = self.outliers[:R].astype(bool), self.gmask[:R].astype(bool)
+        else:
+            fields = self.out
+            outl, gmask = self.outliers, self.gmask
         res = []
         for p in range(self.npairs):
             a, b = int(self.offsets[p]), int(self.offsets[p + 1])
@@ -184,13 +192,13 @@ class BatchRunner:
             x, y = self._grids[key]
 
             def f(arr):
-                v = arr[a:b].reshape((ny, nx), order="F")
-                return v.copy(order="F") if copy else v
+                return arr[a:b].reshape((ny, nx), order="F")
 
             sweeps = np.zeros(len(sched), np.int32)
             sweeps[-1] = self.sweeps[p]
-            res.append(PIVResult(x.copy(), y.copy(), *[f(self.out[k]) for k in _FIELDS], f(self.outliers).astype(bool),
-                                 f(self.gmask).astype(bool), sched[-1], None, None, None, sweeps))
+            res.append(PIVResult(x.copy(), y.copy(), *[f(fields[k]) for k in _FIELDS],
+                                 f(outl) if copy else f(outl).astype(bool), f(gmask) if copy else f(gmask).astype(bool),
+                                 sched[-1], None, None, None, sweeps))
         return res
 
     def close(self):
