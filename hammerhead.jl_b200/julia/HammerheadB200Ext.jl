@@ -154,6 +154,93 @@ function run_piv_b200(imgA::AbstractMatrix{<:Real}, imgB::AbstractMatrix{<:Real}
     return PIVResult(x, y, u, v, ratio, moment, su, sv, BitMatrix(outl .!= 0), BitMatrix(gm .!= 0), final)
 end
 
+# ---- ensemble (sum-of-correlation) PIV: hh_run_ensemble ------------------
+# hh_batch_pair (include/hammerhead_b200.h), field for field.
+struct BatchPair
+    A::Ptr{Float32}
+    B::Ptr{Float32}
+    mask::Ptr{UInt8}
+    nr::Int64
+    nc::Int64
+    schedule::Int32
+    format::Int32   # 0: Float32 frames
+end
+
+# The reducer of a multi-process ensemble, called by the library once per pass
+# with the device plane sums and FP64 uncertainty sums of this process's
+# pairs; it must leave their sums over all processes in place (for example an
+# MPI.Allreduce! on CuArrays wrapping the pointers), ordered on `stream`.
+const _REDUCER = Ref{Any}(nothing)
+
+function _reduce_trampoline(user::Ptr{Cvoid}, pass::Int32, planes::Ptr{Float32}, nplanes::Int64,
+                            stats::Ptr{Float64}, nstats::Int64, stream::Ptr{Cvoid})::Int32
+    try
+        _REDUCER[](Int(pass), planes, Int(nplanes), stats, Int(nstats), stream)
+        return Int32(0)
+    catch err
+        @error "ensemble reducer failed" exception = err
+        return Int32(1)
+    end
+end
+
+# run_piv_ensemble(pairs, passes; backend = :b200): Float32 frames of one size;
+# `reducer(pass, planes, nplanes, stats, nstats, stream)` when the pairs of the
+# ensemble are split over processes (all processes pass the same image size,
+# passes, mask and options).
+function run_piv_ensemble_b200(pairs::AbstractVector{<:Tuple{AbstractMatrix{<:Real},AbstractMatrix{<:Real}}},
+                               passes::AbstractVector{PIVParameters};
+                               predictor_smoothing::Bool = true,
+                               mask::Union{Nothing,AbstractMatrix{Bool}} = nothing, mask_threshold::Real = 0.5,
+                               reducer::Union{Nothing,Function} = nothing, ctx::Context = Context())
+    _check_backend_params(_B200Backend(), passes)
+    isempty(pairs) && throw(ArgumentError("pairs must not be empty"))
+    frames = [(Matrix{Float32}(a), Matrix{Float32}(b)) for (a, b) in pairs]
+    nr, nc = size(frames[1][1])
+    for (a, b) in frames
+        size(a) == size(b) == (nr, nc) ||
+            throw(DimensionMismatch("all pairs must share the image size ($nr, $nc), got $(size(a)) and $(size(b))"))
+    end
+    M = mask === nothing ? C_NULL : Matrix{UInt8}(mask)
+    final = last(passes)
+    d = [pass_desc(p) for p in passes]
+    ny, nx, nj = Ref{Int32}(0), Ref{Int32}(0), Ref{Int64}(0)
+    check(ccall((:hh_pass_grid, LIB), Int32,
+                (Int64, Int64, Ref{PassDesc}, Ptr{UInt8}, Float64, Ref{Int32}, Ref{Int32}, Ptr{Float32},
+                 Ptr{Float32}, Ptr{UInt8}, Ptr{Int32}, Ref{Int64}),
+                nr, nc, pass_desc(final), C_NULL, mask_threshold, ny, nx, C_NULL, C_NULL, C_NULL, C_NULL, nj))
+    gy, gx = Int(ny[]), Int(nx[])
+    x = Vector{Float32}(undef, gx); y = Vector{Float32}(undef, gy)
+    f() = Matrix{Float32}(undef, gy, gx)
+    u, v, ratio, moment, su, sv = f(), f(), f(), f(), f(), f()
+    outl = Matrix{UInt8}(undef, gy, gx); gm = Matrix{UInt8}(undef, gy, gx)
+    cb = @cfunction(_reduce_trampoline, Int32,
+                    (Ptr{Cvoid}, Int32, Ptr{Float32}, Int64, Ptr{Float64}, Int64, Ptr{Cvoid}))
+    GC.@preserve frames M x y u v ratio moment su sv outl gm begin
+        bp = [BatchPair(pointer(a), pointer(b), C_NULL, nr, nc, 0, 0) for (a, b) in frames]
+        res = Ref(Result(0, 0, pointer(x), pointer(y), pointer(u), pointer(v), pointer(ratio), pointer(moment),
+                         pointer(su), pointer(sv), pointer(outl), pointer(gm)))
+        if reducer !== nothing
+            _REDUCER[] = reducer
+            check(ccall((:hh_set_ensemble_reducer, LIB), Int32, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}),
+                        ctx.ptr, cb, C_NULL), ctx.ptr)
+        end
+        try
+            check(ccall((:hh_run_ensemble, LIB), Int32,
+                        (Ptr{Cvoid}, Ptr{BatchPair}, Int32, Ptr{PassDesc}, Int32, Ptr{UInt8}, Float64, Int32, Int32,
+                         Ref{Result}),
+                        ctx.ptr, bp, length(bp), d, length(d), M, mask_threshold, predictor_smoothing, 0, res),
+                  ctx.ptr)
+        finally
+            if reducer !== nothing
+                ccall((:hh_set_ensemble_reducer, LIB), Int32, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}),
+                      ctx.ptr, C_NULL, C_NULL)
+                _REDUCER[] = nothing
+            end
+        end
+    end
+    return PIVResult(x, y, u, v, ratio, moment, su, sv, BitMatrix(outl .!= 0), BitMatrix(gm .!= 0), final)
+end
+
 # ---- differentiable correlation loss (hh_ncc_loss_grad) -------------------
 # A staged pair on a context; P is (gny, gnx, 2) Float32 (u, v) on nodes
 # y0 .+ ysp .* (0:gny-1), x0 .+ xsp .* (0:gnx-1).
