@@ -197,7 +197,7 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
       Wt += (nr * nc + 3) / 4 * 4;  // 16-byte aligned per pair: the deformation stores pixel quads
       Q += (nr + 2) * (nc + 2);
       WC += (nc + 31) / 32 * nseg_host(nr + 2);  // column tiles x segments
-      WR += (nr + 2) * nseg_host(nc + 2);
+      WR += (nr + 2 + 31) / 32 * nseg_host(nc + 2);  // 32-row groups x segments
     }
     roff[p] = R;
     const Grid& gf = P.grids[p].back();

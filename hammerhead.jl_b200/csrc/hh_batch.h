@@ -42,7 +42,7 @@ struct BPair {
   int64_t nr, nc;
   int64_t poff;   // warped-pixel storage offset (a multiple of 4)
   int64_t qoff;   // padded-pixel (coefficient) storage offset, compact over deforming pairs
-  int64_t wcol;   // prefilter work offsets (32-column tiles x segments, row segments)
+  int64_t wcol;   // prefilter work offsets (32-column tiles x segments, 32-row groups x segments)
   int64_t wrow;
   int64_t goff;   // cell storage offset
   int64_t aoff;   // alternatives storage offset (nalt planes of ny*nx cells)

@@ -326,30 +326,44 @@ __device__ __forceinline__ int64_t b_nseg(int64_t n) { return n >= 5 ? (n - 4 + 
 constexpr int BS_TILE = BS_WARM + BS_SEG;  // rows staged per column
 constexpr int BS_TLD = BS_TILE + 1;        // odd stride: conflict-free by lane and by row
 constexpr int BSC_WARPS = 4;
-constexpr size_t BSC_SMEM = (size_t)BSC_WARPS * 32 * BS_TLD * sizeof(float);
+// per warp: a tile (32 columns x 96 rows at stride 97, or 96 columns x 32
+// rows at stride 33) and the elimination factors of its 96 unknowns
+constexpr int BS_WTILE = 96 * 33 > 32 * BS_TLD ? 96 * 33 : 32 * BS_TLD;
+constexpr int BS_WSTRIDE = BS_WTILE + BS_TILE;
+constexpr size_t BSC_SMEM = (size_t)BSC_WARPS * BS_WSTRIDE * sizeof(float);
+
+// The factors f[0 .. cnt) into F: every lane of a sweep uses the same factor
+// at each step, and staging them keeps an L2 round trip out of the sweep's
+// dependent chain. The copies join the tile's asynchronous copies, and
+// stage_factors waits for all of them.
+__device__ __forceinline__ void bs_cp_async4(float* dst, const float* src);
+__device__ __forceinline__ void bs_cp_async_wait_all();
+__device__ __forceinline__ void stage_factors(float* F, const float* f, int cnt, int lane) {
+  for (int j = lane; j < cnt; j += 32) bs_cp_async4(F + j, f + j);
+  bs_cp_async_wait_all();
+}
 
 // Rows [0, cnt) (cnt <= 96) of `ncol` columns between global memory (column
 // c at g + c * gld) and a staged tile (column c at T + c * BS_TLD). The
-// lanes walk down the columns; eight columns per batch keep 24 loads of a
-// lane in flight instead of waiting on each column in turn.
+// lanes walk down the columns. Loads are asynchronous copies straight into
+// shared memory, all of the tile's issued before the first is waited for (in
+// stage_factors): one memory round trip per item instead of one per batch of
+// registers.
+__device__ __forceinline__ void bs_cp_async4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void bs_cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
 __device__ __forceinline__ void tile_load(float* T, const float* g, int64_t gld, int ncol, int cnt, int lane) {
-  for (int c0 = 0; c0 < ncol; c0 += 8) {
-    float v[8][3];
+  for (int c = 0; c < ncol; ++c)
 #pragma unroll
-    for (int u = 0; u < 8; ++u)
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const int c = c0 + u, r = lane + 32 * j;
-        v[u][j] = (c < ncol && r < cnt) ? __ldg(g + c * gld + r) : 0.f;
-      }
-#pragma unroll
-    for (int u = 0; u < 8; ++u)
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const int c = c0 + u, r = lane + 32 * j;
-        if (c < ncol && r < cnt) T[c * BS_TLD + r] = v[u][j];
-      }
-  }
+    for (int j = 0; j < 3; ++j) {
+      const int r = lane + 32 * j;
+      if (r < cnt) bs_cp_async4(T + c * BS_TLD + r, g + c * gld + r);
+    }
 }
 __device__ __forceinline__ void tile_store(const float* T, float* g, int64_t gld, int ncol, int cnt, int lane) {
   for (int c0 = 0; c0 < ncol; c0 += 8) {
@@ -376,7 +390,8 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
                                                                       int64_t witems, float* dbuf, int64_t qtot) {
   extern __shared__ float bsc_tile[];
   const int img = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float* T = bsc_tile + warp * 32 * BS_TLD;
+  float* T = bsc_tile + warp * BS_WSTRIDE;
+  float* F = T + BS_WTILE;
   for (int64_t t = (int64_t)blockIdx.x * BSC_WARPS + warp; t < witems; t += (int64_t)gridDim.x * BSC_WARPS) {
     const BPair& b = bp[bp_find<&BPair::wcol>(bp, npairs, t)];
     if (!b.deforms) continue;  // uniform across the warp
@@ -413,6 +428,7 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
       const int cnt = (int)(k1 - ks);
       // stage the right-hand sides: unknown k is padded element k + 2 = image row k + 1
       tile_load(T, im + ks + 1, nr, ncol, cnt, lane);
+      stage_factors(F, b.ivc + ks, cnt, lane);
       __syncwarp();
       if (mine) {
         const float* ic = im + lane * nr;
@@ -425,7 +441,7 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
           float rhs = x[k - ks];
           if (k == 0) rhs = FS(rhs, FM(sixth, c2));
           if (k == m - 1) rhs = FS(rhs, FM(sixth, cn1));
-          dv = k == 0 ? FM(rhs, __ldg(b.ivc)) : FM(FS(rhs, FM(sixth, dv)), __ldg(b.ivc + k));
+          dv = k == 0 ? FM(rhs, F[0]) : FM(FS(rhs, FM(sixth, dv)), F[k - ks]);
           x[k - ks] = dv;
         }
       }
@@ -437,6 +453,7 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
       const int64_t ke = min(m - 1, k1 - 1 + BS_WARM);
       const int cnt = (int)(ke - k0 + 1);
       tile_load(T, d + k0 + 2, n, ncol, cnt, lane);
+      stage_factors(F, b.cpc + k0, cnt, lane);
       __syncwarp();
       if (mine) {
         float* x = T + lane * BS_TLD;
@@ -444,7 +461,7 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
 #pragma unroll 4
         for (int64_t k = ke; k >= k0; --k) {
           const float dk = x[k - k0];
-          xv = k == ke ? dk : FS(dk, FM(__ldg(b.cpc + k), xv));
+          xv = k == ke ? dk : FS(dk, FM(F[k - k0], xv));
           x[k - k0] = xv;
           if (k == m - 1) xlast = xv;
         }
@@ -485,23 +502,95 @@ __global__ void b_pad_cols_kernel(const BPair* __restrict__ bp, int npairs) {
   }
 }
 
-// dim 2 (padded rows, consecutive threads on consecutive rows: coalesced)
+// dim 2: a warp takes 32 consecutive padded rows and one segment of their
+// unknowns. The segment's columns are staged in shared memory (each column's
+// 32 rows are one coalesced 128-byte copy, every column in flight at once),
+// the lanes sweep their rows there (row r of staged column j at
+// T[33 j + r]: conflict-free), and the results leave the same way. The
+// arithmetic is bs_fwd_item / bs_bwd_item's, step for step.
+__device__ __forceinline__ void row_tile_load(float* T, const float* g, int64_t gld, int nrow, int cnt, int lane) {
+  if (lane < nrow)
+    for (int j = 0; j < cnt; ++j) bs_cp_async4(T + j * 33 + lane, g + j * gld + lane);
+}
+__device__ __forceinline__ void row_tile_store(const float* T, float* g, int64_t gld, int nrow, int cnt, int lane) {
+  if (lane >= nrow) return;
+  for (int j = 0; j < cnt; ++j) g[j * gld + lane] = T[j * 33 + lane];
+}
+
 template <int PASS>
-__global__ void b_bspline_row_kernel(const BPair* __restrict__ bp, int npairs, int64_t wtot, float* dbuf, int64_t qtot) {
-  const int img = blockIdx.y;
-  B_STRIDE(t, wtot) {
+__global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_row_kernel(const BPair* __restrict__ bp, int npairs,
+                                                                      int64_t witems, float* dbuf, int64_t qtot) {
+  extern __shared__ float bsc_tile[];
+  const int img = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* T = bsc_tile + warp * BS_WSTRIDE;
+  float* F = T + BS_WTILE;
+  for (int64_t t = (int64_t)blockIdx.x * BSC_WARPS + warp; t < witems; t += (int64_t)gridDim.x * BSC_WARPS) {
     const BPair& b = bp[bp_find<&BPair::wrow>(bp, npairs, t)];
-    if (!b.deforms) continue;
-    const int64_t ld = b.nr + 2, ncols = b.nc + 2;
-    const int64_t n = ncols, nlines = ld;
-    const int64_t l = t - b.wrow;
-    if (l >= nlines * b_nseg(n)) continue;
-    float* coef = img ? b.coefB : b.coefA;
-    float* d = dbuf + (int64_t)img * qtot + b.qoff;
+    if (!b.deforms) continue;  // uniform across the warp
+    const int64_t ld = b.nr + 2, n = b.nc + 2, m = n - 4;
+    const int64_t nrg = (ld + 31) / 32, l = t - b.wrow;
+    if (l >= nrg * b_nseg(n)) continue;
+    const int64_t rg = l % nrg, seg = l / nrg, r0 = rg * 32;
+    const int nrow = (int)min((int64_t)32, ld - r0);
+    const bool mine = lane < nrow;
+    float* coef = (img ? b.coefB : b.coefA) + r0;                  // row r0 of the padded coefficients
+    float* d = dbuf + (int64_t)img * qtot + b.qoff + r0;
     if (PASS == 0) {
-      if (n - 4 >= 1) bs_fwd_item(coef, d, n, ld, 1, nlines, b.ivr, l);
+      if (m < 1) continue;
+      const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG), ks = max((int64_t)0, k0 - BS_WARM);
+      const int cnt = (int)(k1 - ks);
+      row_tile_load(T, coef + (ks + 2) * ld, ld, nrow, cnt, lane);  // unknown k is padded column k + 2
+      stage_factors(F, b.ivr + ks, cnt, lane);
+      __syncwarp();
+      if (mine) {
+        const float sixth = kSixth;
+        const float c2 = coef[ld + lane], cn1 = coef[(n - 2) * ld + lane];
+        float dv = 0.f;
+#pragma unroll 4
+        for (int64_t k = ks; k < k1; ++k) {
+          float* x = T + (k - ks) * 33 + lane;
+          float rhs = *x;
+          if (k == 0) rhs = FS(rhs, FM(sixth, c2));
+          if (k == m - 1) rhs = FS(rhs, FM(sixth, cn1));
+          dv = k == 0 ? FM(rhs, F[0]) : FM(FS(rhs, FM(sixth, dv)), F[k - ks]);
+          *x = dv;
+        }
+      }
+      __syncwarp();
+      row_tile_store(T + (k0 - ks) * 33, d + (k0 + 2) * ld, ld, nrow, (int)(k1 - k0), lane);
+      __syncwarp();  // the tile is restaged by the next item
     } else {
-      if (n >= 4) bs_bwd_item(coef, d, n, ld, 1, nlines, b.cpr, l);
+      if (n < 4) continue;
+      if (m < 1) {  // n == 4: c1 = b1, c2 = b2 only
+        if (mine) {
+          const float c1 = coef[ld + lane], c2 = coef[2 * ld + lane];
+          coef[lane] = FS(FM(2.0f, c1), c2);
+          coef[3 * ld + lane] = FS(FM(2.0f, c2), c1);
+        }
+        continue;
+      }
+      const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG), ke = min(m - 1, k1 - 1 + BS_WARM);
+      const int cnt = (int)(ke - k0 + 1);
+      row_tile_load(T, d + (k0 + 2) * ld, ld, nrow, cnt, lane);
+      stage_factors(F, b.cpr + k0, cnt, lane);
+      __syncwarp();
+      if (mine) {
+        float xv = 0.f, xlast = 0.f;
+#pragma unroll 4
+        for (int64_t k = ke; k >= k0; --k) {
+          float* x = T + (k - k0) * 33 + lane;
+          const float dk = *x;
+          xv = k == ke ? dk : FS(dk, FM(F[k - k0], xv));
+          *x = xv;
+          if (k == m - 1) xlast = xv;
+        }
+        // "Line" boundary columns from the copied columns 1 and n - 2
+        if (k0 == 0) coef[lane] = FS(FM(2.0f, coef[ld + lane]), xv);  // xv == x_0 here
+        if (k1 == m) coef[(n - 1) * ld + lane] = FS(FM(2.0f, coef[(n - 2) * ld + lane]), xlast);
+      }
+      __syncwarp();
+      row_tile_store(T, coef + (k0 + 2) * ld, ld, nrow, (int)(k1 - k0), lane);
+      __syncwarp();
     }
   }
 }
@@ -514,6 +603,10 @@ cudaError_t launch_b_prefilter(const BPair* bp, int npairs, int64_t qtot, int64_
     for (cudaError_t e : {cudaFuncSetAttribute(b_bspline_col_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)BSC_SMEM),
                           cudaFuncSetAttribute(b_bspline_col_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)BSC_SMEM),
+                          cudaFuncSetAttribute(b_bspline_row_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)BSC_SMEM),
+                          cudaFuncSetAttribute(b_bspline_row_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)BSC_SMEM)})
       if (e != cudaSuccess) return e;
     attr_set = true;
@@ -526,8 +619,10 @@ cudaError_t launch_b_prefilter(const BPair* bp, int npairs, int64_t qtot, int64_
   }
   b_pad_cols_kernel<<<dim3(npairs < 148 ? npairs : 148, 2), 128, 0, s>>>(bp, npairs);
   if (wrow_tot > 0) {
-    b_bspline_row_kernel<0><<<dim3(b_blocks(wrow_tot, 32), 2), 256, 0, s>>>(bp, npairs, wrow_tot, dbuf, qtot);
-    b_bspline_row_kernel<1><<<dim3(b_blocks(wrow_tot, 32), 2), 256, 0, s>>>(bp, npairs, wrow_tot, dbuf, qtot);
+    int64_t blocks = (wrow_tot + BSC_WARPS - 1) / BSC_WARPS;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    b_bspline_row_kernel<0><<<dim3((unsigned)blocks, 2), 32 * BSC_WARPS, BSC_SMEM, s>>>(bp, npairs, wrow_tot, dbuf, qtot);
+    b_bspline_row_kernel<1><<<dim3((unsigned)blocks, 2), 32 * BSC_WARPS, BSC_SMEM, s>>>(bp, npairs, wrow_tot, dbuf, qtot);
   }
   return cudaGetLastError();
 }
