@@ -370,10 +370,10 @@ inline hh_status prefilter_pair(hh_ctx* ctx, const float* dA, const float* dB, i
   float *cpc, *ivc, *cpr, *ivr, *bsd;
   HH_TRY(bs_factors(ctx, nr + 2, &cpc, &ivc));
   HH_TRY(bs_factors(ctx, nc + 2, &cpr, &ivr));
-  HH_TRY(buf(ctx, "bs_dbuf", (size_t)(nr + 2) * (nc + 2), &bsd));
+  HH_TRY(buf(ctx, "bs_dbuf", (size_t)2 * (nr + 2) * (nc + 2), &bsd));
   const double P = (double)nr * nc;
-  HH_K(HH_K_PREFILTER, 5, 12 * P, 8 * P, (int64_t)P, hh::launch_prefilter(dA, nr, nc, cA, bsd, cpc, ivc, cpr, ivr, ctx->stream));
-  HH_K(HH_K_PREFILTER, 5, 12 * P, 8 * P, (int64_t)P, hh::launch_prefilter(dB, nr, nc, cB, bsd, cpc, ivc, cpr, ivr, ctx->stream));
+  HH_K(HH_K_PREFILTER, 4, 24 * P, 16 * P, (int64_t)(2 * P),
+       hh::launch_prefilter_pair(dA, dB, nr, nc, cA, cB, bsd, cpc, ivc, cpr, ivr, ctx->stream));
   return HH_OK;
 }
 

@@ -83,8 +83,11 @@ cudaError_t launch_analyze_planes(const AnalyzeArgs& a, cudaStream_t s);
 
 // --- deformation -----------------------------------------------------------
 cudaError_t launch_bspline_factors(int64_t n, float* cp, float* inv, cudaStream_t s);
-cudaError_t launch_prefilter(const float* img, int64_t nr, int64_t nc, float* coef, float* dbuf, const float* cpc,
-                             const float* ivc, const float* cpr, const float* ivr, cudaStream_t s);
+// Cubic B-spline coefficients ((nr + 2) x (nc + 2), padded) of both frames of
+// a pair; dbuf: 2 (nr + 2) (nc + 2) floats for the forward sweeps.
+cudaError_t launch_prefilter_pair(const float* imgA, const float* imgB, int64_t nr, int64_t nc, float* coefA,
+                                  float* coefB, float* dbuf, const float* cpc, const float* ivc, const float* cpr,
+                                  const float* ivr, cudaStream_t s);
 struct PredGrid {
   int32_t gny, gnx;
   float y0, ysp, x0, xsp;

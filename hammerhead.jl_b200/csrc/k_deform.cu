@@ -68,120 +68,19 @@ __global__ void bspline_factors_kernel(int64_t n, float* cp, float* inv) {
   }
 }
 
-// Copy the image into the interior of the zeroed padded array.
-__global__ void pad_copy_kernel(const float* img, int64_t nr, int64_t nc, float* coef) {
-  const int64_t ld = nr + 2, total = ld * (nc + 2);
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = k % ld, j = k / ld;
-    coef[k] = (i >= 1 && i <= nr && j >= 1 && j <= nc) ? img[(i - 1) + (j - 1) * nr] : 0.f;
-  }
-}
-
 // Both Thomas sweeps are contractions (|cp_k| -> 0.268), so each line is cut
 // into independent segments of BS_SEG unknowns whose sweeps start BS_WARM
 // unknowns early from a zero state; the neglected term is below
 // 0.268^32 ~ 5e-19 of the value. The CPU restatement uses the same
-// segmentation, so the coefficients agree bit for bit. One thread per
-// (line, segment): ~65k-way parallel on a 2048x2048 image.
+// segmentation, so the coefficients agree bit for bit. The forward sweep is
+// d_k = (rhs_k - d_{k-1}/6) inv_k (unknown k at line element k + 2; rhs_0 and
+// rhs_{m-1} carry the known c1 and c_{n-2}), the backward sweep
+// x_k = d_k - cp_k x_{k+1}, followed by the "Line" boundary coefficients
+// c0 = 2c1 - c2 and c_{n-1} = 2c_{n-2} - c_{n-3}.
 constexpr int BS_SEG = 64, BS_WARM = 32;
-
-// forward sweep: d_k = (rhs_k - d_{k-1}/6) * inv_k into dbuf. Unknown k lives
-// at line element k + 2; rhs_0 and rhs_{m-1} carry the known c1, c_{n-2}.
-__device__ __forceinline__ void bs_fwd_item(const float* __restrict__ in, float* __restrict__ dbuf, int64_t n,
-                                            int64_t es, int64_t ls, int64_t nlines, const float* __restrict__ inv,
-                                            int64_t t) {
-  const int64_t m = n - 4;
-  const float sixth = kSixth;
-  const int64_t line = t % nlines, seg = t / nlines;
-  const float* x = in + line * ls;
-  float* d = dbuf + line * ls;
-  const float c2 = x[es], cn1 = x[(n - 2) * es];
-  const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG), ks = max((int64_t)0, k0 - BS_WARM);
-  float dv = 0.f;
-  for (int64_t k = ks; k < k1; ++k) {
-    float rhs = x[(k + 2) * es];
-    if (k == 0) rhs = FS(rhs, FM(sixth, c2));
-    if (k == m - 1) rhs = FS(rhs, FM(sixth, cn1));
-    dv = k == 0 ? FM(rhs, inv[0]) : FM(FS(rhs, FM(sixth, dv)), inv[k]);
-    if (k >= k0) d[(k + 2) * es] = dv;
-  }
-}
-
-__global__ void bspline_fwd_kernel(const float* __restrict__ in, float* __restrict__ dbuf, int64_t n, int64_t es,
-                                   int64_t ls, int64_t nlines, const float* __restrict__ inv) {
-  const int64_t m = n - 4;
-  if (m < 1) return;
-  const int64_t nseg = (m + BS_SEG - 1) / BS_SEG;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nlines * nseg;
-       t += (int64_t)gridDim.x * blockDim.x)
-    bs_fwd_item(in, dbuf, n, es, ls, nlines, inv, t);
-}
-
-// backward sweep x_k = d_k - cp_k x_{k+1} into coef, plus the "Line"
-// boundary coefficients c0 = 2c1 - c2 and c_{n-1} = 2c_{n-2} - c_{n-3}.
-__device__ __forceinline__ void bs_bwd_item(float* __restrict__ coef, const float* __restrict__ dbuf, int64_t n,
-                                            int64_t es, int64_t ls, int64_t nlines, const float* __restrict__ cp,
-                                            int64_t t) {
-  const int64_t m = n - 4;
-  const int64_t line = t % nlines, seg = t / nlines;
-  float* x = coef + line * ls;
-  if (m < 1) {  // n == 4: c1 = b1, c2 = b2 only
-    const float c1 = x[es], c2 = x[2 * es];
-    x[0] = FS(FM(2.0f, c1), c2);
-    x[3 * es] = FS(FM(2.0f, c2), c1);
-    return;
-  }
-  const float* d = dbuf + line * ls;
-  const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG), ke = min(m - 1, k1 - 1 + BS_WARM);
-  float xv = 0.f, xlast = 0.f;
-  for (int64_t k = ke; k >= k0; --k) {
-    const float dk = d[(k + 2) * es];
-    xv = k == ke ? dk : FS(dk, FM(cp[k], xv));
-    if (k < k1) x[(k + 2) * es] = xv;
-    if (k == m - 1) xlast = xv;
-  }
-  if (k0 == 0) x[0] = FS(FM(2.0f, x[es]), xv);  // xv == x_0 here
-  if (k1 == m) x[(n - 1) * es] = FS(FM(2.0f, x[(n - 2) * es]), xlast);
-}
-
-__global__ void bspline_bwd_kernel(float* __restrict__ coef, const float* __restrict__ dbuf, int64_t n, int64_t es,
-                                   int64_t ls, int64_t nlines, const float* __restrict__ cp) {
-  const int64_t m = n - 4;
-  if (n < 4) return;
-  const int64_t nseg = m < 1 ? 1 : (m + BS_SEG - 1) / BS_SEG;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nlines * nseg;
-       t += (int64_t)gridDim.x * blockDim.x)
-    bs_bwd_item(coef, dbuf, n, es, ls, nlines, cp, t);
-}
-
-static unsigned seg_blocks(int64_t work) {
-  int64_t b = (work + 255) / 256;
-  if (b > 148 * 32) b = 148 * 32;
-  return (unsigned)(b < 1 ? 1 : b);
-}
 
 cudaError_t launch_bspline_factors(int64_t n, float* cp, float* inv, cudaStream_t s) {
   bspline_factors_kernel<<<1, 1, 0, s>>>(n, cp, inv);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_prefilter(const float* img, int64_t nr, int64_t nc, float* coef, float* dbuf, const float* cpc,
-                             const float* ivc, const float* cpr, const float* ivr, cudaStream_t s) {
-  // (cpc, ivc): factors of the column length nr + 2; (cpr, ivr): of the row
-  // length nc + 2; dbuf: a second (nr + 2) x (nc + 2) array for the forward sweep
-  const int64_t ld = nr + 2, ncols = nc + 2;
-  const int64_t total = ld * ncols;
-  int blocks = (int)((total + 255) / 256);
-  if (blocks > 148 * 16) blocks = 148 * 16;
-  pad_copy_kernel<<<blocks, 256, 0, s>>>(img, nr, nc, coef);
-  // dim 1: the nc image columns (the two zero padding columns stay zero)
-  const int64_t segc = ld >= 5 ? (ld - 4 + BS_SEG - 1) / BS_SEG : 1;
-  bspline_fwd_kernel<<<seg_blocks(nc * segc), 256, 0, s>>>(coef + ld, dbuf + ld, ld, 1, ld, nc, ivc);
-  bspline_bwd_kernel<<<seg_blocks(nc * segc), 256, 0, s>>>(coef + ld, dbuf + ld, ld, 1, ld, nc, cpc);
-  // dim 2: every padded row, consecutive threads on consecutive rows
-  const int64_t segr = ncols >= 5 ? (ncols - 4 + BS_SEG - 1) / BS_SEG : 1;
-  bspline_fwd_kernel<<<seg_blocks(ld * segr), 256, 0, s>>>(coef, dbuf, ncols, ld, 1, ld, ivr);
-  bspline_bwd_kernel<<<seg_blocks(ld * segr), 256, 0, s>>>(coef, dbuf, ncols, ld, 1, ld, cpr);
   return cudaGetLastError();
 }
 
@@ -321,7 +220,7 @@ static unsigned b_blocks(int64_t n, int cap_per_sm = 16) {
 // padded column, the copied rows 1 and n - 2 included, so no padded copy of
 // the image is made first. Work items: (column tile, segment) per pair,
 // counted from BPair::wcol.
-__device__ __forceinline__ int64_t b_nseg(int64_t n) { return n >= 5 ? (n - 4 + BS_SEG - 1) / BS_SEG : 1; }
+__host__ __device__ __forceinline__ int64_t b_nseg(int64_t n) { return n >= 5 ? (n - 4 + BS_SEG - 1) / BS_SEG : 1; }
 
 constexpr int BS_TILE = BS_WARM + BS_SEG;  // rows staged per column
 constexpr int BS_TLD = BS_TILE + 1;        // odd stride: conflict-free by lane and by row
@@ -385,24 +284,21 @@ __device__ __forceinline__ void tile_store(const float* T, float* g, int64_t gld
   }
 }
 
+// Work item l of the column pass of one image (nr x nc, column-major): a
+// tile of 32 columns and one segment of their unknowns. coef0 / d0: the
+// padded coefficients and the forward-sweep buffer ((nr + 2) x (nc + 2)).
 template <int PASS>
-__global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPair* __restrict__ bp, int npairs,
-                                                                      int64_t witems, float* dbuf, int64_t qtot) {
-  extern __shared__ float bsc_tile[];
-  const int img = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float* T = bsc_tile + warp * BS_WSTRIDE;
-  float* F = T + BS_WTILE;
-  for (int64_t t = (int64_t)blockIdx.x * BSC_WARPS + warp; t < witems; t += (int64_t)gridDim.x * BSC_WARPS) {
-    const BPair& b = bp[bp_find<&BPair::wcol>(bp, npairs, t)];
-    if (!b.deforms) continue;  // uniform across the warp
-    const int64_t nr = b.nr, nc = b.nc, n = nr + 2, m = n - 4;
-    const int64_t ncg = (nc + 31) / 32, l = t - b.wcol;
-    if (l >= ncg * b_nseg(n)) continue;
+__device__ __forceinline__ void bs_col_item(const float* __restrict__ img0, float* coef0, float* d0, int64_t nr,
+                                            int64_t nc, const float* __restrict__ cpc, const float* __restrict__ ivc,
+                                            int64_t l, float* T, float* F, int lane) {
+  {
+    const int64_t n = nr + 2, m = n - 4;
+    const int64_t ncg = (nc + 31) / 32;
     const int64_t cg = l % ncg, seg = l / ncg;
     const int ncol = (int)min((int64_t)32, nc - cg * 32);  // columns of this tile
-    const float* im = (img ? b.B : b.A) + cg * 32 * nr;       // image column cg*32
-    float* coef = (img ? b.coefB : b.coefA) + (cg * 32 + 1) * n;  // padded column cg*32 + 1
-    float* d = dbuf + (int64_t)img * qtot + b.qoff + (cg * 32 + 1) * n;
+    const float* im = img0 + cg * 32 * nr;                     // image column cg*32
+    float* coef = coef0 + (cg * 32 + 1) * n;                   // padded column cg*32 + 1
+    float* d = d0 + (cg * 32 + 1) * n;
     const bool mine = lane < ncol;
     if (m < 1) {  // n <= 4: nothing to solve; the backward pass writes the column
       if (PASS == 1 && mine) {
@@ -420,7 +316,7 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
           x[2] = 0.f;
         }
       }
-      continue;
+      return;
     }
     const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG);
     if (PASS == 0) {
@@ -428,7 +324,7 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
       const int cnt = (int)(k1 - ks);
       // stage the right-hand sides: unknown k is padded element k + 2 = image row k + 1
       tile_load(T, im + ks + 1, nr, ncol, cnt, lane);
-      stage_factors(F, b.ivc + ks, cnt, lane);
+      stage_factors(F, ivc + ks, cnt, lane);
       __syncwarp();
       if (mine) {
         const float* ic = im + lane * nr;
@@ -453,7 +349,7 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
       const int64_t ke = min(m - 1, k1 - 1 + BS_WARM);
       const int cnt = (int)(ke - k0 + 1);
       tile_load(T, d + k0 + 2, n, ncol, cnt, lane);
-      stage_factors(F, b.cpc + k0, cnt, lane);
+      stage_factors(F, cpc + k0, cnt, lane);
       __syncwarp();
       if (mine) {
         float* x = T + lane * BS_TLD;
@@ -483,6 +379,23 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPa
       tile_store(T, coef + k0 + 2, n, ncol, nout, lane);
       __syncwarp();
     }
+  }
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_col_kernel(const BPair* __restrict__ bp, int npairs,
+                                                                      int64_t witems, float* dbuf, int64_t qtot) {
+  extern __shared__ float bsc_tile[];
+  const int img = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* T = bsc_tile + warp * BS_WSTRIDE;
+  float* F = T + BS_WTILE;
+  for (int64_t t = (int64_t)blockIdx.x * BSC_WARPS + warp; t < witems; t += (int64_t)gridDim.x * BSC_WARPS) {
+    const BPair& b = bp[bp_find<&BPair::wcol>(bp, npairs, t)];
+    if (!b.deforms) continue;  // uniform across the warp
+    const int64_t l = t - b.wcol;
+    if (l >= (b.nc + 31) / 32 * b_nseg(b.nr + 2)) continue;
+    bs_col_item<PASS>(img ? b.B : b.A, img ? b.coefB : b.coefA, dbuf + (int64_t)img * qtot + b.qoff, b.nr, b.nc,
+                      b.cpc, b.ivc, l, T, F, lane);
   }
 }
 
@@ -517,30 +430,26 @@ __device__ __forceinline__ void row_tile_store(const float* T, float* g, int64_t
   for (int j = 0; j < cnt; ++j) g[j * gld + lane] = T[j * 33 + lane];
 }
 
+// Work item l of the row pass of one image's padded coefficients coef0
+// ((nr + 2) x (nc + 2)), with the forward-sweep buffer d0 of the same shape.
 template <int PASS>
-__global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_row_kernel(const BPair* __restrict__ bp, int npairs,
-                                                                      int64_t witems, float* dbuf, int64_t qtot) {
-  extern __shared__ float bsc_tile[];
-  const int img = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float* T = bsc_tile + warp * BS_WSTRIDE;
-  float* F = T + BS_WTILE;
-  for (int64_t t = (int64_t)blockIdx.x * BSC_WARPS + warp; t < witems; t += (int64_t)gridDim.x * BSC_WARPS) {
-    const BPair& b = bp[bp_find<&BPair::wrow>(bp, npairs, t)];
-    if (!b.deforms) continue;  // uniform across the warp
-    const int64_t ld = b.nr + 2, n = b.nc + 2, m = n - 4;
-    const int64_t nrg = (ld + 31) / 32, l = t - b.wrow;
-    if (l >= nrg * b_nseg(n)) continue;
+__device__ __forceinline__ void bs_row_item(float* coef0, float* d0, int64_t nr, int64_t nc,
+                                            const float* __restrict__ cpr, const float* __restrict__ ivr, int64_t l,
+                                            float* T, float* F, int lane) {
+  {
+    const int64_t ld = nr + 2, n = nc + 2, m = n - 4;
+    const int64_t nrg = (ld + 31) / 32;
     const int64_t rg = l % nrg, seg = l / nrg, r0 = rg * 32;
     const int nrow = (int)min((int64_t)32, ld - r0);
     const bool mine = lane < nrow;
-    float* coef = (img ? b.coefB : b.coefA) + r0;                  // row r0 of the padded coefficients
-    float* d = dbuf + (int64_t)img * qtot + b.qoff + r0;
+    float* coef = coef0 + r0;  // row r0 of the padded coefficients
+    float* d = d0 + r0;
     if (PASS == 0) {
-      if (m < 1) continue;
+      if (m < 1) return;
       const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG), ks = max((int64_t)0, k0 - BS_WARM);
       const int cnt = (int)(k1 - ks);
       row_tile_load(T, coef + (ks + 2) * ld, ld, nrow, cnt, lane);  // unknown k is padded column k + 2
-      stage_factors(F, b.ivr + ks, cnt, lane);
+      stage_factors(F, ivr + ks, cnt, lane);
       __syncwarp();
       if (mine) {
         const float sixth = kSixth;
@@ -560,19 +469,19 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_row_kernel(const BPa
       row_tile_store(T + (k0 - ks) * 33, d + (k0 + 2) * ld, ld, nrow, (int)(k1 - k0), lane);
       __syncwarp();  // the tile is restaged by the next item
     } else {
-      if (n < 4) continue;
+      if (n < 4) return;
       if (m < 1) {  // n == 4: c1 = b1, c2 = b2 only
         if (mine) {
           const float c1 = coef[ld + lane], c2 = coef[2 * ld + lane];
           coef[lane] = FS(FM(2.0f, c1), c2);
           coef[3 * ld + lane] = FS(FM(2.0f, c2), c1);
         }
-        continue;
+        return;
       }
       const int64_t k0 = seg * BS_SEG, k1 = min(m, k0 + BS_SEG), ke = min(m - 1, k1 - 1 + BS_WARM);
       const int cnt = (int)(ke - k0 + 1);
       row_tile_load(T, d + (k0 + 2) * ld, ld, nrow, cnt, lane);
-      stage_factors(F, b.cpr + k0, cnt, lane);
+      stage_factors(F, cpr + k0, cnt, lane);
       __syncwarp();
       if (mine) {
         float xv = 0.f, xlast = 0.f;
@@ -595,22 +504,111 @@ __global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_row_kernel(const BPa
   }
 }
 
+template <int PASS>
+__global__ void __launch_bounds__(32 * BSC_WARPS) b_bspline_row_kernel(const BPair* __restrict__ bp, int npairs,
+                                                                      int64_t witems, float* dbuf, int64_t qtot) {
+  extern __shared__ float bsc_tile[];
+  const int img = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* T = bsc_tile + warp * BS_WSTRIDE;
+  float* F = T + BS_WTILE;
+  for (int64_t t = (int64_t)blockIdx.x * BSC_WARPS + warp; t < witems; t += (int64_t)gridDim.x * BSC_WARPS) {
+    const BPair& b = bp[bp_find<&BPair::wrow>(bp, npairs, t)];
+    if (!b.deforms) continue;  // uniform across the warp
+    const int64_t l = t - b.wrow;
+    if (l >= (b.nr + 2 + 31) / 32 * b_nseg(b.nc + 2)) continue;
+    bs_row_item<PASS>(img ? b.coefB : b.coefA, dbuf + (int64_t)img * qtot + b.qoff, b.nr, b.nc, b.cpr, b.ivr, l, T, F,
+                      lane);
+  }
+}
+
+// The same passes over the two frames of one pair (blockIdx.y: frame), for
+// the single-pair schedule and the hooks.
+struct PrefFrames {
+  const float* img[2];
+  float* coef[2];
+  float* d[2];
+};
+
+template <int PASS>
+__global__ void __launch_bounds__(32 * BSC_WARPS) bspline_col_tiles_kernel(PrefFrames P, int64_t nr, int64_t nc,
+                                                                          const float* cpc, const float* ivc,
+                                                                          int64_t witems) {
+  extern __shared__ float bsc_tile[];
+  const int img = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* T = bsc_tile + warp * BS_WSTRIDE;
+  float* F = T + BS_WTILE;
+  for (int64_t t = (int64_t)blockIdx.x * BSC_WARPS + warp; t < witems; t += (int64_t)gridDim.x * BSC_WARPS)
+    bs_col_item<PASS>(P.img[img], P.coef[img], P.d[img], nr, nc, cpc, ivc, t, T, F, lane);
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(32 * BSC_WARPS) bspline_row_tiles_kernel(PrefFrames P, int64_t nr, int64_t nc,
+                                                                          const float* cpr, const float* ivr,
+                                                                          int64_t witems) {
+  extern __shared__ float bsc_tile[];
+  const int img = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* T = bsc_tile + warp * BS_WSTRIDE;
+  float* F = T + BS_WTILE;
+  for (int64_t t = (int64_t)blockIdx.x * BSC_WARPS + warp; t < witems; t += (int64_t)gridDim.x * BSC_WARPS)
+    bs_row_item<PASS>(P.coef[img], P.d[img], nr, nc, cpr, ivr, t, T, F, lane);
+}
+
+static cudaError_t set_tile_smem() {
+  static bool done = false;
+  if (done) return cudaSuccess;
+  for (cudaError_t e : {cudaFuncSetAttribute(b_bspline_col_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)BSC_SMEM),
+                        cudaFuncSetAttribute(b_bspline_col_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)BSC_SMEM),
+                        cudaFuncSetAttribute(b_bspline_row_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)BSC_SMEM),
+                        cudaFuncSetAttribute(b_bspline_row_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)BSC_SMEM),
+                        cudaFuncSetAttribute(bspline_col_tiles_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)BSC_SMEM),
+                        cudaFuncSetAttribute(bspline_col_tiles_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)BSC_SMEM),
+                        cudaFuncSetAttribute(bspline_row_tiles_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)BSC_SMEM),
+                        cudaFuncSetAttribute(bspline_row_tiles_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)BSC_SMEM)})
+    if (e != cudaSuccess) return e;
+  done = true;
+  return cudaSuccess;
+}
+
+static unsigned tile_blocks(int64_t witems) {
+  int64_t blocks = (witems + BSC_WARPS - 1) / BSC_WARPS;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  return (unsigned)(blocks < 1 ? 1 : blocks);
+}
+
+cudaError_t launch_prefilter_pair(const float* imgA, const float* imgB, int64_t nr, int64_t nc, float* coefA,
+                                  float* coefB, float* dbuf, const float* cpc, const float* ivc, const float* cpr,
+                                  const float* ivr, cudaStream_t s) {
+  cudaError_t e = set_tile_smem();
+  if (e != cudaSuccess) return e;
+  const int64_t ld = nr + 2, q = ld * (nc + 2);
+  const PrefFrames P{{imgA, imgB}, {coefA, coefB}, {dbuf, dbuf + q}};
+  const int64_t wc = (nc + 31) / 32 * b_nseg(ld), wr = (ld + 31) / 32 * b_nseg(nc + 2);
+  bspline_col_tiles_kernel<0><<<dim3(tile_blocks(wc), 2), 32 * BSC_WARPS, BSC_SMEM, s>>>(P, nr, nc, cpc, ivc, wc);
+  bspline_col_tiles_kernel<1><<<dim3(tile_blocks(wc), 2), 32 * BSC_WARPS, BSC_SMEM, s>>>(P, nr, nc, cpc, ivc, wc);
+  if (nc + 2 < 4)  // padding columns 0 and nc + 1 stay zero: no row to solve writes them
+    for (float* c : {coefA, coefB}) {
+      e = cudaMemsetAsync(c, 0, ld * sizeof(float), s);
+      if (e == cudaSuccess) e = cudaMemsetAsync(c + (nc + 1) * ld, 0, ld * sizeof(float), s);
+      if (e != cudaSuccess) return e;
+    }
+  bspline_row_tiles_kernel<0><<<dim3(tile_blocks(wr), 2), 32 * BSC_WARPS, BSC_SMEM, s>>>(P, nr, nc, cpr, ivr, wr);
+  bspline_row_tiles_kernel<1><<<dim3(tile_blocks(wr), 2), 32 * BSC_WARPS, BSC_SMEM, s>>>(P, nr, nc, cpr, ivr, wr);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_b_prefilter(const BPair* bp, int npairs, int64_t qtot, int64_t wcol_tot, int64_t wrow_tot,
                                float* dbuf, cudaStream_t s) {
   if (qtot <= 0) return cudaSuccess;
-  static bool attr_set = false;
-  if (!attr_set) {
-    for (cudaError_t e : {cudaFuncSetAttribute(b_bspline_col_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)BSC_SMEM),
-                          cudaFuncSetAttribute(b_bspline_col_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)BSC_SMEM),
-                          cudaFuncSetAttribute(b_bspline_row_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)BSC_SMEM),
-                          cudaFuncSetAttribute(b_bspline_row_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)BSC_SMEM)})
-      if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  cudaError_t e = set_tile_smem();
+  if (e != cudaSuccess) return e;
   if (wcol_tot > 0) {
     int64_t blocks = (wcol_tot + BSC_WARPS - 1) / BSC_WARPS;
     if (blocks > 148 * 8) blocks = 148 * 8;
