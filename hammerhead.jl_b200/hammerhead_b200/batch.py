@@ -8,6 +8,7 @@ decided on the device, and the launch sequence of a batch shape is captured
 in a CUDA graph once and replayed. Results equal run_piv on each pair.
 """
 import ctypes
+import zlib
 
 import numpy as np
 
@@ -236,7 +237,8 @@ def run_piv_sequence(pairs, params=None, *, preprocess=None, progress=False, on_
     (converted on the device, see BatchRunner).
 
     With `pipeline` (CUDA available, every pair of one shape and pixel type,
-    no masks), the frames of batch k+1 are copied to the device through
+    no mask or one mask for every pair), the frames of batch k+1 are copied
+    to the device through
     page-locked double buffers on a copy stream while batch k is analysed,
     so ingestion overlaps the analysis (the reference prefetches the next
     pair's frames on a background task, src/io.jl:296-306)."""
@@ -248,7 +250,7 @@ def run_piv_sequence(pairs, params=None, *, preprocess=None, progress=False, on_
     if preprocess is not None:
         pairs = [(preprocess(a), preprocess(b)) for a, b in pairs]
     same = len({(tuple(a.shape), str(a.dtype), tuple(b.shape), str(b.dtype)) for a, b in pairs}) == 1
-    if pipeline and mask is None and same and not _is_device(pairs[0][0]):
+    if pipeline and not callable(mask) and same and not _is_device(pairs[0][0]):
         try:
             import torch
             ok = torch.cuda.is_available()
@@ -256,7 +258,7 @@ def run_piv_sequence(pairs, params=None, *, preprocess=None, progress=False, on_
             ok = False
         if ok:
             return _sequence_pipelined(pairs, params, on_result, progress, batch_size, predictor_smoothing,
-                                       mask_threshold, workspace, u16)
+                                       mask_threshold, workspace, u16, mask)
     out = []
     for start in range(0, n, batch_size):
         chunk = pairs[start:start + batch_size]
@@ -286,13 +288,24 @@ def _is_device(a):
     return hasattr(a, "data_ptr") and getattr(a, "is_cuda", False)
 
 
-def _sequence_pipelined(pairs, params, on_result, progress, batch_size, smoothing, thr, workspace, u16):
+def _device_mask(m, shape):
+    """A host mask as a column-major uint8 CUDA tensor (stride (1, nrows))."""
+    import torch
+
+    m = np.asarray(m)
+    if tuple(m.shape) != tuple(shape):
+        raise DimensionMismatch(f"mask must have the same size as the images, got {tuple(m.shape)}")
+    return torch.from_numpy(np.ascontiguousarray(m.T != 0).astype(np.uint8)).cuda().T
+
+
+def _sequence_pipelined(pairs, params, on_result, progress, batch_size, smoothing, thr, workspace, u16, mask=None):
     import concurrent.futures as cf
 
     import torch
 
     n = len(pairs)
     nr, nc = pairs[0][0].shape
+    dmask = None if mask is None else _device_mask(mask, (nr, nc))
     tdt = torch.uint16 if _is_u16(pairs[0][0]) else torch.float32
     ndt = np.uint16 if tdt == torch.uint16 else np.float32
     B = min(batch_size, n)
@@ -321,8 +334,8 @@ def _sequence_pipelined(pairs, params, on_result, progress, batch_size, smoothin
         key = (slot, m)
         if key not in runners:
             frames = [(dev[slot][2 * j].T, dev[slot][2 * j + 1].T) for j in range(m)]
-            runners[key] = BatchRunner(frames, params, predictor_smoothing=smoothing, mask_threshold=thr,
-                                       workspace=ws, u16=u16)
+            runners[key] = BatchRunner(frames, params, masks=None if dmask is None else [dmask] * m,
+                                       predictor_smoothing=smoothing, mask_threshold=thr, workspace=ws, u16=u16)
         return runners[key]
 
     nb = (n + B - 1) // B
@@ -355,8 +368,8 @@ def _sequence_pipelined(pairs, params, on_result, progress, batch_size, smoothin
     return out
 
 
-def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_threshold=0.5, workspace=None,
-                         u16="normalised", on_batch=None):
+def run_piv_batch_stream(batches, passes, *, masks=None, predictor_smoothing=True, mask_threshold=0.5,
+                         workspace=None, u16="normalised", on_batch=None):
     """A stream of batches of the same composition (for example every camera
     of a rig at each time step): batch k+1's frames are copied to the device
     on a copy stream while batch k is analysed, so the host-to-device copies
@@ -368,8 +381,9 @@ def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_thre
     shape and pixel type (float32 or UInt16) in every batch. Frames in
     page-locked memory (for example numpy views of pinned torch tensors,
     column-major) are copied directly; others go through page-locked
-    staging buffers first. Needs a CUDA device visible to torch; masks are
-    not supported on this path (use run_piv_batch). With a caller's
+    staging buffers first. `masks`: None or one mask (or None) per pair,
+    the same for every batch (copied to the device once). Needs a CUDA
+    device visible to torch. With a caller's
     workspace, the device frames and prepared runners of a composition are
     kept in it for the next call of the same composition."""
     import concurrent.futures as cf
@@ -393,8 +407,14 @@ def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_thre
     own = workspace is None
     ws = workspace if workspace is not None else PIVWorkspace()
     scheds, index = _schedules(passes, n)
+    if masks is not None:
+        masks = list(masks)
+        if len(masks) != n:
+            raise DimensionMismatch(f"got {len(masks)} masks for {n} pairs")
+    mkey = None if masks is None else tuple(
+        None if m is None else zlib.crc32(np.asfortranarray(np.asarray(m) != 0).tobytes(order="F")) for m in masks)
     key = (tuple(spec), tuple(index), b"".join(bytes(q.to_desc()) for sc in scheds for q in sc),
-           bool(predictor_smoothing), float(mask_threshold), u16)
+           bool(predictor_smoothing), float(mask_threshold), u16, mkey)
     cache = None if own else ws.__dict__.setdefault("_stream_sessions", {})
     sess = None if cache is None else cache.get(key)
     if sess is None:
@@ -403,7 +423,9 @@ def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_thre
                     dev=[[(torch.empty((nc, nr), dtype=t, device="cuda"), torch.empty((nc, nr), dtype=t, device="cuda"))
                           for nr, nc, t in spec] for _ in range(2)],
                     stage_host={},  # page-locked staging for frames that are not page-locked already
-                    events=[torch.cuda.Event(), torch.cuda.Event()], runners=None)
+                    events=[torch.cuda.Event(), torch.cuda.Event()], runners=None,
+                    masks=None if masks is None else [None if m is None else _device_mask(m, sp[:2])
+                                                      for m, sp in zip(masks, spec)])
     copy_stream, dev, stage_host, events = sess["copy_stream"], sess["dev"], sess["stage_host"], sess["events"]
 
     def host_tensor(x, j, which, slot):
@@ -448,7 +470,7 @@ def run_piv_batch_stream(batches, passes, *, predictor_smoothing=True, mask_thre
         with cf.ThreadPoolExecutor(max_workers=1) as pool, cf.ThreadPoolExecutor(max_workers=1) as post:
             fut = pool.submit(stage, first, 0)
             if runners is None:  # prepared while the first batch is copied in
-                runners = [BatchRunner([(a.T, b.T) for a, b in dev[s]], passes,
+                runners = [BatchRunner([(a.T, b.T) for a, b in dev[s]], passes, masks=sess["masks"],
                                        predictor_smoothing=predictor_smoothing, mask_threshold=mask_threshold,
                                        workspace=ws, u16=u16) for s in range(2)]
                 if cache is not None:

@@ -275,3 +275,37 @@ def test_batch_stream_session_reused(hb, ws):
             _same(x, y)
     hb.run_piv_batch_stream([batches[0][:3]], sched[:3], workspace=ws)
     assert len(ws._stream_sessions) == 2
+
+
+def test_pipelined_paths_with_static_masks(hb, ws):
+    # one mask per pair, the same in every batch: copied to the device once
+    # and used by both pipelined paths exactly as by a batch call
+    s1, s2 = _schedules(hb)
+    sched = [s1, s2, s2, s1]
+    batches = [_mixed(hb, n=4, seed=800 + 10 * k)[0] for k in range(2)]
+    masks = []
+    for j, (A, _) in enumerate(batches[0]):
+        if j == 1:
+            masks.append(None)
+            continue
+        m = np.zeros(A.shape, bool)
+        m[: A.shape[0] // 3, A.shape[1] // 2:] = True
+        masks.append(m)
+    out = hb.run_piv_batch_stream(batches, sched, masks=masks, workspace=ws)
+    for k in range(2):
+        ref = hb.run_piv_batch(batches[k], sched, masks=masks, workspace=ws)
+        for a, b in zip(out[k], ref):
+            _same(a, b)
+        assert out[k][0].mask.any() and not out[k][1].mask.any()
+    # the sequence driver pipelines a single mask for every pair
+    syn = hb.synthetic
+    pairs = [syn.particle_pair((256, 256), syn.sine_shear_flow(2.0, 180.0), seed=90 + i) for i in range(5)]
+    m = np.zeros((256, 256), bool)
+    m[100:160, 40:120] = True
+    piped = hb.run_piv_sequence(pairs, s1, batch_size=2, mask=m, workspace=ws)
+    plain = hb.run_piv_sequence(pairs, s1, batch_size=2, mask=m, workspace=ws, pipeline=False)
+    for a, b in zip(piped, plain):
+        _same(a, b)
+    assert piped[0].mask.any()
+    with pytest.raises(hb.DimensionMismatch):
+        hb.run_piv_batch_stream(batches, sched, masks=masks[:3], workspace=ws)
