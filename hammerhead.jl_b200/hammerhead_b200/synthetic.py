@@ -155,6 +155,32 @@ def config2_case(seed=1001, noise=0.3, window=16, overlap=8):
     return A, B, flow, P.astype(np.float32), (float(y[0]), float(step), float(x[0]), float(step))
 
 
+def config4_frames(n_frames=3, shape=(4096, 4096), seed=1004, peak=6.0, ppp=0.01, noise=0.05, sigma=0.65):
+    """The large-frame time series: chained frames of a Poiseuille channel
+    flow along x (`peak` px at the centre line) at `ppp` particles per pixel,
+    noise sigma `noise`, as 12-bit counts in UInt16 (to_uint16_12bit). Frame
+    k + 1 holds frame k's particles moved by the flow once; pair k is
+    (frames[k], frames[k + 1]). Returns (frames, flow)."""
+    nr, nc = shape
+    flow = poiseuille_flow(nr, peak)
+    rng = np.random.default_rng(seed)
+    margin = 10.0
+    left = margin + peak * n_frames  # particles that drift into the frame
+    n = int(round(ppp * (nr + 2 * margin) * (nc + margin + left)))
+    rows = rng.uniform(1 - margin, nr + margin, n)
+    cols = rng.uniform(1 - left, nc + margin, n)
+    inten = rng.uniform(0.5, 1.0, n)
+    frames = []
+    for _ in range(n_frames):
+        img = _render(shape, rows, cols, inten, sigma)
+        if noise > 0:
+            img += noise * rng.standard_normal((nr, nc))
+        frames.append(to_uint16_12bit(img))
+        du, dv = flow(cols, rows)
+        rows, cols = rows + dv, cols + du
+    return frames, flow
+
+
 def config3_pairs(n512=24, n768=24, n2048=16, seed0=1003):
     """The mixed batch: (shape, flow, schedule kind) per pair, drawn from the
     pair seed: sinusoidal shear (A ~ U[1,6], lambda ~ U[128,512]) or a uniform
