@@ -188,6 +188,7 @@ hh_status run_schedule(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr
       ca.nalt = nalt;
       ca.rec = prec;
       ca.win = p.search[0] != W ? W : 0;
+      ca.variant = corr_variant(ctx, p);
       HH_K(HH_K_CORRELATE, 1, corr_flops(N, njobs), corr_bytes(p.search[0], nalt, njobs), njobs,
            hh::launch_correlate(ca, N, p.search[0], s, ctx->num_sms));
       if (fused_unc) {
@@ -694,6 +695,7 @@ static hh_status hook_correlate(hh_ctx* ctx, const hh_pass_desc* p, const int32_
   ca.planes = dpl;
   ca.rec = drec;
   ca.win = p->search[0] != W ? W : 0;
+  ca.variant = corr_variant(ctx, *p);
   HH_K(HH_K_CORRELATE, 1, 0, 0, 0, hh::launch_correlate(ca, N, p->search[0], s, ctx->num_sms));
   if (uq) {
     HH_TRY(buf(ctx, "hook_uq", (size_t)88 * njobs, &duq));
@@ -953,3 +955,112 @@ hh_status hh_profile_read(hh_ctx* ctx, hh_kernel_profile* out, int32_t reset) {
 int64_t hh_launch_count(const hh_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Autotuning of the correlation kernel's CTA shape.
+static void drop_plans(hh_ctx* ctx) {  // batched graphs captured with an older choice
+  if (ctx->bplan_free)
+    for (auto& kv : ctx->bplans) ctx->bplan_free(kv.second);
+  ctx->bplans.clear();
+}
+
+extern "C" hh_status hh_set_corr_variant(hh_ctx* ctx, int32_t fft_size_, int32_t window, int32_t variant) {
+  if (!ctx) return fail(nullptr, HH_ERR_ARG, "context is NULL");
+  if (variant < 0 || variant >= HH_CORR_VARIANTS)
+    return fail(ctx, HH_ERR_ARG, "variant must be in [0, " + std::to_string(HH_CORR_VARIANTS) + "), got " +
+                                     std::to_string(variant));
+  if (!hh::correlate_supported(fft_size_, window))
+    return fail(ctx, HH_ERR_ARG, "no correlation kernel for FFT size " + std::to_string(fft_size_) + " and window " +
+                                     std::to_string(window));
+  HH_TRY(set_device(ctx));
+  HH_CK(cudaStreamSynchronize(ctx->stream));
+  ctx->corr_var[{fft_size_, window}] = variant;
+  drop_plans(ctx);
+  return HH_OK;
+}
+
+extern "C" hh_status hh_autotune_correlation(hh_ctx* ctx, const hh_pass_desc* p, int32_t reps, float* variant_ms,
+                                             int32_t* best) {
+  if (!ctx) return fail(nullptr, HH_ERR_ARG, "context is NULL");
+  HH_TRY(set_device(ctx));
+  if (!ctx->staged) return fail(ctx, HH_ERR_STATE, "no staged pair: call hh_stage_pair first");
+  HH_TRY(check_passes(ctx, p, 1));
+  const hh_status cs = hh_check_backend_params(p, 1);
+  if (cs != HH_OK) return fail(ctx, cs, hh_last_error(nullptr));
+  if (p->search[0] != p->window[0])
+    return fail(ctx, HH_ERR_ARG, "autotuning covers passes with equal window and search area");
+  if (reps < 1) return fail(ctx, HH_ERR_ARG, "reps must be at least 1, got " + std::to_string(reps));
+  Grid g;
+  HH_TRY(make_grid(ctx, ctx->nr, ctx->nc, *p, nullptr, 0.5, g));
+  const int64_t njobs = (int64_t)g.jobs.size() / 4;
+  if (njobs < 1) return fail(ctx, HH_ERR_ARG, "the staged pair holds no window of this pass");
+  cudaStream_t s = ctx->stream;
+  const int N = fft_size(*p);
+  const int64_t G = (int64_t)g.ny * g.nx;
+  Tables tb;
+  HH_TRY(get_tables(ctx, *p, tb));
+  int32_t* dj;
+  float *du, *dv, *ratio, *moment, *alt = nullptr, *rec;
+  const int nalt = p->n_peaks - 1;
+  HH_TRY(buf(ctx, "tune_jobs", (size_t)g.jobs.size(), &dj));
+  HH_TRY(buf(ctx, "tune_out", (size_t)4 * G, &du));
+  dv = du + G;
+  ratio = dv + G;
+  moment = ratio + G;
+  if (nalt > 0) HH_TRY(buf(ctx, "tune_alt", (size_t)2 * nalt * G, &alt));
+  HH_TRY(buf(ctx, "tune_rec", hh::correlate_record_words(p->n_peaks) * njobs, &rec));
+  HH_CK(cudaMemcpyAsync(dj, g.jobs.data(), g.jobs.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  CorrArgs ca{};
+  ca.A = ctx->curA;
+  ca.B = ctx->curB;
+  ca.ld = ctx->nr;
+  ca.jobs = dj;
+  ca.njobs = njobs;
+  ca.ny = g.ny;
+  ca.G = G;
+  ca.apod = tb.apod;
+  ca.gain = tb.gain;
+  ca.phasew = tb.phasew;
+  ca.box_lo = tb.box_lo;
+  ca.box_hi = tb.box_hi;
+  ca.method = p->method;
+  ca.npeaks = p->n_peaks;
+  ca.finder = p->peak_finder;
+  ca.subpixel = p->subpixel;
+  ca.du = du;
+  ca.dv = dv;
+  ca.ratio = ratio;
+  ca.moment = moment;
+  ca.alt_u = alt;
+  ca.alt_v = nalt > 0 ? alt + (int64_t)nalt * G : nullptr;
+  ca.nalt = nalt;
+  ca.rec = rec;
+  cudaEvent_t e0, e1;
+  HH_CK(cudaEventCreate(&e0));
+  HH_CK(cudaEventCreate(&e1));
+  double tot[HH_CORR_VARIANTS] = {};
+  cudaError_t err = cudaSuccess;
+  for (int r = -1; r < reps && err == cudaSuccess; ++r)  // round -1 warms every shape up
+    for (int v = 0; v < HH_CORR_VARIANTS && err == cudaSuccess; ++v) {
+      ca.variant = v;
+      err = cudaEventRecord(e0, s);
+      if (err == cudaSuccess) err = hh::launch_correlate(ca, N, p->search[0], s, ctx->num_sms);
+      if (err == cudaSuccess) err = cudaEventRecord(e1, s);
+      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+      if (r >= 0) tot[v] += ms;
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  HH_CK(err);
+  int b = 0;
+  for (int v = 0; v < HH_CORR_VARIANTS; ++v) {
+    if (variant_ms) variant_ms[v] = (float)(tot[v] / reps);
+    if (tot[v] < tot[b]) b = v;
+  }
+  if (best) *best = b;
+  ctx->corr_var[{N, (int)p->search[0]}] = b;
+  drop_plans(ctx);
+  return HH_OK;
+}

@@ -433,6 +433,10 @@ static hh_status issue(hh_ctx* ctx, BPlan& P) {
         ca.it = it;
         ca.rec = P.rec;
         ca.win = c.S != c.W ? c.W : 0;
+        {
+          auto cv = ctx->corr_var.find({c.N, c.S});
+          ca.variant = cv == ctx->corr_var.end() ? 0 : cv->second;
+        }
         HH_K(HH_K_CORRELATE, 1, corr_flops(c.N, c.njobs), corr_bytes(c.S, c.npeaks - 1, c.njobs), c.njobs,
              hh::launch_correlate(ca, c.N, c.S, s, ctx->num_sms));
       }

@@ -79,6 +79,9 @@ struct hh_ctx {
   // cross-process reduction of the ensemble sums (hh_set_ensemble_reducer)
   hh_ensemble_reducer ens_reduce = nullptr;
   void* ens_reduce_user = nullptr;
+  // correlation kernel CTA shape per (FFT size, data extent), from
+  // hh_set_corr_variant / hh_autotune_correlation (absent: 0, the default)
+  std::map<std::pair<int, int>, int> corr_var;
 };
 
 namespace hhd {
@@ -190,6 +193,12 @@ inline hh_status make_grid(hh_ctx* ctx, int64_t nr, int64_t nc, const hh_pass_de
 }
 
 inline int fft_size(const hh_pass_desc& p) { return p.padding ? 2 * p.search[0] : p.search[0]; }
+
+// The CTA shape chosen for a pass's correlation launches.
+inline int32_t corr_variant(const hh_ctx* ctx, const hh_pass_desc& p) {
+  auto it = ctx->corr_var.find({fft_size(p), (int)p.search[0]});
+  return it == ctx->corr_var.end() ? 0 : it->second;
+}
 
 // apodization_window (src/correlators.jl:18-25), computed in double like Julia
 inline void apod_table(int W, int apod, std::vector<float>& out) {

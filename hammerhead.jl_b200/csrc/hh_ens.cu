@@ -209,6 +209,7 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
         ca.planes = acc;
         ca.accumulate = 1;
         ca.win = p.search[0] != W ? W : 0;
+        ca.variant = corr_variant(ctx, p);
         HH_K(HH_K_CORRELATE, 1, corr_flops(N, njobs), corr_bytes(p.search[0], 0, njobs) + 8.0 * N * N * njobs, njobs,
              hh::launch_correlate(ca, N, p.search[0], s, ctx->num_sms));
         if (unc) {

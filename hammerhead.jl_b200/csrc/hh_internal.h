@@ -51,6 +51,8 @@ struct CorrArgs {
   // the frame-A window centred in it (jobs give the window's origin); 0 when
   // the two are equal
   int32_t win;
+  // CTA shape of the launch (0: default, 1: the alternative; equal areas only)
+  int32_t variant;
   // peak records (correlate_record_words(npeaks) x njobs floats) or nullptr:
   // with regional maxima the per-window outputs are then formed by a
   // one-thread-per-window epilogue kernel after the correlation kernel

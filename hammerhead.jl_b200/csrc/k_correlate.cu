@@ -643,19 +643,30 @@ __device__ __forceinline__ float2 cross_spectrum(float2 X, float2 Zm, int method
 
 // ---------------------------------------------------------------------------
 // W is the extent of the data: the window, or with SRCH the frame-B search
-// area that holds the (runtime) frame-A window at its centre.
-template <int N, int W, bool SRCH = false> struct CorrCfg {
+// area that holds the (runtime) frame-A window at its centre. VAR selects the
+// CTA shape (windows per CTA, threads per window, register budget): 0 the
+// default, 1 the alternative the autotuner times against it (the same
+// arithmetic on another thread mapping, so the results are identical).
+template <int N, int W, bool SRCH = false, int VAR = 0> struct CorrCfg {
   static constexpr int N1 = AxisSplit<N>::N1, N2 = AxisSplit<N>::N2;
   // 16 x 16 windows padded to 32: every stage of the plane has at most 16
   // lines (16 data columns, 16 canonical column items, 16 row pairs), so
   // half a warp serves a window and each warp carries two
-  static constexpr bool HALF = N == 32 && W == 16;
-  static constexpr int WPC = HALF ? 8 : (N <= 32 ? 4 : (N <= 64 ? 2 : 1));  // windows per CTA
-  static constexpr int NT = N <= 48 ? 128 : (N <= 96 ? 256 : 512);
+  static constexpr bool HALF = VAR == 0 && N == 32 && W == 16;
+  // alternatives: N <= 32 one window per warp in CTAs of 4 (half-warp
+  // windows) or 8 warps; N = 48 a 3-CTA register budget; N = 64 one window
+  // per 256-thread CTA; N = 96 512 threads and N = 128 256 threads per window
+  static constexpr int WPC = VAR == 0 ? (HALF ? 8 : (N <= 32 ? 4 : (N <= 64 ? 2 : 1)))  // windows per CTA
+                                      : (N <= 32 ? (N == 32 && W == 16 ? 4 : 8) : (N <= 48 ? 2 : 1));
+  static constexpr int NT = VAR == 0 ? (N <= 48 ? 128 : (N <= 96 ? 256 : 512))
+                                     : (N <= 32 ? (N == 32 && W == 16 ? 128 : 256)
+                                                : (N <= 48 ? 128 : (N <= 64 ? 256 : (N <= 96 ? 512 : 256))));
   static constexpr int G = NT / WPC;  // threads per window
   // CTAs per SM the register budget is sized for (the shared-memory limit
   // allows at least this many)
-  static constexpr int MINB = HALF ? 3 : (N <= 48 ? 4 : (N <= 64 ? 3 : (N <= 96 ? 2 : 1)));
+  static constexpr int MINB = VAR == 0 ? (HALF ? 3 : (N <= 48 ? 4 : (N <= 64 ? 3 : (N <= 96 ? 2 : 1))))
+                                       : (N <= 32 ? (N == 32 && W == 16 ? 4 : 2)
+                                                  : (N <= 48 ? 3 : (N <= 64 ? 3 : 1)));
   // the peak analysis inline (one window per CTA: its latency is the CTA's)
   static constexpr bool INLINE_ANALYSIS = N >= 96;
   // Canonical column c sits at storage column N2 (c % N1) + c / N1, and with
@@ -693,10 +704,10 @@ template <int N, int W, bool SRCH = false> struct CorrCfg {
   static_assert(N * LDR <= 2 * N * LD, "real plane must fit in the complex plane");
 };
 
-template <int N, int W, bool SRCH>
-__global__ void __launch_bounds__(CorrCfg<N, W, SRCH>::NT, CorrCfg<N, W, SRCH>::MINB)
+template <int N, int W, bool SRCH, int VAR>
+__global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SRCH, VAR>::MINB)
     correlate_kernel(const CorrArgs a) {
-  using C = CorrCfg<N, W, SRCH>;
+  using C = CorrCfg<N, W, SRCH, VAR>;
   constexpr int WPC = C::WPC, NT = C::NT, LD = C::LD, LDR = C::LDR, N1 = C::N1, N2 = C::N2, IPT = C::IPT;
   constexpr int G = C::G, EPT = C::EPT, NC = C::NC, H = N / 2;
   constexpr int PS = C::PS;
@@ -1275,29 +1286,30 @@ __global__ void __launch_bounds__(128) peak_epilogue_kernel(const CorrArgs a, in
 size_t correlate_record_words(int npeaks) { return (size_t)rec_words(npeaks > 2 ? npeaks : 2); }
 
 // ---------------------------------------------------------------------------
-template <int N, int W, bool SRCH> static cudaError_t launch_nw(const CorrArgs& a, cudaStream_t s, int num_sms) {
-  using C = CorrCfg<N, W, SRCH>;
+template <int N, int W, bool SRCH, int VAR>
+static cudaError_t launch_nw(const CorrArgs& a, cudaStream_t s, int num_sms) {
+  using C = CorrCfg<N, W, SRCH, VAR>;
   const size_t sm = C::smem();
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(correlate_kernel<N, W, SRCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = cudaFuncSetAttribute(correlate_kernel<N, W, SRCH, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     // the planes live in shared memory: ask for the largest carveout so the
     // register budget, not the L1 split, sets the CTAs per SM
-    e = cudaFuncSetAttribute(correlate_kernel<N, W, SRCH>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    e = cudaFuncSetAttribute(correlate_kernel<N, W, SRCH, VAR>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, correlate_kernel<N, W, SRCH>, C::NT, sm);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, correlate_kernel<N, W, SRCH, VAR>, C::NT, sm);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   const int64_t units = (a.njobs + C::WPC - 1) / C::WPC;
   int64_t grid = (int64_t)per_sm * num_sms;
   if (grid > units) grid = units;
   if (grid < 1) grid = 1;
-  correlate_kernel<N, W, SRCH><<<(unsigned)grid, C::NT, sm, s>>>(a);
+  correlate_kernel<N, W, SRCH, VAR><<<(unsigned)grid, C::NT, sm, s>>>(a);
   if (a.rec && a.finder == 0 && !a.accumulate) {
     int64_t eb = (a.njobs + 127) / 128;
     if (eb > (int64_t)num_sms * 16) eb = (int64_t)num_sms * 16;
@@ -1326,9 +1338,12 @@ size_t correlate_smem_bytes(int N, int W) {
 
 cudaError_t launch_correlate(const CorrArgs& a, int N, int W, cudaStream_t s, int num_sms) {
   if (a.njobs <= 0) return cudaSuccess;
-#define X(n, w)                                                                                       \
-  if (N == n && W == w)                                                                              \
-    return a.win > 0 && a.win < w ? launch_nw<n, w, true>(a, s, num_sms) : launch_nw<n, w, false>(a, s, num_sms);
+#define X(n, w)                                                                         \
+  if (N == n && W == w) {                                                              \
+    if (a.win > 0 && a.win < w) return launch_nw<n, w, true, 0>(a, s, num_sms);       \
+    return a.variant == 1 ? launch_nw<n, w, false, 1>(a, s, num_sms)                   \
+                          : launch_nw<n, w, false, 0>(a, s, num_sms);                  \
+  }
   HH_CORR_CASES(X)
 #undef X
   return cudaErrorInvalidValue;

@@ -27,6 +27,8 @@ from .batch import BatchRunner, run_piv_batch, run_piv_batch_stream, run_piv_seq
 from .ensemble import collective_reducer, run_piv_ensemble, shard_pairs
 from .statistics import error_statistics, rms_error
 from . import synthetic
+from . import autotune as tuning
+from .autotune import autotune
 
 __all__ = [
     "ArgumentError", "DimensionMismatch", "HammerheadError", "LIBPATH", "PIVParameters", "multipass_parameters",
@@ -35,6 +37,7 @@ __all__ = [
     "piv_workspace", "run_piv", "pass_grid", "check_backend_params", "with_scale", "error_statistics", "rms_error",
     "synthetic", "BatchRunner", "run_piv_batch", "run_piv_batch_stream", "run_piv_sequence", "NCCLoss", "adjoint",
     "run_piv_ensemble",
+    "autotune",
     "shard_pairs",
     "collective_reducer",
 ]

@@ -177,6 +177,9 @@ SIGNATURES = [
      [_CTX, ctypes.POINTER(hh_batch_pair), ctypes.c_int32, _PASS, ctypes.c_int32, _U8, ctypes.c_double,
       ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(hh_result)]),
     ("hh_set_ensemble_reducer", ctypes.c_int32, [_CTX, ctypes.c_void_p, ctypes.c_void_p]),
+    ("hh_autotune_correlation", ctypes.c_int32,
+     [_CTX, _PASS, ctypes.c_int32, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int32)]),
+    ("hh_set_corr_variant", ctypes.c_int32, [_CTX, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     ("hh_ncc_loss_grad", ctypes.c_int32,
      [_CTX, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
       ctypes.c_float, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),

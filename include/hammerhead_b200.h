@@ -209,6 +209,23 @@ hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npair
                           int32_t npasses, const uint8_t* mask, double mask_threshold,
                           int32_t predictor_smoothing, int32_t flags, hh_result* out);
 
+/* ---- Autotuning of the correlation kernel --------------------------------
+ * The correlation kernel of each (FFT size, window) comes in
+ * HH_CORR_VARIANTS CTA shapes (windows per CTA, threads per window,
+ * register budget); all compute the same results. hh_autotune_correlation
+ * times every shape on the windows of `pass` over the staged pair
+ * (hh_stage_pair first), `reps` launches each, interleaved, writes the mean
+ * ms per launch of each shape into variant_ms (HH_CORR_VARIANTS entries)
+ * and makes the fastest the context's choice for that (FFT size, window),
+ * returned in *best. hh_set_corr_variant sets a choice directly (for
+ * example from a cache of earlier tuning). Both drop the context's batched
+ * plans, whose graphs hold the old choice. Enlarged search areas have one
+ * shape. No counterpart in the reference. */
+#define HH_CORR_VARIANTS 2
+hh_status hh_autotune_correlation(hh_ctx* ctx, const hh_pass_desc* pass, int32_t reps, float* variant_ms,
+                                  int32_t* best);
+hh_status hh_set_corr_variant(hh_ctx* ctx, int32_t fft_size, int32_t window, int32_t variant);
+
 /* Cross-process reduction of the ensemble sums (multi-GPU ensemble: each
  * process holds a share of the pairs). The reference sums every plane on one
  * host (accum[j] .+= plane, src/ensemble.jl:170-171; the uncertainty sums,
