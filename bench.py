@@ -21,6 +21,11 @@ e2e    = the same through the public streaming API (run_piv_batch_stream)
          the timed region, the copies of batch k+1 overlapping the analysis of
          batch k; time per batch = total / K.
 
+Before timing, the correlation kernel's CTA shape of every pass class is
+chosen on the device by the autotuner (hammerhead_b200.autotune; the choices
+and the per-shape times appear as "autotune"; --no-autotune keeps the
+defaults).
+
 --impl reference times the CPU restatement of the reference algorithm
 (oracle/, all host threads) on a bounded sample of the same workload; the
 reference itself is Julia, which neither this machine nor the GPU box has.
@@ -233,6 +238,7 @@ def main():
     ap.add_argument("--plain", action="store_true", help="time the plain per-pair form instead of the batched one")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison step")
     ap.add_argument("--limit", type=int, default=None, help="use only the first N pairs (debugging)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default correlation CTA shapes")
     args = ap.parse_args()
 
     import hammerhead_b200 as hb
@@ -265,6 +271,9 @@ def main():
             torch.from_numpy(np.ascontiguousarray(p["B"].T)).cuda().T) for p in pairs]
     scheds = [p["passes"] for p in pairs]
     nvec_rank = sum(final_vectors(hb, p) for p in pairs)
+    # the correlation kernel's CTA shape per pass class, timed on this device
+    # (setup, outside every timed region)
+    tuned = {} if args.no_autotune else hb.autotune(scheds, ws, reps=5)
 
     def dev_time(fn, steps):
         """Device time of `steps` calls of fn on the context stream (ms per call)."""
@@ -404,6 +413,8 @@ def main():
                                 "peak": hbm_peak, "unit": "GB/s"},
             "kernel_share": shares,
             "adjoint": adj,
+            "autotune": {k.split("|", 1)[1]: {"variant": e["variant"], "ms": [round(m, 4) for m in e["ms"]]}
+                         for k, e in tuned.items()},
             "clocks": clk.summary(sm_max),
             "cpu_baseline": base,
         }
