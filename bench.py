@@ -21,6 +21,10 @@ e2e    = the same through the public streaming API (run_piv_batch_stream)
          the timed region, the copies of batch k+1 overlapping the analysis of
          batch k; time per batch = total / K.
 
+rms_px is the RMS error of all final-pass vectors against the synthetic
+truth; fp64_oracle_error the device's deviation from the oracle's FP64 run
+on the CPU baseline's sample pairs (vectors valid in both).
+
 Before timing, the correlation kernel's CTA shape of every pass class is
 chosen on the device by the autotuner (hammerhead_b200.autotune; the choices
 and the per-shape times appear as "autotune"; --no-autotune keeps the
@@ -182,14 +186,17 @@ def workload_name(w):
             "vortex": "1024x1024 Lamb-Oseen vortex, [64,32,16] padded+gauss, final 3 sweeps + UQ"}[w]
 
 
-def cpu_baseline(hb, pairs, budget_s=20.0):
-    """The oracle (CPU restatement, all host threads) on a bounded sample."""
+def cpu_baseline(hb, pairs, results=None, budget_s=20.0):
+    """The oracle (CPU restatement, all host threads) on a bounded sample;
+    with the device `results` of `pairs`, also the device's error against
+    the oracle's FP64 run of the sample pairs (the checker, untimed)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
     oracle.build()
     threads = os.cpu_count() or 1
-    sample = sorted(pairs, key=lambda p: p["A"].size)[:2]
+    sample_idx = sorted(range(len(pairs)), key=lambda i: pairs[i]["A"].size)[:2]
+    sample = [pairs[i] for i in sample_idx]
     nvec, t_total, runs = 0, 0.0, 0
     t_start = time.perf_counter()
     while time.perf_counter() - t_start < budget_s or runs == 0:
@@ -202,8 +209,20 @@ def cpu_baseline(hb, pairs, budget_s=20.0):
         if runs >= 3:
             break
     desc = ", ".join(f"{p['shape'][0]}x{p['shape'][1]} {p['schedule']}" for p in sample)
+    fp64 = None
+    if results is not None:
+        diffs = []
+        for i in sample_idx:
+            p, r = pairs[i], results[i]
+            o = oracle.run_piv(p["A"], p["B"], p["passes"], nthreads=threads, dtype=np.float64)
+            ok = ~(r.outliers | r.mask | o["outliers"] | o["mask"])
+            diffs.append(np.abs(r.u - o["u"])[ok])
+            diffs.append(np.abs(r.v - o["v"])[ok])
+        d = np.concatenate(diffs).astype(np.float64)
+        fp64 = {"sample": desc, "components": int(d.size), "max_abs_px": float(d.max()),
+                "p999_abs_px": float(np.quantile(d, 0.999)), "rms_px": float(np.sqrt(np.mean(d * d)))}
     return {"value": nvec / t_total, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{runs}x [{desc}] (oracle, float32, {threads} threads)"}
+            "sample": f"{runs}x [{desc}] (oracle, float32, {threads} threads)", "fp64_oracle_error": fp64}
 
 
 def adjoint_bench(hb, ws, torch, stream, dev_time, reps):
@@ -312,7 +331,7 @@ def main():
     for _ in range(args.warmup):
         step()
     runner.run()
-    results = runner.results(copy=False)
+    results = runner.results(copy=True)
     rms = [hb.rms_error(r, p["flow"]) for r, p in zip(results, pairs)]
     rms_all = float(np.sqrt(np.mean(np.square(rms))))
     launches0 = L.hh_launch_count(ws.ctx)
@@ -384,7 +403,7 @@ def main():
 
     base = None
     if rank == 0 and not args.no_cpu_baseline:
-        base = cpu_baseline(hb, pairs)
+        base = cpu_baseline(hb, pairs, results)
 
     if rank == 0:
         form = "plain (per-pair device schedule)" if args.plain else \
@@ -401,6 +420,7 @@ def main():
                 "value": nvec_total / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
                 "batched_speedup": plain_ms / ms_max},
             "rms_px": rms_all,
+            "fp64_oracle_error": base.pop("fp64_oracle_error") if base else None,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
