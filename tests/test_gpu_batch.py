@@ -309,3 +309,19 @@ def test_pipelined_paths_with_static_masks(hb, ws):
     assert piped[0].mask.any()
     with pytest.raises(hb.DimensionMismatch):
         hb.run_piv_batch_stream(batches, sched, masks=masks[:3], workspace=ws)
+
+
+def test_batch_stream_error_leaves_session_usable(hb, ws):
+    # a batch whose pair changed size raises DimensionMismatch; the cached
+    # session of the composition stays usable for the next stream
+    s1, s2 = _schedules(hb)
+    sched = [s1, s2, s2, s1]
+    good = [_mixed(hb, n=4, seed=900 + 10 * k)[0] for k in range(2)]
+    bad = list(good[1])
+    bad[2] = (bad[2][0][:-8], bad[2][1][:-8])
+    with pytest.raises(hb.DimensionMismatch):
+        hb.run_piv_batch_stream([good[0], bad, good[1]], sched, workspace=ws)
+    out = hb.run_piv_batch_stream(good, sched, workspace=ws)
+    for k in range(2):
+        for a, b in zip(out[k], hb.run_piv_batch(good[k], sched, workspace=ws)):
+            _same(a, b)
