@@ -241,6 +241,33 @@ function run_piv_ensemble_b200(pairs::AbstractVector{<:Tuple{AbstractMatrix{<:Re
     return PIVResult(x, y, u, v, ratio, moment, su, sv, BitMatrix(outl .!= 0), BitMatrix(gm .!= 0), final)
 end
 
+# ---- autotuning of the correlation kernel's CTA shape ---------------------
+# Times the shapes of every equal-area pass class of `passes` on the pair
+# (imgA, imgB) and makes the fastest the context's choice; returns
+# [(fft_size, window, variant, ms per shape)].
+function autotune_b200!(ctx::Context, imgA::AbstractMatrix{<:Real}, imgB::AbstractMatrix{<:Real},
+                        passes::AbstractVector{PIVParameters}; reps::Integer = 5)
+    A = Matrix{Float32}(imgA)
+    B = Matrix{Float32}(imgB)
+    size(A) == size(B) || throw(DimensionMismatch("images must have the same size"))
+    check(ccall((:hh_stage_pair, LIB), Int32, (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Int64, Int64),
+                ctx.ptr, A, B, size(A, 1), size(A, 2)), ctx.ptr)
+    out = Tuple{Int,Int,Int,Vector{Float32}}[]
+    for p in passes
+        p.search_area_size == p.window_size || continue
+        w = p.window_size[1]
+        n = p.padding ? 2w : w
+        any(o -> o[1] == n && o[2] == w, out) && continue
+        ms = zeros(Float32, 2)  # HH_CORR_VARIANTS
+        best = Ref{Int32}(0)
+        check(ccall((:hh_autotune_correlation, LIB), Int32,
+                    (Ptr{Cvoid}, Ref{PassDesc}, Int32, Ptr{Float32}, Ref{Int32}),
+                    ctx.ptr, pass_desc(p), reps, ms, best), ctx.ptr)
+        push!(out, (n, w, Int(best[]), ms))
+    end
+    return out
+end
+
 # ---- differentiable correlation loss (hh_ncc_loss_grad) -------------------
 # A staged pair on a context; P is (gny, gnx, 2) Float32 (u, v) on nodes
 # y0 .+ ysp .* (0:gny-1), x0 .+ xsp .* (0:gnx-1).
