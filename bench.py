@@ -142,22 +142,53 @@ class ClockSampler:
 
 
 # --- reference arm: the CPU restatement on the host cores -----------------------------
-def run_reference(args, hb):
+def _load_synthetic():
+    """The synthetic-pair generator (pure numpy) without importing the device
+    package, so that the CPU-only reference arm loads no device library."""
+    import importlib.util
+
+    path = os.path.join(ROOT, "hammerhead.jl_b200", "hammerhead_b200", "synthetic.py")
+    spec = importlib.util.spec_from_file_location("_hh_synthetic", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def oracle_schedule(oracle, kind, uq=True):
+    final = dict(max_iterations=3, uncertainty=uq)
+    sizes = {"64-32-16": [64, 32, 16], "48-24": [48, 24]}[kind]
+    return oracle.multipass(sizes, padding=True, apodization="gauss", final=final)
+
+
+def size_sample(specs):
+    """A bounded sample of the workload with its size mix: the first pair of
+    each image size (512x512, 768x1024, 2048x2048), with its own schedule."""
+    seen, idx = set(), []
+    for i, sp in enumerate(specs):
+        if tuple(sp["shape"]) not in seen:
+            seen.add(tuple(sp["shape"]))
+            idx.append(i)
+    return idx
+
+
+def run_reference(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
     oracle.build()
+    syn = _load_synthetic()
     threads = os.cpu_count() or 1
-    pairs = make_workload(hb, args.workload, limit=None)
-    # a bounded sample per step: one pair of each image size present
-    seen, sample = set(), []
-    for p in pairs:
-        if p["shape"] not in seen and p["shape"][0] <= 1024:
-            seen.add(p["shape"])
-            sample.append(p)
-    if not sample:
-        sample = pairs[:1]
-    nvec = sum(final_vectors(hb, p) for p in sample)
+    if args.workload == "batch64":
+        specs = syn.config3_pairs(seed0=1003)
+    else:
+        specs = [dict(shape=(1024, 1024), flow=syn.lamb_oseen_flow((512.5, 512.5), 80.0, 8.0),
+                      schedule="64-32-16", seed=1001)]
+    sample = []
+    for i in size_sample(specs):
+        sp = specs[i]
+        A, B = syn.particle_pair(sp["shape"], sp["flow"], seed=sp["seed"])
+        sample.append(dict(sp, A=A, B=B, passes=oracle_schedule(oracle, sp["schedule"])))
+    nvec = sum(oracle.final_vectors(p["A"].shape, p["passes"]) for p in sample)
     for _ in range(args.warmup):
         for p in sample:
             oracle.run_piv(p["A"], p["B"], p["passes"], nthreads=threads)
@@ -173,7 +204,8 @@ def run_reference(args, hb):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_name(args.workload), "sample": desc},
+            "config": {"workload": workload_name(args.workload),
+                       "sample": f"one pair of each image size per step: {desc} ({nvec} final-pass vectors)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{len(sample)} pairs per step ({desc}), {nvec} final-pass vectors"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -195,7 +227,7 @@ def cpu_baseline(hb, pairs, results=None, budget_s=20.0):
 
     oracle.build()
     threads = os.cpu_count() or 1
-    sample_idx = sorted(range(len(pairs)), key=lambda i: pairs[i]["A"].size)[:2]
+    sample_idx = size_sample(pairs)
     sample = [pairs[i] for i in sample_idx]
     nvec, t_total, runs = 0, 0.0, 0
     t_start = time.perf_counter()
@@ -204,7 +236,7 @@ def cpu_baseline(hb, pairs, results=None, budget_s=20.0):
             t0 = time.perf_counter()
             oracle.run_piv(p["A"], p["B"], p["passes"], nthreads=threads)
             t_total += time.perf_counter() - t0
-            nvec += final_vectors(hb, p)
+            nvec += oracle.final_vectors(p["A"].shape, p["passes"])
         runs += 1
         if runs >= 3:
             break
@@ -260,16 +292,18 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default correlation CTA shapes")
     args = ap.parse_args()
 
-    import hammerhead_b200 as hb
-
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-
     if args.impl == "reference":
+        # CPU only: the reference algorithm (oracle/) on the host cores; the
+        # device package is not imported
         if rank == 0:
-            run_reference(args, hb)
+            run_reference(args)
         return
+
+    import hammerhead_b200 as hb
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
 
     import torch
     import torch.distributed as dist

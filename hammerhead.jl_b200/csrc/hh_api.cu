@@ -189,11 +189,13 @@ hh_status run_schedule(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr
       ca.rec = prec;
       ca.win = p.search[0] != W ? W : 0;
       ca.variant = corr_variant(ctx, p);
-      HH_K(HH_K_CORRELATE, 1, corr_flops(N, njobs), corr_bytes(p.search[0], nalt, njobs), njobs,
-           hh::launch_correlate(ca, N, p.search[0], s, ctx->num_sms));
+      if (!corr_special(p)) HH_TRY(gcorr_prepare(ctx, p, ca));
+      HH_K(HH_K_CORRELATE, 1, corr_flops(p, njobs), corr_bytes(p, nalt, njobs), njobs, corr_launch(ctx, p, ca, s));
       if (fused_unc) {
         hh::UQArgs ua{srcA, srcB, dmask, nr, djobs, njobs, ny, W, tb.apod, nullptr, uncu, uncv};
-        HH_K(HH_K_UQ, 1, uq_flops(W, njobs), 8.0 * W * W * njobs, njobs, hh::launch_uq(ua, s, ctx->num_sms));
+        HH_TRY(uq_prepare(ctx, p.window[0], p.window[1], ua));
+        HH_K(HH_K_UQ, 1, uq_flops(p, njobs), 8.0 * p.window[0] * p.window[1] * njobs, njobs,
+             hh::launch_uq(ua, s, ctx->num_sms));
       }
       HH_K(HH_K_VECTOR, 1, 0, (28 + 8 * nalt) * G, G, hh::launch_combine(u, v, resu, resv, ratio, moment, nalt > 0 ? altu : nullptr, nalt > 0 ? altv : nullptr,
                                nalt, g.any_mask ? gm : nullptr, G, keep_measured ? measu : nullptr,
@@ -237,7 +239,9 @@ hh_status run_schedule(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr
     }
     if (unc && !fused_unc) {
       hh::UQArgs ua{srcA, srcB, dmask, nr, djobs, njobs, ny, W, tb.apod, nullptr, uncu, uncv};
-      HH_K(HH_K_UQ, 1, uq_flops(W, njobs), 8.0 * W * W * njobs, njobs, hh::launch_uq(ua, s, ctx->num_sms));
+      HH_TRY(uq_prepare(ctx, p.window[0], p.window[1], ua));
+      HH_K(HH_K_UQ, 1, uq_flops(p, njobs), 8.0 * p.window[0] * p.window[1] * njobs, njobs,
+           hh::launch_uq(ua, s, ctx->num_sms));
     }
     if (keep_measured) HH_K(HH_K_VECTOR, 1, 0, 20 * G, G, hh::launch_restore_measured(u, v, measu, measv, outl, G, s));
     ctx->pass_sweeps[k] = sweeps;
@@ -334,22 +338,15 @@ hh_status hh_check_backend_params(const hh_pass_desc* passes, int32_t npasses) {
     if (p.keep_correlation_planes)
       return fail(ctx, HH_ERR_UNSUPPORTED,
                   "backend :b200 does not support keep_correlation_planes yet; use backend = :cpu");
-    if (p.window[0] != p.window[1])
-      return fail(ctx, HH_ERR_UNSUPPORTED, "backend :b200 supports square windows only, got window_size=" + tup(p.window));
-    if (p.search[0] != p.search[1])
+    // every window and search-area shape runs: the fused kernels where one
+    // exists, the general-shape kernel otherwise (FFT lengths whose prime
+    // factors are at most 61, planes up to 4 M points)
+    if (!corr_special(p) && !gcorr_shape_ok(p))
       return fail(ctx, HH_ERR_UNSUPPORTED,
-                  "backend :b200 supports square search areas only, got search_area_size=" + tup(p.search));
-    const int N = fft_size(p), W = p.window[0], S = p.search[0];
-    if (S != W && !hh::correlate_supported(N, S))
-      return fail(ctx, HH_ERR_UNSUPPORTED,
-                  "backend :b200 has no correlation kernel for search area " + std::to_string(S) +
-                      (p.padding ? " padded" : "") + " (FFT size " + std::to_string(N) +
-                      "); supported search areas: 16, 24, 32, 48, 64 (padded), 16, 24, 32, 48, 64, 96, 128 (unpadded)");
-    if (S == W && !hh::correlate_supported(N, W))
-      return fail(ctx, HH_ERR_UNSUPPORTED,
-                  "backend :b200 has no correlation kernel for window " + std::to_string(W) +
-                      (p.padding ? " padded" : "") + " (FFT size " + std::to_string(N) +
-                      "); supported windows: 8, 12, 16, 24, 32, 48, 64 (padded), 16, 24, 32, 48, 64, 96, 128 (unpadded)");
+                  "backend :b200 has no correlation kernel for an FFT plane of " + std::to_string(fft_rows(p)) + " x " +
+                      std::to_string(fft_cols(p)) + " (window_size=" + tup(p.window) + ", search_area_size=" +
+                      tup(p.search) + (p.padding ? ", padded" : "") +
+                      "): FFT lengths need prime factors of at most 61 and planes at most 4194304 points");
     if (p.n_peaks > hh::KMAX)
       return fail(ctx, HH_ERR_UNSUPPORTED,
                   "backend :b200 locates at most " + std::to_string(hh::KMAX) + " peaks, got n_peaks=" + std::to_string(p.n_peaks));
@@ -358,8 +355,6 @@ hh_status hh_check_backend_params(const hh_pass_desc* passes, int32_t npasses) {
     for (int q = 0; q < p.n_validators; ++q)
       if (p.validators[q].kind == HH_VAL_UOD && p.validators[q].neighborhood > 4)
         return fail(ctx, HH_ERR_UNSUPPORTED, "backend :b200 supports UOD neighborhood_size <= 4");
-    if (p.uncertainty && W > 64)
-      return fail(ctx, HH_ERR_UNSUPPORTED, "backend :b200 supports uncertainty for windows up to 64 px");
   }
   return HH_OK;
 }
@@ -514,6 +509,7 @@ hh_status hh_stage_pair(hh_ctx* ctx, const float* A, const float* B, int64_t nr,
   ctx->curA = dA;
   ctx->curB = dB;
   ctx->staged = true;
+  ctx->hook_mask = nullptr;  // a new pair starts unmasked (hh_stage_mask)
   return HH_OK;
 }
 
@@ -627,15 +623,15 @@ hh_status hh_apply_predictor(hh_ctx* ctx, const float* pu, const float* pv, int3
 }
 
 // Jobs of a hook call (1-based, from the caller) checked and copied to the
-// device 0-based; m is the margin of an enlarged search area around each
-// window.
-static hh_status hook_jobs(hh_ctx* ctx, const int32_t* jobs, int64_t njobs, int64_t nr, int64_t nc, int W,
-                           int32_t** djobs_out, int32_t* ny_out, int m = 0) {
+// device 0-based; the window is wr x wc and (mr, mc) the margins of an
+// enlarged search area around it.
+static hh_status hook_jobs(hh_ctx* ctx, const int32_t* jobs, int64_t njobs, int64_t nr, int64_t nc, int wr, int wc,
+                           int32_t** djobs_out, int32_t* ny_out, int mr = 0, int mc = 0) {
   std::vector<int32_t> hj((size_t)4 * njobs);
   int32_t ny = 1;
   for (int64_t k = 0; k < njobs; ++k) {
     const int32_t gi = jobs[4 * k] - 1, gj = jobs[4 * k + 1] - 1, rs = jobs[4 * k + 2] - 1, cs = jobs[4 * k + 3] - 1;
-    if (rs - m < 0 || cs - m < 0 || rs + W + m > nr || cs + W + m > nc || gi < 0 || gj < 0)
+    if (rs - mr < 0 || cs - mc < 0 || rs + wr + mr > nr || cs + wc + mc > nc || gi < 0 || gj < 0)
       return fail(ctx, HH_ERR_ARG, "job " + std::to_string(k + 1) + " lies outside the image");
     hj[4 * k] = gi;
     hj[4 * k + 1] = gj;
@@ -659,10 +655,12 @@ static hh_status hook_correlate(hh_ctx* ctx, const hh_pass_desc* p, const int32_
   HH_TRY(check_passes(ctx, p, 1));
   if (njobs <= 0) return HH_OK;
   cudaStream_t s = ctx->stream;
-  const int W = p->window[0], N = fft_size(*p), K = std::max(p->n_peaks, 2);
+  const int W = p->window[0], K = std::max(p->n_peaks, 2);
+  const int64_t PL = (int64_t)fft_rows(*p) * fft_cols(*p);  // plane size
   int32_t* dj;
   int32_t ny;
-  HH_TRY(hook_jobs(ctx, jobs, njobs, ctx->nr, ctx->nc, W, &dj, &ny, (p->search[0] - W) / 2));
+  HH_TRY(hook_jobs(ctx, jobs, njobs, ctx->nr, ctx->nc, p->window[0], p->window[1], &dj, &ny,
+                   (p->search[0] - p->window[0]) / 2, (p->search[1] - p->window[1]) / 2));
   Tables tb;
   HH_TRY(get_tables(ctx, *p, tb));
   float *dpk = nullptr, *dpl = nullptr;
@@ -670,7 +668,7 @@ static hh_status hook_correlate(hh_ctx* ctx, const hh_pass_desc* p, const int32_
   double* duq = nullptr;
   if (out) HH_TRY(buf(ctx, "hook_packed", (size_t)(5 + 2 * (K - 1)) * njobs, &dpk));
   if (locs) HH_TRY(buf(ctx, "hook_locs", (size_t)2 * K * njobs, &dlc));
-  if (planes) HH_TRY(buf(ctx, "hook_planes", (size_t)N * N * njobs, &dpl));
+  if (planes) HH_TRY(buf(ctx, "hook_planes", (size_t)PL * njobs, &dpl));
   float* drec;
   HH_TRY(buf(ctx, "hook_rec", hh::correlate_record_words(p->n_peaks) * njobs, &drec));
   CorrArgs ca{};
@@ -690,23 +688,42 @@ static hh_status hook_correlate(hh_ctx* ctx, const hh_pass_desc* p, const int32_
   ca.npeaks = p->n_peaks;
   ca.finder = p->peak_finder;
   ca.subpixel = p->subpixel;
+  ca.mask = ctx->hook_mask;
   ca.packed = dpk;
   ca.locs = dlc;
   ca.planes = dpl;
   ca.rec = drec;
   ca.win = p->search[0] != W ? W : 0;
   ca.variant = corr_variant(ctx, *p);
-  HH_K(HH_K_CORRELATE, 1, 0, 0, 0, hh::launch_correlate(ca, N, p->search[0], s, ctx->num_sms));
+  if (!corr_special(*p)) HH_TRY(gcorr_prepare(ctx, *p, ca));
+  HH_K(HH_K_CORRELATE, 1, 0, 0, 0, corr_launch(ctx, *p, ca, s));
   if (uq) {
     HH_TRY(buf(ctx, "hook_uq", (size_t)88 * njobs, &duq));
-    hh::UQArgs ua{ctx->curA, ctx->curB, nullptr, ctx->nr, dj, njobs, ny, W, tb.apod, duq, nullptr, nullptr};
+    hh::UQArgs ua{ctx->curA, ctx->curB, ctx->hook_mask, ctx->nr, dj, njobs, ny, W, tb.apod, duq, nullptr, nullptr};
+    HH_TRY(uq_prepare(ctx, p->window[0], p->window[1], ua));
     HH_K(HH_K_UQ, 1, 0, 0, 0, hh::launch_uq(ua, s, ctx->num_sms));
     HH_CK(cudaMemcpyAsync(uq, duq, (size_t)88 * njobs * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
   if (out) HH_CK(cudaMemcpyAsync(out, dpk, (size_t)(5 + 2 * (K - 1)) * njobs * sizeof(float), cudaMemcpyDeviceToHost, s));
   if (locs) HH_CK(cudaMemcpyAsync(locs, dlc, (size_t)2 * K * njobs * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  if (planes) HH_CK(cudaMemcpyAsync(planes, dpl, (size_t)N * N * njobs * sizeof(float), cudaMemcpyDeviceToHost, s));
+  if (planes) HH_CK(cudaMemcpyAsync(planes, dpl, (size_t)PL * njobs * sizeof(float), cudaMemcpyDeviceToHost, s));
   HH_CK(cudaStreamSynchronize(s));
+  return HH_OK;
+}
+
+hh_status hh_stage_mask(hh_ctx* ctx, const uint8_t* mask) {
+  if (!ctx) return fail(nullptr, HH_ERR_ARG, "context is NULL");
+  HH_TRY(set_device(ctx));
+  if (!ctx->staged) return fail(ctx, HH_ERR_STATE, "no staged pair: call hh_stage_pair first");
+  if (!mask) {
+    ctx->hook_mask = nullptr;
+    return HH_OK;
+  }
+  uint8_t* dm;
+  HH_TRY(buf(ctx, "hook_mask", (size_t)(ctx->nr * ctx->nc), &dm));
+  HH_CK(cudaMemcpyAsync(dm, mask, (size_t)(ctx->nr * ctx->nc), cudaMemcpyHostToDevice, ctx->stream));
+  HH_CK(cudaStreamSynchronize(ctx->stream));
+  ctx->hook_mask = dm;
   return HH_OK;
 }
 
@@ -964,6 +981,8 @@ static void drop_plans(hh_ctx* ctx) {  // batched graphs captured with an older 
   ctx->bplans.clear();
 }
 
+extern "C" int32_t hh_corr_fused(const hh_pass_desc* p) { return p && corr_special(*p) ? 1 : 0; }
+
 extern "C" hh_status hh_set_corr_variant(hh_ctx* ctx, int32_t fft_size_, int32_t window, int32_t variant) {
   if (!ctx) return fail(nullptr, HH_ERR_ARG, "context is NULL");
   if (variant < 0 || variant >= HH_CORR_VARIANTS)
@@ -989,6 +1008,9 @@ extern "C" hh_status hh_autotune_correlation(hh_ctx* ctx, const hh_pass_desc* p,
   if (cs != HH_OK) return fail(ctx, cs, hh_last_error(nullptr));
   if (p->search[0] != p->window[0])
     return fail(ctx, HH_ERR_ARG, "autotuning covers passes with equal window and search area");
+  if (!corr_special(*p))
+    return fail(ctx, HH_ERR_ARG, "autotuning covers the fused correlation kernels (square windows of the specialised "
+                                 "sizes); the general-shape kernel has one shape");
   if (reps < 1) return fail(ctx, HH_ERR_ARG, "reps must be at least 1, got " + std::to_string(reps));
   Grid g;
   HH_TRY(make_grid(ctx, ctx->nr, ctx->nc, *p, nullptr, 0.5, g));

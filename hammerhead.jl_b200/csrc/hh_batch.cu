@@ -19,10 +19,14 @@ namespace hhd {
 
 struct BClass {
   int N = 0, W = 0, S = 0, method = 0, npeaks = 1, finder = 0, subpixel = 0, apod = 0, padding = 0;  // S: search area
+  hh_pass_desc pd{};  // a pass of this class (its shape and options)
+  bool special = true;  // a fused kernel exists; else the general-shape kernel (fields in gen)
+  CorrArgs gen{};
   Tables tb;
   std::vector<int32_t> hjobs;
   int32_t* jobs = nullptr;
   int64_t njobs = 0;
+  std::vector<int64_t> pair_jobs;  // jobs of each pair in this class
   bool unc_fused = false, unc_post = false;
 };
 
@@ -50,9 +54,12 @@ struct BPlan {
   uint8_t* h_gmask = nullptr; // pinned grid-mask staging (nslots * gcap), when masks
   int32_t* d_done = nullptr;
   int32_t* d_sweeps = nullptr;
+  int32_t* d_slot_sweeps = nullptr;  // nslots x npairs: sweeps run by each pair in each slot
   uint8_t* d_gmask = nullptr;
   float *warpA = nullptr, *warpB = nullptr, *coefA = nullptr, *coefB = nullptr, *dbuf = nullptr;
   float* rec = nullptr;  // peak records of a correlation launch
+  float2* gscr = nullptr;  // general-shape correlation scratch (plan-owned: captured graphs keep the pointer)
+  double* uqscr = nullptr; // general-form uncertainty scratch
   float *stageA = nullptr, *stageB = nullptr;
   uint16_t *stage16A = nullptr, *stage16B = nullptr;  // host UInt16 frames before conversion
   uint8_t* stageM = nullptr;
@@ -63,6 +70,15 @@ struct BPlan {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int64_t graph_launches = 0;
+  // profiled runs: the launches whose algorithmic work depends on which
+  // pairs are live (converged pairs and pairs without the slot are skipped
+  // by the kernels); their charge is recomputed from the sweeps each pair
+  // ran once the run has finished
+  struct Charge {
+    size_t pending;  // index into ctx->pending
+    int cls, slot, it, jclass, mode;
+  };
+  std::vector<Charge> charges;
 };
 
 static void free_plan(void* vp) {
@@ -235,6 +251,7 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
   HH_TRY(plan_alloc(ctx, P, 2 * Q, &P.dbuf));
   HH_TRY(plan_alloc(ctx, P, (size_t)npairs, &P.d_done));
   HH_TRY(plan_alloc(ctx, P, (size_t)npairs, &P.d_sweeps));
+  HH_TRY(plan_alloc(ctx, P, (size_t)npairs * std::max(P.nslots, 1), &P.d_slot_sweeps));
   HH_TRY(plan_alloc(ctx, P, (size_t)nslots * npairs, &P.d_tables));
   hh::BResult& r = P.r;
   float** rf[] = {&r.u, &r.v, &r.ratio, &r.moment, &r.unc_u, &r.unc_v};
@@ -251,7 +268,7 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
   P.slots.resize(nslots);
   for (int k = 0; k < nslots; ++k) {
     BSlot& S = P.slots[k];
-    std::map<std::tuple<int, int, int, int, int, int, int, int>, int> cls;
+    std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int, int>, int> cls;
     int64_t coff = 0, pcoff = 0;
     for (int p = 0; p < npairs; ++p) {
       const hh_batch_pair& q = pairs[p];
@@ -336,7 +353,8 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
       S.any_deform |= deforms[p] != 0;
       S.any_pred0 |= k > 0;
       // job class of this pass
-      const auto key = std::make_tuple(fft_size(pd), (int)pd.window[0], (int)pd.method, (int)pd.n_peaks,
+      const auto key = std::make_tuple(fft_rows(pd), fft_cols(pd), (int)pd.window[0], (int)pd.window[1],
+                                       (int)pd.search[0], (int)pd.search[1], (int)pd.method, (int)pd.n_peaks,
                                        (int)pd.peak_finder, (int)pd.subpixel, (int)pd.apodization, (int)pd.padding);
       auto it = cls.find(key);
       if (it == cls.end()) {
@@ -351,12 +369,17 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
         c.subpixel = pd.subpixel;
         c.apod = pd.apodization;
         c.padding = pd.padding;
+        c.pd = pd;
+        c.special = corr_special(pd);
+        if (!c.special) HH_TRY(gcorr_setup(ctx, pd, c.gen));
         HH_TRY(get_tables(ctx, pd, c.tb));
         S.classes.push_back(std::move(c));
       }
       BClass& c = S.classes[it->second];
       c.unc_fused |= b.unc_fused != 0;
       c.unc_post |= b.unc_post != 0;
+      c.pair_jobs.resize(npairs, 0);
+      c.pair_jobs[p] += (int64_t)gr.jobs.size() / 4;
       for (size_t j = 0; j + 3 < gr.jobs.size(); j += 4) {
         c.hjobs.push_back(p);
         c.hjobs.push_back(gr.jobs[j] | (gr.jobs[j + 1] << 16));
@@ -378,10 +401,17 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
   }
   // peak records of the largest correlation launch (launches of a sweep run
   // one after another on the stream, so they share it)
-  size_t recw = 0;
+  size_t recw = 0, gw = 0, uw = 0;
   for (const auto& S : P.slots)
-    for (const auto& c : S.classes) recw = std::max(recw, (size_t)c.njobs * hh::correlate_record_words(c.npeaks));
+    for (const auto& c : S.classes) {
+      recw = std::max(recw, (size_t)c.njobs * hh::correlate_record_words(c.npeaks));
+      if (!c.special) gw = std::max(gw, (size_t)(c.gen.gscr_slices * c.gen.gscr_stride));
+      if ((c.unc_fused || c.unc_post) && hh::uq_general(c.pd.window[0], c.pd.window[1]))
+        uw = std::max(uw, (size_t)(4 * ctx->num_sms) * hh::uq_general_stride(c.pd.window[0], c.pd.window[1]));
+    }
   HH_TRY(plan_alloc(ctx, P, recw, &P.rec));
+  if (gw) HH_TRY(plan_alloc(ctx, P, gw, &P.gscr));
+  if (uw) HH_TRY(plan_alloc(ctx, P, uw, &P.uqscr));
   return HH_OK;
 }
 
@@ -391,6 +421,12 @@ static hh_status issue(hh_ctx* ctx, BPlan& P) {
   const int np = P.npairs;
   const hh::BGrid& g = P.g;
   HH_CK(cudaMemsetAsync(P.d_sweeps, 0, np * sizeof(int32_t), s));
+  HH_CK(cudaMemsetAsync(P.d_slot_sweeps, 0, (size_t)np * P.nslots * sizeof(int32_t), s));
+  P.charges.clear();
+  // remember the profiled launch just issued for the live-work charge
+  auto charge = [&](int cls, int slot, int it, int jclass, int mode) {
+    if (ctx->prof && !ctx->pending.empty()) P.charges.push_back({ctx->pending.size() - 1, cls, slot, it, jclass, mode});
+  };
   if (P.qtot > 0) {
     const double px = (double)P.wtot;
     HH_K(HH_K_PREFILTER, 10, 24 * px, 16 * px, (int64_t)px,
@@ -405,11 +441,17 @@ static hh_status issue(hh_ctx* ctx, BPlan& P) {
     HH_CK(cudaMemsetAsync(P.d_done, 0, np * sizeof(int32_t), s));
     for (int it = 1; it <= S.max_maxit; ++it) {
       HH_K(HH_K_VECTOR, 1, 0, 8 * Gs, S.gtot,
-           hh::launch_b_sweep_begin(T, np, P.d_done, it, S.gtot, pu, pv, g.u, g.v, g.unc_u, g.unc_v, P.d_sweeps, s));
-      if (S.any_deform && (it > 1 || S.any_pred0))
+           hh::launch_b_sweep_begin(T, np, P.d_done, it, S.gtot, pu, pv, g.u, g.v, g.unc_u, g.unc_v, P.d_sweeps,
+                                    P.d_slot_sweeps + (size_t)k * np, s));
+      charge(HH_K_VECTOR, k, it, -1, 0);
+      if (S.any_deform && (it > 1 || S.any_pred0)) {
         HH_K(HH_K_DEFORM, 1, 120 * Ps, 16 * Ps, S.ptot, hh::launch_b_deform(T, np, P.d_done, it, S.ptot, pu, pv, s));
-      for (const BClass& c : S.classes) {
-        CorrArgs ca{};
+        charge(HH_K_DEFORM, k, it, -1, 0);
+      }
+      for (size_t ci = 0; ci < S.classes.size(); ++ci) {
+        const BClass& c = S.classes[ci];
+        CorrArgs ca = c.gen;  // general-shape fields (zero for the fused kernels)
+        ca.gscr = P.gscr;
         ca.jobs = c.jobs;
         ca.njobs = c.njobs;
         ca.apod = c.tb.apod;
@@ -437,11 +479,13 @@ static hh_status issue(hh_ctx* ctx, BPlan& P) {
           auto cv = ctx->corr_var.find({c.N, c.S});
           ca.variant = cv == ctx->corr_var.end() ? 0 : cv->second;
         }
-        HH_K(HH_K_CORRELATE, 1, corr_flops(c.N, c.njobs), corr_bytes(c.S, c.npeaks - 1, c.njobs), c.njobs,
-             hh::launch_correlate(ca, c.N, c.S, s, ctx->num_sms));
+        HH_K(HH_K_CORRELATE, 1, corr_flops(c.pd, c.njobs), corr_bytes(c.pd, c.npeaks - 1, c.njobs), c.njobs,
+             corr_launch(ctx, c.pd, ca, s));
+        charge(HH_K_CORRELATE, k, it, (int)ci, 0);
       }
       if (it == 1)
-        for (const BClass& c : S.classes)
+        for (size_t ci = 0; ci < S.classes.size(); ++ci) {
+          const BClass& c = S.classes[ci];
           if (c.unc_fused) {
             hh::UQArgs ua{};
             ua.jobs = c.jobs;
@@ -453,18 +497,27 @@ static hh_status issue(hh_ctx* ctx, BPlan& P) {
             ua.bp = T;
             ua.done = P.d_done;
             ua.mode = 0;
-            HH_K(HH_K_UQ, 1, uq_flops(c.W, c.njobs), 8.0 * c.W * c.W * c.njobs, c.njobs, hh::launch_uq(ua, s, ctx->num_sms));
+            uq_setup(ctx, c.pd.window[0], c.pd.window[1], ua);
+            ua.gscr = P.uqscr;
+            HH_K(HH_K_UQ, 1, uq_flops(c.pd, c.njobs), 8.0 * c.pd.window[0] * c.pd.window[1] * c.njobs, c.njobs,
+                 hh::launch_uq(ua, s, ctx->num_sms));
+            charge(HH_K_UQ, k, 1, (int)ci, 0);
           }
+        }
       const bool fc = S.any_tol && it >= 2 && it < S.max_maxit;
       const int nv = 2 + S.any_nalt + S.any_replace + fc;
       HH_K(HH_K_VECTOR, nv, 0, 120 * Gs, S.gtot,
            hh::launch_b_vector(T, np, P.d_done, it, S.gtot, g, S.any_nalt, S.any_replace, S.any_tol, S.max_maxit, s,
                                nullptr));
-      if (it < S.max_maxit)
+      charge(HH_K_VECTOR, k, it, -1, 1);
+      if (it < S.max_maxit) {
         HH_K(HH_K_VECTOR, P.smoothing ? 2 : 1, 0, 24 * Gs, S.gtot,
              hh::launch_b_predictor(T, np, P.d_done, it, 0, S.gtot, g, P.smoothing, s, nullptr));
+        charge(HH_K_VECTOR, k, it, -1, 2);
+      }
     }
-    for (const BClass& c : S.classes)
+    for (size_t ci = 0; ci < S.classes.size(); ++ci) {
+      const BClass& c = S.classes[ci];
       if (c.unc_post) {
         hh::UQArgs ua{};
         ua.jobs = c.jobs;
@@ -476,14 +529,67 @@ static hh_status issue(hh_ctx* ctx, BPlan& P) {
         ua.bp = T;
         ua.done = P.d_done;
         ua.mode = 1;
-        HH_K(HH_K_UQ, 1, uq_flops(c.W, c.njobs), 8.0 * c.W * c.W * c.njobs, c.njobs, hh::launch_uq(ua, s, ctx->num_sms));
+        uq_setup(ctx, c.pd.window[0], c.pd.window[1], ua);
+        ua.gscr = P.uqscr;
+        HH_K(HH_K_UQ, 1, uq_flops(c.pd, c.njobs), 8.0 * c.pd.window[0] * c.pd.window[1] * c.njobs, c.njobs,
+             hh::launch_uq(ua, s, ctx->num_sms));
+        charge(HH_K_UQ, k, 0, (int)ci, 1);
       }
+    }
     if (S.any_keep) HH_K(HH_K_VECTOR, 1, 0, 20 * Gs, S.gtot, hh::launch_b_restore(T, np, S.gtot, g, s));
     if (S.any_next)
       HH_K(HH_K_VECTOR, P.smoothing ? 2 : 1, 0, 24 * Gs, S.gtot,
            hh::launch_b_predictor(T, np, P.d_done, S.max_maxit, 1, S.gtot, g, P.smoothing, s, nullptr));
   }
   HH_K(HH_K_VECTOR, 1, 0, 50.0 * P.rtot, P.rtot, hh::launch_b_gather(P.d_tables, np, P.rtot, g, P.r, s));
+  return HH_OK;
+}
+
+// Algorithmic work of the profiled launches of the last run, counted over
+// the pairs each launch actually served: a pair takes part in sweep `it` of
+// slot k when it has the slot and ran at least `it` sweeps there (converged
+// pairs are skipped by the kernels). Replaces the launch-time charge, which
+// counted every pair of the slot.
+static hh_status recharge_live(hh_ctx* ctx, BPlan& P) {
+  if (P.charges.empty()) return HH_OK;
+  const int np = P.npairs;
+  std::vector<int32_t> sw((size_t)np * P.nslots);
+  HH_CK(cudaMemcpy(sw.data(), P.d_slot_sweeps, sw.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  for (const auto& ch : P.charges) {
+    if (ch.pending >= ctx->pending.size()) continue;
+    auto& q = ctx->pending[ch.pending];
+    const BSlot& S = P.slots[ch.slot];
+    const int32_t* ran = sw.data() + (size_t)ch.slot * np;
+    const BPair* tb = P.tables.data() + (size_t)ch.slot * np;
+    auto live = [&](int p, int it) { return tb[p].live && ran[p] >= it; };
+    double units = 0;
+    if (ch.cls == HH_K_CORRELATE) {
+      const BClass& c = S.classes[ch.jclass];
+      for (int p = 0; p < np && p < (int)c.pair_jobs.size(); ++p)
+        if (live(p, ch.it)) units += (double)c.pair_jobs[p];
+      q.flops = corr_flops(c.pd, (int64_t)units);
+      q.bytes = corr_bytes(c.pd, c.npeaks - 1, (int64_t)units);
+    } else if (ch.cls == HH_K_UQ) {
+      const BClass& c = S.classes[ch.jclass];
+      for (int p = 0; p < np && p < (int)c.pair_jobs.size(); ++p) {
+        const bool on = ch.mode == 0 ? (tb[p].unc_fused && live(p, 1)) : (tb[p].unc_post && tb[p].live);
+        if (on) units += (double)c.pair_jobs[p];
+      }
+      q.flops = uq_flops(c.pd, (int64_t)units);
+      q.bytes = 8.0 * c.pd.window[0] * c.pd.window[1] * units;
+    } else if (ch.cls == HH_K_DEFORM) {
+      for (int p = 0; p < np; ++p)
+        if (live(p, ch.it) && tb[p].deforms && (ch.it > 1 || tb[p].has_pred0)) units += (double)(tb[p].nr * tb[p].nc);
+      q.flops = 120 * units;
+      q.bytes = 16 * units;
+    } else {  // vector-grid stages: cells of the live pairs
+      for (int p = 0; p < np; ++p)
+        if (live(p, ch.it)) units += (double)tb[p].ny * tb[p].nx;
+      q.bytes = (ch.mode == 0 ? 8.0 : ch.mode == 1 ? 120.0 : 24.0) * units;
+    }
+    q.units = (int64_t)units;
+  }
+  P.charges.clear();
   return HH_OK;
 }
 
@@ -689,6 +795,7 @@ hh_status hh_run_batched(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npairs
     if (out->offsets) out->offsets[npairs] = R;
   }
   HH_CK(cudaStreamSynchronize(s));
+  if (ctx->prof) HH_TRY(recharge_live(ctx, *P));
   return flush_profile(ctx);
 }
 

@@ -104,7 +104,7 @@ cudaError_t launch_b_prefilter(const BPair* bp, int npairs, int64_t qtot, int64_
                                float* dbuf, cudaStream_t s);
 cudaError_t launch_b_sweep_begin(const BPair* bp, int npairs, const int32_t* done, int it, int64_t gtot,
                                  const float* pu, const float* pv, float* u, float* v, float* uncu, float* uncv,
-                                 int32_t* sweeps, cudaStream_t s);
+                                 int32_t* sweeps, int32_t* slot_sweeps, cudaStream_t s);
 cudaError_t launch_b_deform(const BPair* bp, int npairs, const int32_t* done, int it, int64_t ptot, const float* pu,
                             const float* pv, cudaStream_t s);
 struct BGrid {  // concatenated grid arrays, indexed by goff + cell

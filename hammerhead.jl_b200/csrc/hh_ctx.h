@@ -28,9 +28,9 @@ struct DevBuf {
 };
 
 struct TableKey {
-  int W, S, N, apod, method, padded;
+  int wr, wc, sr, sc, apod, method, padded;
   bool operator<(const TableKey& o) const {
-    return std::tie(W, S, N, apod, method, padded) < std::tie(o.W, o.S, o.N, o.apod, o.method, o.padded);
+    return std::tie(wr, wc, sr, sc, apod, method, padded) < std::tie(o.wr, o.wc, o.sr, o.sc, o.apod, o.method, o.padded);
   }
 };
 struct Tables {
@@ -57,6 +57,7 @@ struct hh_ctx {
   const float* curA = nullptr;
   const float* curB = nullptr;
   bool staged = false;
+  const uint8_t* hook_mask = nullptr;  // image mask of the hook calls (hh_stage_mask), device
   // timing of the last schedule
   std::vector<float> pass_ms;
   std::vector<int32_t> pass_sweeps;
@@ -82,6 +83,8 @@ struct hh_ctx {
   // correlation kernel CTA shape per (FFT size, data extent), from
   // hh_set_corr_variant / hh_autotune_correlation (absent: 0, the default)
   std::map<std::pair<int, int>, int> corr_var;
+  // general-shape correlation: twiddle tables exp(-2 pi i t / n) by length
+  std::map<int, float2*> gc_twiddles;
 };
 
 namespace hhd {
@@ -193,6 +196,14 @@ inline hh_status make_grid(hh_ctx* ctx, int64_t nr, int64_t nc, const hh_pass_de
 }
 
 inline int fft_size(const hh_pass_desc& p) { return p.padding ? 2 * p.search[0] : p.search[0]; }
+inline int fft_rows(const hh_pass_desc& p) { return p.padding ? 2 * p.search[0] : p.search[0]; }
+inline int fft_cols(const hh_pass_desc& p) { return p.padding ? 2 * p.search[1] : p.search[1]; }
+
+// A fused shared-memory kernel exists for this pass (square window and
+// search area of a specialised size); otherwise the general-shape kernel runs.
+inline bool corr_special(const hh_pass_desc& p) {
+  return p.window[0] == p.window[1] && p.search[0] == p.search[1] && hh::correlate_supported(fft_size(p), p.search[0]);
+}
 
 // The CTA shape chosen for a pass's correlation launches.
 inline int32_t corr_variant(const hh_ctx* ctx, const hh_pass_desc& p) {
@@ -200,95 +211,221 @@ inline int32_t corr_variant(const hh_ctx* ctx, const hh_pass_desc& p) {
   return it == ctx->corr_var.end() ? 0 : it->second;
 }
 
-// apodization_window (src/correlators.jl:18-25), computed in double like Julia
-inline void apod_table(int W, int apod, std::vector<float>& out) {
-  out.assign((size_t)W * W, 1.0f);
+// apodization_window (src/correlators.jl:18-25), computed in double like
+// Julia: centre (w + 1)/2 and sigma w/4 per axis, wr x wc column-major
+inline void apod_table(int wr, int wc, int apod, std::vector<float>& out) {
+  out.assign((size_t)wr * wc, 1.0f);
   if (apod == HH_APOD_NONE) return;
-  const double c = (W + 1) / 2.0, s = W / 4.0;
-  for (int j = 1; j <= W; ++j)
-    for (int i = 1; i <= W; ++i)
-      out[(i - 1) + (size_t)(j - 1) * W] =
-          (float)std::exp(-((i - c) * (i - c) / (2 * s * s) + (j - c) * (j - c) / (2 * s * s)));
+  const double cr = (wr + 1) / 2.0, cc = (wc + 1) / 2.0, sr = wr / 4.0, sc = wc / 4.0;
+  for (int j = 1; j <= wc; ++j)
+    for (int i = 1; i <= wr; ++i)
+      out[(i - 1) + (size_t)(j - 1) * wr] =
+          (float)std::exp(-((i - cr) * (i - cr) / (2 * sr * sr) + (j - cc) * (j - cc) / (2 * sc * sc)));
 }
 
-// overlap gain (src/correlators.jl:170-181): the reference forms the
-// autocorrelation of the apodization window with an FFT; here it is summed
-// directly in double (the same quantity without transform round-off), then
-// thresholded at half the zero-lag weight in float.
-inline void gain_table(int W, const std::vector<float>& apod, std::vector<float>& out) {
-  const int N = 2 * W;
-  std::vector<float> wt((size_t)N * N, 0.f);
-  for (int qs = 0; qs < N; ++qs)
-    for (int ps = 0; ps < N; ++ps) {
-      const int dp = ps - N / 2, dq = qs - N / 2;
-      if (std::abs(dp) >= W || std::abs(dq) >= W) continue;
-      double acc = 0;
-      for (int q = std::max(0, -dq); q < std::min(W, W - dq); ++q)
-        for (int p = std::max(0, -dp); p < std::min(W, W - dp); ++p)
-          acc += (double)apod[p + (size_t)q * W] * (double)apod[(p + dp) + (size_t)(q + dq) * W];
-      wt[ps + (size_t)qs * N] = (float)std::fabs(acc);
-    }
+// overlap gain (src/correlators.jl:170-181): the weight of each lag is the
+// autocorrelation of the apodization window (the reference forms it with an
+// FFT in T); gain = wmax / w where w >= wmax / 2, else 0, in the fftshifted
+// layout of the 2wr x 2wc plane. Square windows up to 64 px sum the float
+// window's products directly in double; larger or rectangular windows use
+// the separable form of the same window (the product of the row and column
+// autocorrelations of the double-precision factors), the same quantity to
+// within the float rounding of the window values.
+inline void gain_table(int wr, int wc, int apod, const std::vector<float>& ap, std::vector<float>& out) {
+  const int NR = 2 * wr, NC = 2 * wc;
+  std::vector<float> wt((size_t)NR * NC, 0.f);
+  if (wr == wc && wr <= 64) {
+    const int W = wr, N = NR;
+    for (int qs = 0; qs < N; ++qs)
+      for (int ps = 0; ps < N; ++ps) {
+        const int dp = ps - N / 2, dq = qs - N / 2;
+        if (std::abs(dp) >= W || std::abs(dq) >= W) continue;
+        double acc = 0;
+        for (int q = std::max(0, -dq); q < std::min(W, W - dq); ++q)
+          for (int p = std::max(0, -dp); p < std::min(W, W - dp); ++p)
+            acc += (double)ap[p + (size_t)q * W] * (double)ap[(p + dp) + (size_t)(q + dq) * W];
+        wt[ps + (size_t)qs * N] = (float)std::fabs(acc);
+      }
+  } else {
+    auto axis = [apod](int w, std::vector<double>& ac) {
+      std::vector<double> g(w, 1.0);
+      if (apod == HH_APOD_GAUSS) {
+        const double c = (w + 1) / 2.0, s = w / 4.0;
+        for (int i = 1; i <= w; ++i) g[i - 1] = std::exp(-(i - c) * (i - c) / (2 * s * s));
+      }
+      ac.assign(2 * w, 0.0);  // lag d at index d + w
+      for (int d = -(w - 1); d <= w - 1; ++d) {
+        double a = 0;
+        for (int i = std::max(0, -d); i < std::min(w, w - d); ++i) a += g[i] * g[i + d];
+        ac[d + w] = a;
+      }
+    };
+    std::vector<double> ar, acol;
+    axis(wr, ar);
+    axis(wc, acol);
+    for (int qs = 0; qs < NC; ++qs)
+      for (int ps = 0; ps < NR; ++ps) {
+        const int dp = ps - NR / 2, dq = qs - NC / 2;
+        if (std::abs(dp) >= wr || std::abs(dq) >= wc) continue;
+        wt[ps + (size_t)qs * NR] = (float)std::fabs(ar[dp + wr] * acol[dq + wc]);
+      }
+  }
   float wmax = 0.f;
   for (float w : wt) wmax = std::max(wmax, w);
   out.resize(wt.size());
   for (size_t k = 0; k < wt.size(); ++k) out[k] = wt[k] >= wmax / 2 ? wmax / wt[k] : 0.f;
 }
 
-// PhaseCorrelator Gaussian spectral filter (src/correlators.jl:96-129)
-inline void phase_table(int N, std::vector<float>& out) {
-  out.resize((size_t)N * N);
-  const double fs = N / 8.0;
-  for (int j = 0; j < N; ++j)
-    for (int i = 0; i < N; ++i) {
-      const double fi = i < (N + 1) / 2 ? i : i - N, fj = j < (N + 1) / 2 ? j : j - N;
-      out[i + (size_t)j * N] = (float)std::exp(-(fi * fi + fj * fj) / (2 * fs * fs));
+// PhaseCorrelator Gaussian spectral filter (src/correlators.jl:96-129):
+// fftfreq bins of each axis, sigma = min(nr, nc) / 8, natural FFT order
+inline void phase_table(int NR, int NC, std::vector<float>& out) {
+  out.resize((size_t)NR * NC);
+  const double fs = std::min(NR, NC) / 8.0;
+  for (int j = 0; j < NC; ++j)
+    for (int i = 0; i < NR; ++i) {
+      const double fi = i < (NR + 1) / 2 ? i : i - NR, fj = j < (NC + 1) / 2 ? j : j - NC;
+      out[i + (size_t)j * NR] = (float)std::exp(-(fi * fi + fj * fj) / (2 * fs * fs));
     }
 }
 
 inline hh_status get_tables(hh_ctx* ctx, const hh_pass_desc& p, Tables& t) {
-  const int W = p.window[0], S = p.search[0], N = fft_size(p);
-  TableKey key{W, S, N, p.apodization, p.method, p.padding};
+  const int wr = p.window[0], wc = p.window[1], sr = p.search[0], sc = p.search[1];
+  const int NR = fft_rows(p), NC = fft_cols(p);
+  TableKey key{wr, wc, sr, sc, p.apodization, p.method, p.padding};
   auto it = ctx->tables.find(key);
   if (it != ctx->tables.end()) {
     t = it->second;
     return HH_OK;
   }
   std::vector<float> ap, gn, ph;
-  apod_table(W, p.apodization, ap);
+  apod_table(wr, wc, p.apodization, ap);
   Tables nt;
   HH_CK(cudaMalloc(&nt.apod, ap.size() * sizeof(float)));
   HH_CK(cudaMemcpy(nt.apod, ap.data(), ap.size() * sizeof(float), cudaMemcpyHostToDevice));
-  if (S != W) {
+  if (sr != wr || sc != wc) {
     // enlarged search area: no overlap gain (CrossCorrelator, src/correlators.jl:73);
     // only lags with |lag| <= (S - W) / 2 are kept (restrict_search_lags!, :347-355)
-    const int m = (S - W) / 2;
-    nt.box_lo = N / 2 - m;
-    nt.box_hi = N / 2 + m;
+    if (NR == NC && sr == sc && wr == wc) {
+      const int m = (sr - wr) / 2;
+      nt.box_lo = NR / 2 - m;
+      nt.box_hi = NR / 2 + m;
+    }
   } else if (p.padding) {
-    gain_table(W, ap, gn);
-    // bounding box of the nonzero gain (square and centred, by symmetry)
-    int lo = N, hi = -1;
-    for (int q = 0; q < N; ++q)
-      for (int r = 0; r < N; ++r)
-        if (gn[r + (size_t)q * N] != 0.f) {
-          lo = std::min(lo, std::min(r, q));
-          hi = std::max(hi, std::max(r, q));
-        }
-    if (hi > 0) {
-      nt.box_lo = lo;
-      nt.box_hi = hi;
+    gain_table(wr, wc, p.apodization, ap, gn);
+    if (NR == NC) {
+      // bounding box of the nonzero gain (square and centred, by symmetry)
+      int lo = NR, hi = -1;
+      for (int q = 0; q < NC; ++q)
+        for (int r = 0; r < NR; ++r)
+          if (gn[r + (size_t)q * NR] != 0.f) {
+            lo = std::min(lo, std::min(r, q));
+            hi = std::max(hi, std::max(r, q));
+          }
+      if (hi > 0) {
+        nt.box_lo = lo;
+        nt.box_hi = hi;
+      }
     }
     HH_CK(cudaMalloc(&nt.gain, gn.size() * sizeof(float)));
     HH_CK(cudaMemcpy(nt.gain, gn.data(), gn.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
   if (p.method == HH_PHASE) {
-    phase_table(N, ph);
+    phase_table(NR, NC, ph);
     HH_CK(cudaMalloc(&nt.phasew, ph.size() * sizeof(float)));
     HH_CK(cudaMemcpy(nt.phasew, ph.data(), ph.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
   ctx->tables[key] = nt;
   t = nt;
   return HH_OK;
+}
+
+// Twiddle table exp(-2 pi i t / n), t = 0 .. n-1, of one FFT length, built
+// once per context (double-precision angles, each entry rounded once).
+inline hh_status gc_twiddles(hh_ctx* ctx, int n, const float2** out) {
+  auto it = ctx->gc_twiddles.find(n);
+  if (it == ctx->gc_twiddles.end()) {
+    std::vector<float2> h(n);
+    for (int t = 0; t < n; ++t) {
+      // the angle in double (relative error ~1e-16, far below float rounding)
+      const double a = -2.0 * M_PI * (double)t / (double)n;
+      h[t] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    float2* d = nullptr;
+    HH_CK(cudaMalloc(&d, (size_t)n * sizeof(float2)));
+    HH_CK(cudaMemcpy(d, h.data(), (size_t)n * sizeof(float2), cudaMemcpyHostToDevice));
+    it = ctx->gc_twiddles.emplace(n, d).first;
+  }
+  *out = it->second;
+  return HH_OK;
+}
+
+// Shared memory of the general kernel's two line buffers (at most this much)
+constexpr size_t GC_SMEM_LINES = 192 * 1024;
+// planes the general kernel accepts (complex + real plane per CTA slice)
+constexpr int64_t GC_MAX_POINTS = (int64_t)1 << 22;
+
+// Is the pass's FFT shape one the general kernel can run?
+inline bool gcorr_shape_ok(const hh_pass_desc& p) {
+  int8_t rr[24];
+  const int NR = fft_rows(p), NC = fft_cols(p);
+  return NR >= 2 && NC >= 2 && (int64_t)NR * NC <= GC_MAX_POINTS && hh::gcorr_radix_plan(NR, rr) > 0 &&
+         hh::gcorr_radix_plan(NC, rr) > 0 && 2 * (size_t)(NC + 1) * 2 * sizeof(float2) <= GC_SMEM_LINES;
+}
+
+// Fill the general-shape fields of a correlation launch: shapes, radix
+// plans, twiddles, chunking and the scratch slice geometry (one slice per
+// CTA, as many as SMs); gcorr_prepare also points it at the context's
+// scratch buffer (grown on demand), a batched plan at its own.
+inline hh_status gcorr_setup(hh_ctx* ctx, const hh_pass_desc& p, CorrArgs& ca) {
+  ca.wr = p.window[0];
+  ca.wc = p.window[1];
+  ca.sr = p.search[0];
+  ca.sc = p.search[1];
+  ca.nfr = fft_rows(p);
+  ca.nfc = fft_cols(p);
+  ca.gc_nst_r = hh::gcorr_radix_plan(ca.nfr, ca.gc_radix_r);
+  ca.gc_nst_c = hh::gcorr_radix_plan(ca.nfc, ca.gc_radix_c);
+  if (ca.gc_nst_r < 0 || ca.gc_nst_c < 0 || !gcorr_shape_ok(p))
+    return fail(ctx, HH_ERR_UNSUPPORTED,
+                "backend :b200 has no correlation kernel for an FFT plane of " + std::to_string(ca.nfr) + " x " +
+                    std::to_string(ca.nfc));
+  HH_TRY(gc_twiddles(ctx, ca.nfr, &ca.twr));
+  HH_TRY(gc_twiddles(ctx, ca.nfc, &ca.twc));
+  ca.gc_chunk_r = std::max(1, std::min(32, (int)(GC_SMEM_LINES / (2 * (size_t)(ca.nfr + 1) * sizeof(float2)))));
+  ca.gc_chunk_c = std::max(2, std::min(32, (int)(GC_SMEM_LINES / (2 * (size_t)(ca.nfc + 1) * sizeof(float2)))) & ~1);
+  const size_t lines = std::max((size_t)ca.gc_chunk_r * (ca.nfr + 1), (size_t)ca.gc_chunk_c * (ca.nfc + 1));
+  ca.gc_smem_lines = (int64_t)(2 * lines * sizeof(float2));
+  const int64_t P = (int64_t)ca.nfr * ca.nfc;
+  ca.gscr_stride = (P + (P + 1) / 2 + 31) & ~(int64_t)31;  // complex plane + real plane, 256-byte aligned slices
+  ca.gscr_slices = ctx->num_sms;
+  return HH_OK;
+}
+inline hh_status gcorr_prepare(hh_ctx* ctx, const hh_pass_desc& p, CorrArgs& ca) {
+  HH_TRY(gcorr_setup(ctx, p, ca));
+  return buf(ctx, "gcorr_scratch", (size_t)ca.gscr_slices * ca.gscr_stride, &ca.gscr);
+}
+
+// The window shape of an uncertainty launch (rows W, columns Wc), and for
+// rectangular or large windows the general form's scratch slices (one per
+// CTA; the buffer is the context's and grows on demand).
+inline void uq_setup(hh_ctx* ctx, int wr, int wc, hh::UQArgs& ua) {
+  ua.W = wr;
+  ua.Wc = wc;
+  if (!hh::uq_general(wr, wc)) return;
+  ua.gscr_stride = hh::uq_general_stride(wr, wc);
+  ua.gscr_slices = 4 * ctx->num_sms;
+}
+inline hh_status uq_prepare(hh_ctx* ctx, int wr, int wc, hh::UQArgs& ua) {
+  uq_setup(ctx, wr, wc, ua);
+  if (!hh::uq_general(wr, wc)) return HH_OK;
+  return buf(ctx, "uq_scratch", (size_t)ua.gscr_slices * ua.gscr_stride, &ua.gscr);
+}
+
+// Launch the correlation of one pass: the fused kernel where one exists,
+// else the general-shape kernel (gcorr_prepare must have filled ca).
+inline cudaError_t corr_launch(hh_ctx* ctx, const hh_pass_desc& p, const CorrArgs& ca, cudaStream_t s) {
+  if (corr_special(p)) return hh::launch_correlate(ca, fft_size(p), p.search[0], s, ctx->num_sms);
+  return hh::launch_correlate_general(ca, s);
 }
 
 inline hh_status set_device(hh_ctx* ctx) {
@@ -372,7 +509,21 @@ inline double corr_flops(int N, int64_t njobs) {
   return (double)njobs * (3.0 * 2.5 * M * std::log2(M) + 8.0 * M);
 }
 inline double corr_bytes(int W, int nalt, int64_t njobs) { return (double)njobs * (2.0 * W * W * 4 + 4.0 * (4 + 2 * nalt)); }
+// the same for a pass of any shape: FFT plane NR x NC, frame-A window and
+// frame-B search area read once
+inline double corr_flops(const hh_pass_desc& p, int64_t njobs) {
+  const double M = (double)fft_rows(p) * fft_cols(p);
+  return (double)njobs * (3.0 * 2.5 * M * std::log2(M) + 8.0 * M);
+}
+inline double corr_bytes(const hh_pass_desc& p, int nalt, int64_t njobs) {
+  return (double)njobs * (4.0 * ((double)p.window[0] * p.window[1] + (double)p.search[0] * p.search[1]) +
+                          4.0 * (4 + 2 * nalt));
+}
 inline double uq_flops(int W, int64_t njobs) { return (double)njobs * 2.0 * 2.0 * (3 + 41) * W * (W - 1); }
+inline double uq_flops(const hh_pass_desc& p, int64_t njobs) {
+  const double wr = p.window[0], wc = p.window[1];
+  return (double)njobs * 2.0 * (3 + 41) * (wr * (wc - 1) + wc * (wr - 1));
+}
 
 // Cubic B-spline coefficients of both images of a pair.
 inline hh_status prefilter_pair(hh_ctx* ctx, const float* dA, const float* dB, int64_t nr, int64_t nc, float* cA, float* cB) {

@@ -38,10 +38,10 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
   for (int k = 0; k < np; ++k) {
     HH_TRY(make_grid(ctx, nr, nc, passes[k], hmask, thr, grids[k]));
     const int64_t nj = (int64_t)grids[k].jobs.size() / 4;
-    const int64_t N = fft_size(passes[k]);
+    const int64_t PL = (int64_t)fft_rows(passes[k]) * fft_cols(passes[k]);
     Gmax = std::max<int64_t>(Gmax, (int64_t)grids[k].ny * grids[k].nx);
     Jmax = std::max<int64_t>(Jmax, nj);
-    accmax = std::max<int64_t>(accmax, nj * N * N);
+    accmax = std::max<int64_t>(accmax, nj * PL);
     nalt_max = std::max(nalt_max, passes[k].n_peaks - 1);
   }
   float *dA = nullptr, *dB = nullptr, *coefA, *coefB, *warpA, *warpB, *acc;
@@ -114,7 +114,8 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
     const int ny = g.ny, nx = g.nx;
     const int64_t G = (int64_t)ny * nx;
     const int64_t njobs = (int64_t)g.jobs.size() / 4;
-    const int W = p.window[0], N = fft_size(p);
+    const int W = p.window[0], NR = fft_rows(p), NC = fft_cols(p);
+    const int64_t PL = (int64_t)NR * NC;
     const int nalt = p.n_peaks - 1;
     const bool unc = p.uncertainty && !force_replace;
     Tables tb;
@@ -155,7 +156,7 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
       HH_CK(cudaMemsetAsync(u, 0, G * sizeof(float), s));
       HH_CK(cudaMemsetAsync(v, 0, G * sizeof(float), s));
     }
-    HH_CK(cudaMemsetAsync(acc, 0, (size_t)njobs * N * N * sizeof(float), s));
+    HH_CK(cudaMemsetAsync(acc, 0, (size_t)njobs * PL * sizeof(float), s));
     if (unc) HH_CK(cudaMemsetAsync(stats, 0, (size_t)njobs * 88 * sizeof(double), s));
     for (int q = 0; q < npairs; ++q) {
       const float* A = pairs[q].A;
@@ -210,8 +211,9 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
         ca.accumulate = 1;
         ca.win = p.search[0] != W ? W : 0;
         ca.variant = corr_variant(ctx, p);
-        HH_K(HH_K_CORRELATE, 1, corr_flops(N, njobs), corr_bytes(p.search[0], 0, njobs) + 8.0 * N * N * njobs, njobs,
-             hh::launch_correlate(ca, N, p.search[0], s, ctx->num_sms));
+        if (!corr_special(p)) HH_TRY(gcorr_prepare(ctx, p, ca));
+        HH_K(HH_K_CORRELATE, 1, corr_flops(p, njobs), corr_bytes(p, 0, njobs) + 8.0 * PL * njobs, njobs,
+             corr_launch(ctx, p, ca, s));
         if (unc) {
           hh::UQArgs ua{};
           ua.A = A;
@@ -225,14 +227,16 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
           ua.apod = tb.apod;
           ua.stats = stats;
           ua.accumulate = 1;
-          HH_K(HH_K_UQ, 1, uq_flops(W, njobs), 8.0 * W * W * njobs, njobs, hh::launch_uq(ua, s, ctx->num_sms));
+          HH_TRY(uq_prepare(ctx, p.window[0], p.window[1], ua));
+          HH_K(HH_K_UQ, 1, uq_flops(p, njobs), 8.0 * p.window[0] * p.window[1] * njobs, njobs,
+               hh::launch_uq(ua, s, ctx->num_sms));
         }
       }
     }
     // partial sums of this process's pairs -> sums over all processes
     if (ctx->ens_reduce && njobs > 0) {
       const int64_t nst = unc ? njobs * 88 : 0;
-      if (ctx->ens_reduce(ctx->ens_reduce_user, k, acc, njobs * N * N, unc ? stats : nullptr, nst, (void*)s) != 0)
+      if (ctx->ens_reduce(ctx->ens_reduce_user, k, acc, njobs * PL, unc ? stats : nullptr, nst, (void*)s) != 0)
         return fail(ctx, HH_ERR_STATE, "ensemble reducer failed in pass " + std::to_string(k + 1));
     }
     // ensemble_analyze! (src/ensemble.jl:273-305): one analysis of every summed plane
@@ -246,8 +250,8 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
       hh::AnalyzeArgs aa{};
       aa.planes = acc;
       aa.nplanes = njobs;
-      aa.nr = N;
-      aa.nc = N;
+      aa.nr = NR;
+      aa.nc = NC;
       aa.npeaks = p.n_peaks;
       aa.finder = p.peak_finder;
       aa.subpixel = p.subpixel;
@@ -261,7 +265,7 @@ extern "C" hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, in
       aa.alt_u = nalt > 0 ? altu : nullptr;
       aa.alt_v = nalt > 0 ? altv : nullptr;
       aa.nalt = nalt;
-      HH_K(HH_K_CORRELATE, 1, 0, 4.0 * N * N * njobs, njobs, hh::launch_analyze_planes(aa, s));
+      HH_K(HH_K_CORRELATE, 1, 0, 4.0 * PL * njobs, njobs, hh::launch_analyze_planes(aa, s));
       if (unc) HH_K(HH_K_UQ, 1, 0, 88.0 * 8 * njobs, njobs, hh::launch_uq_finalize(stats, djobs, njobs, ny, uncu, uncv, s));
     }
     HH_K(HH_K_VECTOR, 1, 0, (28 + 8 * nalt) * G, G,

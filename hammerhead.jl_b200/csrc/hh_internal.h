@@ -57,12 +57,36 @@ struct CorrArgs {
   // with regional maxima the per-window outputs are then formed by a
   // one-thread-per-window epilogue kernel after the correlation kernel
   float* rec;
+  // general-shape path (correlate_general_kernel): window wr x wc, search
+  // area sr x sc, FFT plane nfr x nfc; gscr holds one scratch slice of
+  // gscr_stride float2 per CTA (complex plane + real plane); twr / twc the
+  // twiddle tables exp(-2 pi i t / n) of the two lengths and their radix
+  // plans; lines staged per chunk and the shared bytes of the line buffers
+  int32_t wr, wc, sr, sc, nfr, nfc;
+  float2* gscr;
+  int64_t gscr_stride;
+  int32_t gscr_slices;
+  const float2* twr;
+  const float2* twc;
+  int8_t gc_radix_r[24], gc_radix_c[24];
+  int32_t gc_nst_r, gc_nst_c;
+  int32_t gc_chunk_r, gc_chunk_c;
+  int64_t gc_smem_lines;
 };
 
 // Launch the correlation kernel for FFT size N (square) and window W (the
 // search area when a.win is set).
 cudaError_t launch_correlate(const CorrArgs& a, int N, int W, cudaStream_t s, int num_sms);
 bool correlate_supported(int N, int W);
+// The general-shape correlation (any FFT lengths, rectangular windows and
+// search areas): a.wr .. a.gc_smem_lines set by the host (gcorr_prepare).
+cudaError_t launch_correlate_general(const CorrArgs& a, cudaStream_t s);
+// Radix plan of an FFT length (factors 4, 2, then odd primes <= 61);
+// returns the stage count, or -1 when a factor exceeds 61 or there are more
+// than 24 stages.
+int gcorr_radix_plan(int n, int8_t* radix);
+// Shared bytes the general kernel needs beyond its line buffers.
+size_t gcorr_smem_extra();
 size_t correlate_record_words(int npeaks);  // per job
 size_t correlate_smem_bytes(int N, int W);
 
@@ -150,8 +174,19 @@ struct UQArgs {
   int32_t mode;
   // ensemble mode: stats += this pair's statistics
   int32_t accumulate;
+  // rectangular windows (W rows x Wc columns; Wc == 0: square) and windows
+  // above 64 px run the general form, whose per-window buffers live in a
+  // global scratch slice per CTA (gscr_slices slices of gscr_stride doubles)
+  int32_t Wc;
+  double* gscr;
+  int64_t gscr_stride;
+  int32_t gscr_slices;
 };
 cudaError_t launch_uq(const UQArgs& a, cudaStream_t s, int num_sms);
+// Does this window shape run the general (global-scratch) form, and how many
+// doubles does one window's scratch slice take?
+bool uq_general(int wr, int wc);
+int64_t uq_general_stride(int wr, int wc);
 // finalize_uncertainty of pooled statistics (88 per job) into grid cells
 cudaError_t launch_uq_finalize(const double* stats, const int32_t* jobs, int64_t njobs, int32_t ny, float* unc_u,
                                float* unc_v, cudaStream_t s);

@@ -641,6 +641,10 @@ __device__ __forceinline__ float2 cross_spectrum(float2 X, float2 Zm, int method
   return S;
 }
 
+// the general-shape kernel (any FFT lengths, rectangular windows, planes
+// larger than a CTA's shared memory)
+#include "hh_corr_general.cuh"
+
 // ---------------------------------------------------------------------------
 // W is the extent of the data: the window, or with SRCH the frame-B search
 // area that holds the (runtime) frame-A window at its centre. VAR selects the
@@ -1227,21 +1231,27 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
 }
 
 // Device analysis of caller-supplied planes (one CTA of 128 threads each).
-__global__ void __launch_bounds__(128) analyze_planes_kernel(const AnalyzeArgs a) {
+// The plane is staged in shared memory when it fits (in_smem), else read in
+// place from global memory (planes above 200 KB: 256 x 256 and larger).
+__global__ void __launch_bounds__(128) analyze_planes_kernel(const AnalyzeArgs a, bool in_smem) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float* R = reinterpret_cast<float*>(smem_raw);
   const int P = a.nr * a.nc;
-  uint32_t* red = reinterpret_cast<uint32_t*>(R + P);
+  float* R = reinterpret_cast<float*>(smem_raw);
+  uint32_t* red = reinterpret_cast<uint32_t*>(smem_raw + (in_smem ? (size_t)P * sizeof(float) : 0));
   float* s_vals = reinterpret_cast<float*>(red + 8 * KMAX);
   int* s_locs = reinterpret_cast<int*>(s_vals + KMAX);
   const int K = a.npeaks > 2 ? a.npeaks : 2;
   PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
   const ScanPlan sp = scan_plan(threadIdx.x, 128, 0, a.nr - 1, 0, a.nc - 1);
   for (int64_t pl = blockIdx.x; pl < a.nplanes; pl += gridDim.x) {
-    for (int k = threadIdx.x; k < P; k += blockDim.x) R[k] = a.planes[pl * (int64_t)P + k];
+    const float* Rp = a.planes + pl * (int64_t)P;
+    if (in_smem) {
+      for (int k = threadIdx.x; k < P; k += blockDim.x) R[k] = Rp[k];
+      Rp = R;
+    }
     __syncthreads();
     const int64_t gid = a.jobs ? (int64_t)a.jobs[4 * pl] + (int64_t)a.jobs[4 * pl + 1] * a.ny : -1;
-    analyze_group(R, a.nr, a.nc, a.nr, K, a.npeaks, a.finder, a.subpixel, threadIdx.x, 128, red, true, s_vals,
+    analyze_group(Rp, a.nr, a.nc, a.nr, K, a.npeaks, a.finder, a.subpixel, threadIdx.x, 128, red, true, s_vals,
                   s_locs, gid, pl, &po, false, 0, sp, nullptr, 0);
     __syncthreads();
   }
@@ -1349,15 +1359,61 @@ cudaError_t launch_correlate(const CorrArgs& a, int N, int W, cudaStream_t s, in
   return cudaErrorInvalidValue;
 }
 
+int gcorr_radix_plan(int n, int8_t* radix) {
+  if (n < 1) return -1;
+  int ns = 0;
+  auto push = [&](int r) {
+    if (ns >= 24) return false;
+    radix[ns++] = (int8_t)r;
+    return true;
+  };
+  while (n % 4 == 0) {
+    if (!push(4)) return -1;
+    n /= 4;
+  }
+  while (n % 2 == 0) {
+    if (!push(2)) return -1;
+    n /= 2;
+  }
+  for (int f = 3; f <= 61 && n > 1; f += 2)
+    while (n % f == 0) {
+      if (!push(f)) return -1;
+      n /= f;
+    }
+  return n == 1 ? ns : -1;
+}
+
+size_t gcorr_smem_extra() {
+  return 4 * GC_WARPS * sizeof(double) + GC_WARPS * 2 * KMAX * sizeof(uint32_t) + KMAX * sizeof(float) +
+         2 * KMAX * sizeof(int) + 64;
+}
+
+cudaError_t launch_correlate_general(const CorrArgs& a, cudaStream_t s) {
+  if (a.njobs <= 0) return cudaSuccess;
+  if (!a.gscr || !a.twr || !a.twc || a.gscr_slices < 1 || a.gc_chunk_r < 1 || a.gc_chunk_c < 2)
+    return cudaErrorInvalidValue;
+  const size_t sm = (size_t)a.gc_smem_lines + gcorr_smem_extra();
+  static size_t attr = 0;
+  if (sm > attr) {
+    cudaError_t e = cudaFuncSetAttribute(correlate_general_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    attr = sm;
+  }
+  const int64_t grid = a.njobs < a.gscr_slices ? a.njobs : a.gscr_slices;
+  correlate_general_kernel<<<(unsigned)grid, GC_THREADS, sm, s>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_analyze_planes(const AnalyzeArgs& a, cudaStream_t s) {
   if (a.nplanes <= 0) return cudaSuccess;
-  const size_t sm = (size_t)a.nr * a.nc * sizeof(float) + 8 * KMAX * sizeof(uint32_t) + KMAX * sizeof(float) +
-                    2 * KMAX * sizeof(int) + 16;
-  if (sm > 200 * 1024) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(analyze_planes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  const size_t extra = 8 * KMAX * sizeof(uint32_t) + KMAX * sizeof(float) + 2 * KMAX * sizeof(int) + 16;
+  size_t sm = (size_t)a.nr * a.nc * sizeof(float) + extra;
+  const bool in_smem = sm <= 200 * 1024;
+  if (!in_smem) sm = extra;
+  cudaError_t e = cudaFuncSetAttribute(analyze_planes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e != cudaSuccess) return e;
   int64_t grid = a.nplanes < 4096 ? a.nplanes : 4096;
-  analyze_planes_kernel<<<(unsigned)grid, 128, sm, s>>>(a);
+  analyze_planes_kernel<<<(unsigned)grid, 128, sm, s>>>(a, in_smem);
   return cudaGetLastError();
 }
 

@@ -642,14 +642,17 @@ __device__ __forceinline__ PredGrid b_pred_grid(const BPair& b, int it) {
 // in their final pass.
 __global__ void b_sweep_begin_kernel(const BPair* __restrict__ bp, int npairs, const int32_t* __restrict__ done, int it,
                                      int64_t gtot, const float* __restrict__ pu, const float* __restrict__ pv, float* u,
-                                     float* v, float* uncu, float* uncv, int32_t* sweeps) {
+                                     float* v, float* uncu, float* uncv, int32_t* sweeps, int32_t* slot_sweeps) {
   B_STRIDE(k, gtot) {
     const int p = bp_find<&BPair::coff>(bp, npairs, k);
     const BPair& b = bp[p];
     const int64_t l = k - b.coff;
     if (!bp_live(b, it, done, p) || l >= (int64_t)b.ny * b.nx) continue;
     const int64_t id = b.goff + l;
-    if (l == 0 && b.is_final) sweeps[p] = it;
+    if (l == 0) {
+      slot_sweeps[p] = it;
+      if (b.is_final) sweeps[p] = it;
+    }
     if (it == 1) {
       uncu[id] = __int_as_float(0x7fc00000);
       uncv[id] = __int_as_float(0x7fc00000);
@@ -669,9 +672,10 @@ __global__ void b_sweep_begin_kernel(const BPair* __restrict__ bp, int npairs, c
 
 cudaError_t launch_b_sweep_begin(const BPair* bp, int npairs, const int32_t* done, int it, int64_t gtot,
                                  const float* pu, const float* pv, float* u, float* v, float* uncu, float* uncv,
-                                 int32_t* sweeps, cudaStream_t s) {
+                                 int32_t* sweeps, int32_t* slot_sweeps, cudaStream_t s) {
   if (gtot <= 0) return cudaSuccess;
-  b_sweep_begin_kernel<<<b_blocks(gtot), 256, 0, s>>>(bp, npairs, done, it, gtot, pu, pv, u, v, uncu, uncv, sweeps);
+  b_sweep_begin_kernel<<<b_blocks(gtot), 256, 0, s>>>(bp, npairs, done, it, gtot, pu, pv, u, v, uncu, uncv, sweeps,
+                                                      slot_sweeps);
   return cudaGetLastError();
 }
 

@@ -570,6 +570,166 @@ __global__ void uq_finalize_kernel(const double* __restrict__ stats, const int32
   }
 }
 
+// ---------------------------------------------------------------------------
+// General form: rectangular windows (wr x wc) and windows above 64 px. The
+// same operations as uq_kernel, per component in its own frame (u: the
+// window as stored, wr rows x wc columns, shifts along the columns; v: its
+// transpose, wc rows x wr columns), with the windows, dC, its smoothing and
+// the FP64 field in a global scratch slice per CTA instead of shared memory.
+struct UQGeom {
+  int R, C, m;          // rows, columns of the component's frame; m = C - 1 columns of dC
+  int sr_, sc_;         // strides of (r, c) into the stored window
+};
+__device__ __forceinline__ UQGeom uq_geom(int comp, int wr, int wc) {
+  return comp == 0 ? UQGeom{wr, wc, wc - 1, 1, wr} : UQGeom{wc, wr, wr - 1, wr, 1};
+}
+
+bool uq_general(int wr, int wc) { return wr != wc || wr > 64; }
+int64_t uq_general_stride(int wr, int wc) {
+  const int64_t n = (int64_t)wr * wc, mu = (int64_t)wr * (wc - 1), mv = (int64_t)wc * (wr - 1);
+  // doubles: dd (mu + mv); floats: wa, wb (n each), dC and dCs (mu + mv each)
+  const int64_t fl = 2 * n + 2 * (mu + mv);
+  return ((mu + mv) + (fl + 1) / 2 + 31) & ~(int64_t)31;
+}
+
+__global__ void __launch_bounds__(UQ_THREADS) uq_general_kernel(const UQArgs a, const UQOffsets o) {
+  __shared__ double stats[88];
+  __shared__ double part[4 * (UQ_THREADS / 32)];
+  const int wr = a.W, wc = a.Wc > 0 ? a.Wc : a.W, n = wr * wc;
+  const int mu = wr * (wc - 1), mv = wc * (wr - 1);
+  double* dd = a.gscr + (int64_t)blockIdx.x * a.gscr_stride;  // mu + mv
+  float* wa = reinterpret_cast<float*>(dd + mu + mv);          // n
+  float* wb = wa + n;                                          // n
+  float* dC = wb + n;                                          // mu + mv
+  float* dCs = dC + mu + mv;                                   // mu + mv
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int64_t job = blockIdx.x; job < a.njobs; job += gridDim.x) {
+    const UQSrc src = uq_src(a, job);
+    if (!src.on) continue;  // uniform across the CTA
+    double sa = 0.0, sb = 0.0, cnt = 0.0;
+    for (int k = tid; k < n; k += UQ_THREADS) {
+      const int p = k % wr, q = k / wr;
+      const int64_t off = (int64_t)(src.rs + p) + (int64_t)(src.cs + q) * src.ld;
+      const float va = src.A[off], vb = src.B[off];
+      const bool mk = src.M ? src.M[off] != 0 : false;
+      wa[k] = mk ? __int_as_float(0x7fc00000) : va;  // NaN marks a masked pixel until the means are known
+      wb[k] = vb;
+      if (!mk) {
+        sa += (double)va;
+        sb += (double)vb;
+        cnt += 1.0;
+      }
+    }
+    sa = warp_sum(sa);
+    sb = warp_sum(sb);
+    cnt = warp_sum(cnt);
+    if (lane == 0) {
+      part[3 * warp] = sa;
+      part[3 * warp + 1] = sb;
+      part[3 * warp + 2] = cnt;
+    }
+    __syncthreads();
+    double ta = 0, tb = 0, tn = 0;
+    for (int w = 0; w < UQ_THREADS / 32; ++w) {
+      ta += part[3 * w];
+      tb += part[3 * w + 1];
+      tn += part[3 * w + 2];
+    }
+    const float ma = tn > 0 ? (float)(ta / tn) : 0.f, mb = tn > 0 ? (float)(tb / tn) : 0.f;
+    for (int k = tid; k < n; k += UQ_THREADS) {
+      const int p = k % wr, q = k / wr;
+      const int64_t off = (int64_t)(src.rs + p) + (int64_t)(src.cs + q) * src.ld;
+      const bool mk = src.M ? src.M[off] != 0 : false;
+      const float ap = a.apod[k];
+      const float va = src.A[off];
+      wa[k] = mk ? 0.f : __fmul_rn(ap, __fsub_rn(va, ma));
+      wb[k] = mk ? 0.f : __fmul_rn(ap, __fsub_rn(wb[k], mb));
+    }
+    __syncthreads();
+    // dC = a0 b1 - a1 b0 per component
+    for (int k = tid; k < mu + mv; k += UQ_THREADS) {
+      const int comp = k >= mu, e = comp ? k - mu : k;
+      const UQGeom g = uq_geom(comp, wr, wc);
+      const int r = e % g.R, c = e / g.R;
+      const float a0 = wa[r * g.sr_ + c * g.sc_], a1 = wa[r * g.sr_ + (c + 1) * g.sc_];
+      const float b0 = wb[r * g.sr_ + c * g.sc_], b1 = wb[r * g.sr_ + (c + 1) * g.sc_];
+      dC[k] = __fsub_rn(__fmul_rn(a0, b1), __fmul_rn(a1, b0));
+    }
+    __syncthreads();
+    double s0 = 0.0, s1 = 0.0;
+    for (int k = tid; k < mu + mv; k += UQ_THREADS) {
+      const int comp = k >= mu, e = comp ? k - mu : k;
+      const UQGeom g = uq_geom(comp, wr, wc);
+      const float* d = dC + (comp ? mu : 0);
+      const int r = e % g.R, c = e / g.R;
+      const int cl = c > 0 ? c - 1 : 0, cr = c < g.m - 1 ? c + 1 : g.m - 1;
+      const float v = __fmul_rn(0.25f, __fadd_rn(__fadd_rn(d[r + cl * g.R], __fmul_rn(2.0f, d[r + c * g.R])), d[r + cr * g.R]));
+      dCs[k] = v;
+      if (comp == 0) s0 += (double)v;
+      else s1 += (double)v;
+    }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    __syncthreads();  // part reused
+    if (lane == 0) {
+      part[3 * warp] = s0;
+      part[3 * warp + 1] = s1;
+    }
+    __syncthreads();
+    double mu0 = 0, mu1 = 0;
+    for (int w = 0; w < UQ_THREADS / 32; ++w) {
+      mu0 += part[3 * w];
+      mu1 += part[3 * w + 1];
+    }
+    mu0 /= (double)mu;
+    mu1 /= (double)mv;
+    for (int k = tid; k < mu + mv; k += UQ_THREADS) dd[k] = (double)dCs[k] - (k < mu ? mu0 : mu1);
+    __syncthreads();
+    // the 2 x 44 statistics, one warp per statistic (uq_component!, :104-151)
+    for (int st = warp; st < 88; st += UQ_THREADS / 32) {
+      const int comp = st / 44, si = st % 44;
+      const UQGeom g = uq_geom(comp, wr, wc);
+      const double* d = dd + (comp ? mu : 0);
+      const int WM = g.R * g.m;
+      double acc = 0.0;
+      if (si < 3) {
+        for (int t = lane; t < WM; t += 32) {
+          const int r = t % g.R, c = t / g.R;
+          const float a0 = wa[r * g.sr_ + c * g.sc_], a1 = wa[r * g.sr_ + (c + 1) * g.sc_];
+          const float b0 = wb[r * g.sr_ + c * g.sc_], b1 = wb[r * g.sr_ + (c + 1) * g.sc_];
+          const float pr = si == 0 ? __fmul_rn(a0, b0) : (si == 1 ? __fmul_rn(a0, b1) : __fmul_rn(a1, b0));
+          acc += (double)pr;
+        }
+      } else if (si == 3) {
+        for (int t = lane; t < WM; t += 32) acc = fma(d[t], d[t], acc);
+      } else {
+        const int k = si - 4, dr = o.dr[k], dc = o.dc[k];
+        const int c0 = dc < 0 ? -dc : 0, c1 = dc > 0 ? g.m - dc : g.m;  // c in [c0, c1)
+        const int r0 = dr < 0 ? -dr : 0, r1 = dr > 0 ? g.R - dr : g.R;  // r in [r0, r1)
+        const int nrr = r1 - r0, ncc = c1 - c0;
+        for (int t = lane; t < nrr * ncc; t += 32) {
+          const int r = r0 + t % nrr, c = c0 + t / nrr;
+          acc = fma(d[r + c * g.R], d[(r + dr) + (c + dc) * g.R], acc);
+        }
+      }
+      acc = warp_sum(acc);
+      if (lane == 0) stats[st] = acc;
+    }
+    __syncthreads();
+    if (a.stats)
+      for (int it = tid; it < 88; it += UQ_THREADS) {
+        if (a.accumulate) a.stats[job * 88 + it] += stats[it];
+        else a.stats[job * 88 + it] = stats[it];
+      }
+    if (a.unc_u && tid < 2) {
+      const float sg = uq_finalize(stats + 44 * tid, o);
+      if (tid == 0) a.unc_u[src.gid] = sg;
+      else a.unc_v[src.gid] = sg;
+    }
+    __syncthreads();
+  }
+}
+
 template <int W> static cudaError_t launch_uq_warp(const UQArgs& a, cudaStream_t s, int num_sms, const UQOffsets& offs) {
   using C = UQWCfg<W>;
   const size_t sm = C::smem();
@@ -589,6 +749,14 @@ template <int W> static cudaError_t launch_uq_warp(const UQArgs& a, cudaStream_t
 cudaError_t launch_uq(const UQArgs& a, cudaStream_t s, int num_sms) {
   if (a.njobs <= 0) return cudaSuccess;
   static const UQOffsets offs = make_offsets();
+  const int wc = a.Wc > 0 ? a.Wc : a.W;
+  if (uq_general(a.W, wc)) {
+    if (!a.gscr || a.gscr_slices < 1 || a.gscr_stride < uq_general_stride(a.W, wc) || a.W < 2 || wc < 2)
+      return cudaErrorInvalidValue;
+    const int64_t grid = a.njobs < a.gscr_slices ? a.njobs : a.gscr_slices;
+    uq_general_kernel<<<(unsigned)grid, UQ_THREADS, 0, s>>>(a, offs);
+    return cudaGetLastError();
+  }
   switch (a.W) {
     case 8: return launch_uq_warp<8>(a, s, num_sms, offs);
     case 12: return launch_uq_warp<12>(a, s, num_sms, offs);

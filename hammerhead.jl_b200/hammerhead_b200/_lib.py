@@ -160,6 +160,7 @@ SIGNATURES = [
     ("hh_apply_predictor", ctypes.c_int32,
      [_CTX, _F, _F, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
       _F, ctypes.c_int32, _F, ctypes.c_int32, _F, _F, _F, _F]),
+    ("hh_stage_mask", ctypes.c_int32, [_CTX, _U8]),
     ("hh_process_windows", ctypes.c_int32, [_CTX, _PASS, _I32, ctypes.c_int64, _F, _I32, _D]),
     ("hh_analyze_planes", ctypes.c_int32,
      [_CTX, _F, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _F,
@@ -180,6 +181,7 @@ SIGNATURES = [
     ("hh_autotune_correlation", ctypes.c_int32,
      [_CTX, _PASS, ctypes.c_int32, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int32)]),
     ("hh_set_corr_variant", ctypes.c_int32, [_CTX, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    ("hh_corr_fused", ctypes.c_int32, [_PASS]),
     ("hh_ncc_loss_grad", ctypes.c_int32,
      [_CTX, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
       ctypes.c_float, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),

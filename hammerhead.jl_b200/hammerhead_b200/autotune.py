@@ -33,11 +33,14 @@ def _flatten(passes):
 
 def pass_classes(passes):
     """The distinct (FFT size, window, peaks) of the equal-area passes of a
-    pass, a schedule or a list of schedules, in first-seen order."""
+    pass, a schedule or a list of schedules that run on the fused
+    correlation kernels, in first-seen order."""
     seen = []
     for p in _flatten(passes):
         if p.search_area_size != p.window_size:
             continue  # enlarged search areas have one shape
+        if not _lib.lib().hh_corr_fused(ctypes.byref(p.to_desc())):
+            continue  # the general-shape kernel has one shape
         w = p.window_size[0]
         c = (2 * w if p.padding else w, w, p.n_peaks)
         if c not in seen:

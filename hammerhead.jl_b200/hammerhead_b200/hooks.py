@@ -12,6 +12,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
+from ._lib import ArgumentError
 from .params import PIVParameters
 
 
@@ -33,6 +34,14 @@ class DeviceSession:
         self.shape = A.shape
         _lib.check(_lib.lib().hh_stage_pair(self.ws.ctx, _lib.fptr(A), _lib.fptr(B), A.shape[0], A.shape[1]),
                    self.ws.ctx)
+
+    def stage_mask(self, mask):
+        """Image mask of the following process_windows / correlation_planes
+        calls (None clears it): masked pixels leave the window means."""
+        m = None if mask is None else np.asfortranarray(mask, np.uint8)
+        if m is not None and m.shape != tuple(self.shape):
+            raise ArgumentError(f"mask must have the staged image size {tuple(self.shape)}, got {m.shape}")
+        _lib.check(_lib.lib().hh_stage_mask(self.ws.ctx, _lib.u8ptr(m)), self.ws.ctx)
 
     def apply_predictor(self, pu, pv, py, px, y, x, return_warped=False):
         """Deform the staged pair by predictor (pu, pv) on knots (py, px);
@@ -81,12 +90,13 @@ class DeviceSession:
     def correlation_planes(self, params: PIVParameters, jobs):
         jobs = np.ascontiguousarray(jobs, np.int32)
         nj = jobs.shape[0]
-        n = 2 * params.search_area_size[0] if params.padding else params.search_area_size[0]
-        planes = np.empty((nj, n * n), np.float32)
+        f = 2 if params.padding else 1
+        nr, nc = f * params.search_area_size[0], f * params.search_area_size[1]
+        planes = np.empty((nj, nr * nc), np.float32)
         d = params.to_desc()
         _lib.check(_lib.lib().hh_correlation_planes(self.ws.ctx, ctypes.byref(d), _lib.i32ptr(jobs), nj,
                                                     _lib.fptr(planes)), self.ws.ctx)
-        return planes.reshape(nj, n, n).transpose(0, 2, 1)  # planes[j] indexed [row, col]
+        return planes.reshape(nj, nc, nr).transpose(0, 2, 1)  # planes[j] indexed [row, col]
 
 
 _FINDER = {"regionalmax": 0, "exclusion": 1}

@@ -10,7 +10,11 @@ module HammerheadB200Ext
 using Hammerhead
 using ChainRulesCore: ChainRulesCore, NoTangent, unthunk
 import Hammerhead: _AbstractHammerheadBackend, _resolve_backend, _check_backend_params, _engine_nchunks,
-    _supports_fft, _supports_batched_fft, _supports_fp64, PIVParameters, PIVResult, run_piv
+    _supports_fft, _supports_batched_fft, _supports_fp64, PIVParameters, PIVResult, run_piv,
+    piv_correlation_engines, process_windows!, uncertainty_sweep!, _deform_context, apply_predictor,
+    release_piv_engines!, _correlation_apod, pooled_engines, apodization_window, finalize_uncertainty,
+    _plane_accumulator, accumulate_planes!, ensemble_analyze!, _uncertainty_accumulator,
+    _uncertainty_scratch, UQ_NSTATS
 
 const LIB = get(ENV, "HAMMERHEAD_B200_LIB", "libhammerhead_b200.so")
 
@@ -152,6 +156,265 @@ function run_piv_b200(imgA::AbstractMatrix{<:Real}, imgB::AbstractMatrix{<:Real}
                     ctx.ptr, A, B, nr, nc, d, length(d), M, mask_threshold, predictor_smoothing, res), ctx.ptr)
     end
     return PIVResult(x, y, u, v, ratio, moment, su, sv, BitMatrix(outl .!= 0), BitMatrix(gm .!= 0), final)
+end
+
+# ---- the backend hooks: run_piv(A, B, passes; backend = :b200) -----------
+#
+# Hammerhead's run_piv resolves `backend = :b200` through _resolve_backend
+# above and then drives every pass through these private hooks
+# (docs/src/reference/backends.md:40-71; the :cuda counterparts are
+# ext/HammerheadCUDAExt.jl:105-437):
+#   piv_correlation_engines -> one engine per pass configuration (nchunks = 1)
+#   _deform_context         -> a handle on the context that holds the pair
+#   apply_predictor         -> hh_stage_pair (once per pair: upload + device
+#                              B-spline prefilter) + hh_apply_predictor (device
+#                              deformation; the warped pair stays on the device)
+#   process_windows!        -> hh_process_windows on the staged (warped) pair
+#   uncertainty_sweep!      -> hh_process_windows' Wieneke statistics +
+#                              hh_finalize_uncertainty
+#   release_piv_engines!    -> nothing to release (the context's arena is
+#                              reused by the next call)
+# and run_piv_ensemble through _plane_accumulator / accumulate_planes! /
+# ensemble_analyze! (hh_correlation_planes + hh_analyze_planes; the
+# device-resident ensemble is run_piv_ensemble_b200 below).
+
+# The library context of a workspace (one per PIVWorkspace, pooled like an
+# engine), or of the process when run_piv gets no workspace.
+const _DEFAULT_CTX = Ref{Union{Nothing,Context}}(nothing)
+function _b200_context(workspace)
+    if workspace === nothing
+        _DEFAULT_CTX[] === nothing && (_DEFAULT_CTX[] = Context())
+        return _DEFAULT_CTX[]
+    end
+    return pooled_engines(() -> Context(), workspace, (:b200_context,), 1)[1]
+end
+
+# A correlation engine: the pass configuration on a context. Every buffer is
+# the context's (grown on demand), so engines are cheap and pure scratch.
+struct _B200Engine
+    ctx::Context
+    params::PIVParameters
+    desc::PassDesc
+    apod::Matrix{Float32}
+end
+
+_correlation_apod(e::_B200Engine) = e.apod
+
+piv_correlation_engines(::_B200Backend, workspace, params::PIVParameters, ::Type{T}, nchunks::Int) where {T} =
+    pooled_engines(() -> _B200Engine(_b200_context(workspace), params, pass_desc(params),
+                                     apodization_window(Float32, params.window_size, params.apodization)),
+                   workspace, (:b200, T, params.correlation_method, params.window_size, params.search_area_size,
+                               params.padding, params.apodization, max(params.n_peaks, 2)), nchunks)
+
+release_piv_engines!(::_B200Backend, engines, workspace) = nothing
+
+# The pair held by a context: after apply_predictor it is the deformed pair,
+# resident on the device; engines correlate it in place.
+struct _B200Pair <: AbstractMatrix{Float32}
+    ctx::Context
+    nr::Int
+    nc::Int
+end
+Base.size(p::_B200Pair) = (p.nr, p.nc)
+Base.getindex(::_B200Pair, ::Int, ::Int) =
+    throw(ArgumentError("backend :b200 keeps the deformed images on the device"))
+
+mutable struct _B200Deform
+    ctx::Context
+    imgsize::Dims{2}
+    staged::Bool
+end
+
+_deform_context(::_B200Backend, workspace, itpA, itpB, imgsize::Dims{2}, ::Type{T}) where {T} =
+    _B200Deform(_b200_context(workspace), imgsize, false)
+
+function _stage!(ctx::Context, imgA::AbstractMatrix, imgB::AbstractMatrix)
+    A = Matrix{Float32}(imgA)
+    B = Matrix{Float32}(imgB)
+    check(ccall((:hh_stage_pair, LIB), Int32, (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Int64, Int64),
+                ctx.ptr, A, B, size(A, 1), size(A, 2)), ctx.ptr)
+    return nothing
+end
+
+function apply_predictor(::_B200Backend, imgA::AbstractMatrix, imgB::AbstractMatrix, itpA, itpB, predictor,
+                         x::AbstractVector, y::AbstractVector, ::Type{T}; ctx = nothing, kwargs...) where {T}
+    ny, nx = length(y), length(x)
+    predictor === nothing && return imgA, imgB, zeros(T, ny, nx), zeros(T, ny, nx)
+    # direct calls without a deform context: the CPU deformation
+    ctx === nothing && return apply_predictor(imgA, imgB, itpA, itpB, predictor, x, y, T; kwargs...)
+    if !ctx.staged  # once per pair: upload and prefilter on the device
+        _stage!(ctx.ctx, imgA, imgB)
+        ctx.staged = true
+    end
+    px, py = predictor.x, predictor.y
+    pu = Matrix{Float32}(predictor.u)
+    pv = Matrix{Float32}(predictor.v)
+    gny, gnx = size(pu)
+    ysp = gny > 1 ? Float32(py[2] - py[1]) : 1.0f0
+    xsp = gnx > 1 ? Float32(px[2] - px[1]) : 1.0f0
+    yy = Vector{Float32}(y)
+    xx = Vector{Float32}(x)
+    nu = Matrix{Float32}(undef, ny, nx)
+    nv = Matrix{Float32}(undef, ny, nx)
+    check(ccall((:hh_apply_predictor, LIB), Int32,
+                (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Int32, Int32, Float32, Float32, Float32, Float32,
+                 Ptr{Float32}, Int32, Ptr{Float32}, Int32, Ptr{Float32}, Ptr{Float32}, Ptr{Float32}, Ptr{Float32}),
+                ctx.ctx.ptr, pu, pv, gny, gnx, Float32(py[1]), ysp, Float32(px[1]), xsp, yy, ny, xx, nx, nu, nv,
+                C_NULL, C_NULL), ctx.ctx.ptr)
+    r = _B200Pair(ctx.ctx, ctx.imgsize...)
+    return r, r, T.(nu), T.(nv)
+end
+
+# The pair an engine correlates: the context's resident (deformed) pair, or
+# host images of a non-deforming pass, uploaded here.
+function _engine_pair!(e::_B200Engine, imgA, imgB, mask)
+    imgA isa _B200Pair || _stage!(e.ctx, imgA, imgB)
+    if mask === nothing
+        check(ccall((:hh_stage_mask, LIB), Int32, (Ptr{Cvoid}, Ptr{UInt8}), e.ctx.ptr, C_NULL), e.ctx.ptr)
+    else
+        M = Matrix{UInt8}(mask)
+        check(ccall((:hh_stage_mask, LIB), Int32, (Ptr{Cvoid}, Ptr{UInt8}), e.ctx.ptr, M), e.ctx.ptr)
+    end
+    return nothing
+end
+
+_job_matrix(jobs) = Int32[j[k] for k in 1:4, j in jobs]  # 4 x njobs, 1-based (gi, gj, rs, cs)
+
+function process_windows!(u, v, peak_ratio, correlation_moment, alt_u, alt_v, uncertainty_u, uncertainty_v, jobs,
+                          imgA, imgB, params::PIVParameters, engine::_B200Engine,
+                          mask::Union{Nothing,AbstractMatrix{Bool}} = nothing, planes = nothing)
+    planes === nothing ||
+        throw(ArgumentError("backend :b200 does not support correlation-plane storage yet; use backend = :cpu"))
+    jobvec = jobs isa AbstractVector ? jobs : collect(jobs)
+    njobs = length(jobvec)
+    njobs == 0 && return nothing
+    _engine_pair!(engine, imgA, imgB, mask)
+    K = max(params.n_peaks, 2)
+    J = _job_matrix(jobvec)
+    out = Matrix{Float32}(undef, 5 + 2 * (K - 1), njobs)  # packed rows of src/ka_backend.jl:497-506
+    want_uq = uncertainty_u !== nothing
+    stats = want_uq ? Matrix{Float64}(undef, 2 * UQ_NSTATS, njobs) : nothing
+    check(ccall((:hh_process_windows, LIB), Int32,
+                (Ptr{Cvoid}, Ref{PassDesc}, Ptr{Int32}, Int64, Ptr{Float32}, Ptr{Int32}, Ptr{Float64}),
+                engine.ctx.ptr, engine.desc, J, njobs, out, C_NULL,
+                want_uq ? pointer(stats) : Ptr{Float64}(C_NULL)), engine.ctx.ptr)
+    T = eltype(u)
+    nalt = K - 1
+    for m in 1:njobs
+        gi, gj = jobvec[m][1], jobvec[m][2]
+        u[gi, gj] = out[1, m]
+        v[gi, gj] = out[2, m]
+        peak_ratio[gi, gj] = out[3, m]
+        correlation_moment[gi, gj] = out[4, m]
+        if want_uq
+            uncertainty_u[gi, gj] = finalize_uncertainty(T, view(stats, 1:UQ_NSTATS, m))
+            uncertainty_v[gi, gj] = finalize_uncertainty(T, view(stats, (UQ_NSTATS + 1):(2 * UQ_NSTATS), m))
+        end
+        if alt_u !== nothing
+            found = Int(out[5, m])
+            for mm in 2:min(found, params.n_peaks)
+                alt_u[gi, gj, mm - 1] = out[5 + (mm - 1), m]
+                alt_v[gi, gj, mm - 1] = out[5 + nalt + (mm - 1), m]
+            end
+        end
+    end
+    return nothing
+end
+
+function uncertainty_sweep!(uncertainty_u, uncertainty_v, jobs, imgA, imgB, params::PIVParameters, apod, mask,
+                            engine::_B200Engine)
+    jobvec = jobs isa AbstractVector ? jobs : collect(jobs)
+    njobs = length(jobvec)
+    njobs == 0 && return nothing
+    _engine_pair!(engine, imgA, imgB, mask)
+    J = _job_matrix(jobvec)
+    K = max(params.n_peaks, 2)
+    out = Matrix{Float32}(undef, 5 + 2 * (K - 1), njobs)
+    stats = Matrix{Float64}(undef, 2 * UQ_NSTATS, njobs)
+    check(ccall((:hh_process_windows, LIB), Int32,
+                (Ptr{Cvoid}, Ref{PassDesc}, Ptr{Int32}, Int64, Ptr{Float32}, Ptr{Int32}, Ptr{Float64}),
+                engine.ctx.ptr, engine.desc, J, njobs, out, C_NULL, stats), engine.ctx.ptr)
+    T = eltype(uncertainty_u)
+    for m in 1:njobs
+        gi, gj = jobvec[m][1], jobvec[m][2]
+        uncertainty_u[gi, gj] = finalize_uncertainty(T, view(stats, 1:UQ_NSTATS, m))
+        uncertainty_v[gi, gj] = finalize_uncertainty(T, view(stats, (UQ_NSTATS + 1):(2 * UQ_NSTATS), m))
+    end
+    return nothing
+end
+
+# Ensemble trio over the hook entry points: each pair's planes of a pass come
+# back from hh_correlation_planes and are summed in pair order on the host
+# (accum[j] .+= plane, src/ensemble.jl:317-343); the summed planes are
+# analysed by hh_analyze_planes. run_piv_ensemble_b200 keeps the sums on the
+# device instead.
+struct _B200Planes
+    sums::Array{Float32,3}  # (nr, nc, njobs)
+end
+
+function _plane_accumulator(engine::_B200Engine, params::PIVParameters, ::Type{T}, njobs::Int) where {T}
+    f = params.padding ? 2 : 1
+    return _B200Planes(zeros(Float32, f * params.search_area_size[1], f * params.search_area_size[2], njobs))
+end
+_uncertainty_accumulator(::_B200Engine, ::Type, njobs::Int) = zeros(Float64, 2 * UQ_NSTATS, njobs)
+_uncertainty_scratch(::_B200Engine, ::Type) = nothing
+
+function accumulate_planes!(acc::_B200Planes, jobrange::AbstractUnitRange, engine::_B200Engine, imgA, imgB, jobs,
+                            params::PIVParameters, mask, uacc = nothing, uscratch = nothing)
+    isempty(jobrange) && return nothing
+    _engine_pair!(engine, imgA, imgB, mask)
+    sub = jobs[jobrange]
+    J = _job_matrix(sub)
+    nr, nc = size(acc.sums, 1), size(acc.sums, 2)
+    pl = Array{Float32,3}(undef, nr, nc, length(sub))
+    check(ccall((:hh_correlation_planes, LIB), Int32,
+                (Ptr{Cvoid}, Ref{PassDesc}, Ptr{Int32}, Int64, Ptr{Float32}),
+                engine.ctx.ptr, engine.desc, J, length(sub), pl), engine.ctx.ptr)
+    acc.sums[:, :, jobrange] .+= pl
+    if uacc !== nothing
+        K = max(params.n_peaks, 2)
+        out = Matrix{Float32}(undef, 5 + 2 * (K - 1), length(sub))
+        stats = Matrix{Float64}(undef, 2 * UQ_NSTATS, length(sub))
+        check(ccall((:hh_process_windows, LIB), Int32,
+                    (Ptr{Cvoid}, Ref{PassDesc}, Ptr{Int32}, Int64, Ptr{Float32}, Ptr{Int32}, Ptr{Float64}),
+                    engine.ctx.ptr, engine.desc, J, length(sub), out, C_NULL, stats), engine.ctx.ptr)
+        uacc[:, jobrange] .+= stats
+    end
+    return nothing
+end
+
+function ensemble_analyze!(acc::_B200Planes, engine::_B200Engine, u, v, peak_ratio, correlation_moment,
+                           uncertainty_u, uncertainty_v, planes, alt_u, alt_v, jobs, params::PIVParameters, uacc)
+    planes === nothing ||
+        throw(ArgumentError("backend :b200 does not support correlation-plane storage yet; use backend = :cpu"))
+    njobs = length(jobs)
+    K = max(params.n_peaks, 2)
+    nr, nc = size(acc.sums, 1), size(acc.sums, 2)
+    out = Matrix{Float32}(undef, 5 + 2 * (K - 1), njobs)
+    check(ccall((:hh_analyze_planes, LIB), Int32,
+                (Ptr{Cvoid}, Ptr{Float32}, Int64, Int32, Int32, Int32, Int32, Int32, Ptr{Float32}, Ptr{Int32}),
+                engine.ctx.ptr, acc.sums, njobs, nr, nc, params.n_peaks, params.peak_finder === :exclusion ? 1 : 0,
+                SUBPIXEL[params.subpixel_method], out, C_NULL), engine.ctx.ptr)
+    T = eltype(u)
+    nalt = K - 1
+    for (j, job) in enumerate(jobs)
+        gi, gj = job[1], job[2]
+        if alt_u !== nothing
+            for m in 2:min(Int(out[5, j]), params.n_peaks)  # total = shared predictor + residual
+                alt_u[gi, gj, m - 1] = u[gi, gj] + out[5 + (m - 1), j]
+                alt_v[gi, gj, m - 1] = v[gi, gj] + out[5 + nalt + (m - 1), j]
+            end
+        end
+        u[gi, gj] += out[1, j]
+        v[gi, gj] += out[2, j]
+        peak_ratio[gi, gj] = out[3, j]
+        correlation_moment[gi, gj] = out[4, j]
+        if uacc !== nothing
+            uncertainty_u[gi, gj] = finalize_uncertainty(T, view(uacc, 1:UQ_NSTATS, j))
+            uncertainty_v[gi, gj] = finalize_uncertainty(T, view(uacc, (UQ_NSTATS + 1):(2 * UQ_NSTATS), j))
+        end
+    end
+    return nothing
 end
 
 # ---- ensemble (sum-of-correlation) PIV: hh_run_ensemble ------------------

@@ -108,8 +108,12 @@ const char* hh_last_error(const hh_ctx* ctx);
 hh_status hh_pass_validate(const hh_pass_desc* p);
 
 /* Reject options the device path does not implement, before any work:
- * replaces _check_backend_params / _ka_scope_check (src/ka_backend.jl:13-29),
- * except that enlarged (square) search areas are accepted. */
+ * replaces _check_backend_params / _ka_scope_check (src/ka_backend.jl:13-29).
+ * Wider than the reference's device backends: enlarged search areas,
+ * rectangular windows and search areas, and every FFT plane whose lengths
+ * factor into primes up to 61 (at most 4194304 points) are accepted;
+ * rejected are subpixel_method :gauss2d, keep_correlation_planes,
+ * n_peaks > 8 and UOD neighbourhoods above 4. */
 hh_status hh_check_backend_params(const hh_pass_desc* passes, int32_t npasses);
 
 /* Interrogation grid of one pass: replaces pass_grid (src/pipeline.jl:529-555).
@@ -225,6 +229,13 @@ hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npair
 hh_status hh_autotune_correlation(hh_ctx* ctx, const hh_pass_desc* pass, int32_t reps, float* variant_ms,
                                   int32_t* best);
 hh_status hh_set_corr_variant(hh_ctx* ctx, int32_t fft_size, int32_t window, int32_t variant);
+/* 1 when a fused shared-memory correlation kernel (the shapes the
+ * autotuner chooses between) serves the pass: square windows and search
+ * areas of FFT size 16, 24, 32, 48, 64, 96 or 128; 0 when the general-shape
+ * kernel does (any other window or search-area shape, rectangular ones and
+ * planes that exceed a CTA's shared memory, such as the 256 x 256 planes of
+ * padded 128-px windows). Host-only; no counterpart in the reference. */
+int32_t hh_corr_fused(const hh_pass_desc* p);
 
 /* Cross-process reduction of the ensemble sums (multi-GPU ensemble: each
  * process holds a share of the pairs). The reference sums every plane on one
@@ -291,6 +302,14 @@ hh_status hh_apply_predictor(hh_ctx* ctx, const float* pu, const float* pv, int3
                              float y0, float ysp, float x0, float xsp, const float* y, int32_t ny,
                              const float* x, int32_t nx, float* node_u, float* node_v, float* warpA,
                              float* warpB);
+
+/* The image mask (nr x nc of the staged pair, column-major uint8, nonzero =
+ * excluded) of the next hh_process_windows / hh_correlation_planes calls:
+ * masked pixels leave the window means and enter as zero (load_windows!,
+ * src/correlators.jl:188-263; the mask argument of process_windows!,
+ * ext/HammerheadCUDAExt.jl:303-308). NULL clears it; hh_stage_pair clears
+ * it too. */
+hh_status hh_stage_mask(hh_ctx* ctx, const uint8_t* mask);
 
 /* process_windows!: correlate the jobs of one pass on the current (warped
  * or raw) staged pair and return the packed per-window scalars, layout of

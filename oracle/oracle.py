@@ -294,8 +294,8 @@ def correlation_plane(subA, subB, params, dtype=np.float32):
         A = np.zeros((sr, sc), T, order="F")
         A[orr:orr + wr, oc:oc + wc] = subA
         pa = ctypes.cast(A.ctypes.data + (orr + oc * sr) * A.itemsize, ctypes.POINTER(ct))
-    n = 2 * params.search_area_size[0] if params.padding else params.search_area_size[0]
-    R = np.empty((n, n), T, order="F")
+    f = 2 if params.padding else 1
+    R = np.empty((f * params.search_area_size[0], f * params.search_area_size[1]), T, order="F")
     d = to_pass(params)
     _fn("correlation_plane", suf)(pa, _p(B, ct), ctypes.c_int64(B.shape[0]), ctypes.byref(d), _p(R, ct))
     return R
@@ -455,3 +455,56 @@ def run_ensemble(pairs, passes, mask=None, mask_threshold=0.5, predictor_smoothi
     out["outliers"] = outl.astype(bool)
     out["mask"] = gm.astype(bool)
     return out
+
+
+class Params:
+    """A pass configuration with the fields and defaults of the reference's
+    PIVParameters (src/types.jl:212-291), for callers of the oracle that do
+    not load the device library (the CPU legs of the benchmark). No
+    validation beyond what the C restatement does."""
+
+    def __init__(self, window_size=(32, 32), search_area_size=None, overlap=(16, 16), correlation_method="cross",
+                 padding=False, apodization="none", subpixel_method="gauss3", n_peaks=3, peak_finder="regionalmax",
+                 uncertainty=False, uod_enable=True, uod_threshold=2.0, uod_neighborhood=2, min_peak_ratio=1.0,
+                 validation=(), replace_outliers=True, max_iterations=1, convergence_tol=0.05,
+                 keep_correlation_planes=False):
+        pair = lambda v: (int(v), int(v)) if np.isscalar(v) else (int(v[0]), int(v[1]))  # noqa: E731
+        self.window_size = pair(window_size)
+        self.search_area_size = self.window_size if search_area_size is None else pair(search_area_size)
+        self.overlap = pair(overlap)
+        self.correlation_method = correlation_method
+        self.padding = bool(padding)
+        self.apodization = apodization
+        self.subpixel_method = subpixel_method
+        self.n_peaks = int(n_peaks)
+        self.peak_finder = peak_finder
+        self.uncertainty = bool(uncertainty)
+        self.uod_enable = bool(uod_enable)
+        self.uod_threshold = float(uod_threshold)
+        self.uod_neighborhood = int(uod_neighborhood)
+        self.min_peak_ratio = float(min_peak_ratio)
+        self.validation = tuple(validation)
+        self.replace_outliers = bool(replace_outliers)
+        self.max_iterations = int(max_iterations)
+        self.convergence_tol = float(convergence_tol)
+        self.keep_correlation_planes = bool(keep_correlation_planes)
+
+
+def multipass(window_sizes, overlap_fraction=0.5, final=None, **kw):
+    """multipass_parameters (src/pipeline.jl:509-524): one pass per window
+    size, overlap floor(w * fraction), `final` merged into the last pass."""
+    out = []
+    for i, w in enumerate(window_sizes):
+        extra = dict(kw)
+        if i == len(window_sizes) - 1:
+            extra.update(final or {})
+        w = (w, w) if np.isscalar(w) else tuple(w)
+        out.append(Params(window_size=w, overlap=(int(w[0] * overlap_fraction), int(w[1] * overlap_fraction)),
+                          **extra))
+    return out
+
+
+def final_vectors(shape, passes, mask=None, thr=0.5):
+    """Unmasked cells of the final pass grid (pass_grid, src/pipeline.jl:529-555)."""
+    ny, nx, gm, _ = pass_grid(shape, passes[-1], mask, thr)
+    return int(gm.size - gm.sum())

@@ -938,21 +938,15 @@ static T field_change(const T* u, const T* v, const T* pu, const T* pv, const ui
 // ---------------------------------------------------------------------------
 // Deformation: Interpolations.jl BSpline(Cubic(Line(OnGrid()))) restated.
 // Padded (nr+2) x (nc+2) coefficient array; logical index k at parent k+1.
-constexpr i64 BS_SEG = 64, BS_WARM = 32;
-
 template <class T> static void bspline_line(T* x, i64 n, i64 stride) {
   // Solve, on the padded index set 1..n (n = m + 2):
   //   row 1: c1 - 2c2 + c3 = 0;   rows 2..n-1: (c_{i-1} + 4c_i + c_{i+1})/6 = b_i;
   //   row n: c_{n-2} - 2c_{n-1} + c_n = 0
   // with b_1 = b_n = 0 (zero padding). Eliminating the boundary rows gives
   // c2 = b2, c_{n-1} = b_{n-1}, a tridiagonal [1 4 1]/6 interior system, and
-  // c1 = 2c2 - c3, cn = 2c_{n-1} - c_{n-2}. Solved in T by the Thomas
-  // algorithm; the elimination factors inv_k = 1/den_k and cp_k = inv_k/6
-  // do not depend on the data. Both sweeps are contractions (|cp_k| -> 0.268),
-  // so the line is processed in independent segments of BS_SEG unknowns, each
-  // sweep started BS_WARM unknowns early from a zero state (the neglected
-  // term is below 0.268^32 ~ 5e-19 of the value, far under FP32 rounding);
-  // the device kernels use the same segmentation, unknown for unknown.
+  // c1 = 2c2 - c3, cn = 2c_{n-1} - c_{n-2}. The interior system is solved in
+  // T over the whole line by one forward and one backward Thomas sweep, with
+  // elimination factors inv_k = 1/den_k and cp_k = inv_k/6.
   auto X = [&](i64 i) -> T& { return x[(i - 1) * stride]; };
   if (n < 4) return;
   const T sixth = T(1) / T(6), four6 = T(4) / T(6);
@@ -960,7 +954,7 @@ template <class T> static void bspline_line(T* x, i64 n, i64 stride) {
   T c2 = X(2), cn1 = X(n - 1);
   if (hi >= lo) {
     const i64 m = hi - lo + 1;
-    std::vector<T> cp(m), inv(m), dp(m), xs(m);
+    std::vector<T> cp(m), inv(m), dp(m);
     for (i64 k = 0; k < m; ++k) {
       T den = k == 0 ? four6 : four6 - sixth * cp[k - 1];
       inv[k] = T(1) / den;
@@ -972,23 +966,16 @@ template <class T> static void bspline_line(T* x, i64 n, i64 stride) {
       if (k == m - 1) r -= sixth * cn1;
       return r;
     };
-    for (i64 k0 = 0; k0 < m; k0 += BS_SEG) {  // forward, per segment
-      const i64 k1 = std::min(m, k0 + BS_SEG), ks = std::max<i64>(0, k0 - BS_WARM);
-      T d = 0;
-      for (i64 k = ks; k < k1; ++k) {
-        d = k == 0 ? rhs(k) * inv[0] : (rhs(k) - sixth * d) * inv[k];
-        if (k >= k0) dp[k] = d;
-      }
+    T d = 0;
+    for (i64 k = 0; k < m; ++k) {  // forward sweep
+      d = k == 0 ? rhs(k) * inv[0] : (rhs(k) - sixth * d) * inv[k];
+      dp[k] = d;
     }
-    for (i64 k0 = 0; k0 < m; k0 += BS_SEG) {  // backward, per segment
-      const i64 k1 = std::min(m, k0 + BS_SEG), ke = std::min(m - 1, k1 - 1 + BS_WARM);
-      T xv = 0;
-      for (i64 k = ke; k >= k0; --k) {
-        xv = k == ke ? dp[k] : dp[k] - cp[k] * xv;
-        if (k < k1) xs[k] = xv;
-      }
+    T xv = 0;
+    for (i64 k = m - 1; k >= 0; --k) {  // backward sweep
+      xv = k == m - 1 ? dp[k] : dp[k] - cp[k] * xv;
+      X(lo + k) = xv;
     }
-    for (i64 k = 0; k < m; ++k) X(lo + k) = xs[k];
   }
   X(2) = c2;
   X(n - 1) = cn1;

@@ -52,3 +52,38 @@ class Grid:
     def __init__(self, d):
         for k in ("x", "y", "u", "v", "mask", "outliers"):
             setattr(self, k, d[k])
+
+
+def plane_decision_margin(R, locs_a, locs_b, k, finder="regionalmax", excl=2):
+    """Smallest gap, in the plane R, between two values whose order decides
+    the peaks a finder reports: consecutive values of the ranked candidates
+    (the first k + 1), each reported location (of either result) against its
+    neighbourhood (8 neighbours for regional maxima, the exclusion box for the
+    exclusion finder), and each secondary value against zero. Two planes that
+    differ by at most e element-wise can report different peaks only when
+    this margin is at most 2 e (src/localmax.jl:3-19, src/correlators.jl:390-454)."""
+    import oracle
+
+    nr, nc = R.shape
+    R64 = np.asarray(R, np.float64)
+    cand = oracle.find_peaks(R64, k + 1, finder, excl)
+    vals = [v for v, _ in cand]
+    gaps = [abs(vals[i] - vals[i + 1]) for i in range(len(vals) - 1)]
+    gaps += [abs(v) for v in vals[1:k + 1]]
+    rad = 1 if finder == "regionalmax" else excl
+    locs = set()
+    for L in (locs_a, locs_b):
+        L = np.asarray(L).ravel()
+        for m in range(0, len(L) - 1, 2):
+            r, c = int(L[m]), int(L[m + 1])
+            if 1 <= r <= nr and 1 <= c <= nc:
+                locs.add((r, c))
+    for r, c in locs:
+        r0, r1 = max(r - 1 - rad, 0), min(r + rad, nr)
+        c0, c1 = max(c - 1 - rad, 0), min(c + rad, nc)
+        box = R64[r0:r1, c0:c1].copy()
+        box[r - 1 - r0, c - 1 - c0] = -np.inf
+        nb = box.max() if box.size > 1 else -np.inf
+        if np.isfinite(nb):
+            gaps.append(abs(R64[r - 1, c - 1] - nb))
+    return min(gaps) if gaps else np.inf

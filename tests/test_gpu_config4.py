@@ -42,10 +42,13 @@ def test_config4_cut_against_oracle(hb, orc, ws):
         A, B = _f32(frames[k]), _f32(frames[k + 1])
         r = hb.run_piv(A, B, passes, workspace=ws)
         o = orc.run_piv(A, B, passes, nthreads=8)
-        valid = ~(o["outliers"] | o["mask"]) & ~(r.outliers | r.mask)
-        du, dv = np.abs(r.u - o["u"])[valid], np.abs(r.v - o["v"])[valid]
-        assert np.quantile(du, 0.999) <= TOL_PX and np.quantile(dv, 0.999) <= TOL_PX
-        assert int((r.outliers != o["outliers"]).sum()) <= 2
+        # flags identical, every vector within the parity tolerance
+        assert np.array_equal(r.mask, o["mask"])
+        flips = np.argwhere(r.outliers != o["outliers"])
+        assert len(flips) == 0, f"outlier flags differ at {flips[:10].tolist()}"
+        ok = ~o["mask"]
+        du, dv = np.abs(r.u - o["u"])[ok], np.abs(r.v - o["v"])[ok]
+        assert du.max() <= TOL_PX and dv.max() <= TOL_PX, (du.max(), dv.max())
         assert list(r.sweeps) == list(o["sweeps"])
         both = np.isfinite(r.uncertainty_u) & np.isfinite(o["uncertainty_u"])
         assert both.mean() > 0.9
@@ -58,9 +61,9 @@ def test_config4_cut_against_oracle(hb, orc, ws):
     e = hb.run_piv_ensemble([(frames[0], frames[1]), (frames[1], frames[2])], passes, workspace=ws)
     oe = orc.run_ensemble([(_f32(frames[0]), _f32(frames[1])), (_f32(frames[1]), _f32(frames[2]))], passes,
                           nthreads=8)
-    both = ~(e.outliers | oe["outliers"])
-    assert np.quantile(np.abs(e.u - oe["u"])[both], 0.99) <= TOL_PX
-    assert np.quantile(np.abs(e.v - oe["v"])[both], 0.99) <= TOL_PX
+    flips = np.argwhere(e.outliers != oe["outliers"])
+    assert len(flips) == 0, f"outlier flags differ at {flips[:10].tolist()}"
+    assert np.abs(e.u - oe["u"]).max() <= TOL_PX and np.abs(e.v - oe["v"]).max() <= TOL_PX
     assert _truth_rms(e, flow) < 0.3
 
 

@@ -28,13 +28,13 @@ def test_ensemble_matches_oracle(hb, orc, ws):
     passes = hb.multipass_parameters([32, 16], padding=True, uncertainty=True)
     e = hb.run_piv_ensemble(pairs, passes, workspace=ws)
     o = orc.run_ensemble(pairs, passes, nthreads=8)
-    both = ~(e.outliers | o["outliers"])
-    du = np.abs(e.u - o["u"])[both]
-    dv = np.abs(e.v - o["v"])[both]
-    assert np.quantile(du, 0.99) <= 1e-3 and np.quantile(dv, 0.99) <= 1e-3
-    assert (e.outliers != o["outliers"]).sum() <= 2
-    fin = np.isfinite(e.uncertainty_u) & np.isfinite(o["uncertainty_u"])
-    assert fin.mean() > 0.9
+    # the planes of every pair are summed in pair order on both sides: flags
+    # identical and every vector within the parity tolerance
+    flips = np.argwhere(e.outliers != o["outliers"])
+    assert len(flips) == 0, f"outlier flags differ at {flips[:10].tolist()}"
+    assert np.abs(e.u - o["u"]).max() <= 1e-3 and np.abs(e.v - o["v"]).max() <= 1e-3
+    fin = np.isfinite(e.uncertainty_u)
+    assert np.array_equal(fin, np.isfinite(o["uncertainty_u"])) and fin.mean() > 0.9
     assert np.quantile(np.abs(e.uncertainty_u - o["uncertainty_u"])[fin], 0.99) < 1e-3
 
 

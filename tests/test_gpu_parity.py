@@ -13,7 +13,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import Grid, particle_pair, random_positions, shear_pair
+from helpers import Grid, particle_pair, plane_decision_margin, random_positions, shear_pair
 
 pytestmark = pytest.mark.gpu
 
@@ -124,38 +124,56 @@ def test_correlation_planes_and_peaks(ws, orc, hb, hooks, pair256, kw):
     planes = sess.correlation_planes(p, jobs)
     out, locs, _ = sess.process_windows(p, jobs, want_locs=True)
     w = p.window_size[0]
-    K = max(p.n_peaks, 2)
-    near_ties = 0
+    near_ties = []
     # the phase method divides every bin by its magnitude, so FFT round-off in
     # bins of small magnitude reaches the plane at full weight: 2.9e-5 of the
     # peak is seen for unapodized 16 px windows, against ~3e-7 for the cross
     # method
     ptol = 1e-4 if p.correlation_method == "phase" else 2e-5
+    close = 0
     for q, (gi, gj, rs, cs) in enumerate(jobs):
         sa = A[rs - 1:rs - 1 + w, cs - 1:cs - 1 + w]
         sb = B[rs - 1:rs - 1 + w, cs - 1:cs - 1 + w]
         R = orc.correlation_plane(sa, sb, p)
         scale = np.abs(R).max()
-        assert np.abs(planes[q] - R).max() <= ptol * scale + 1e-12
+        err = float(np.abs(planes[q] - R).max())
+        assert err <= ptol * scale + 1e-12
         ref, rl = orc.analyze_plane(R, p.n_peaks, p.peak_finder, p.subpixel_method)
         f = int(ref[4])
+        margin = plane_decision_margin(R, rl[:2 * f], locs[q, :2 * int(out[q, 4])], p.n_peaks, p.peak_finder)
+        close += margin <= 1e-6 * scale
         if int(out[q, 4]) != f or not np.array_equal(locs[q, :2 * f], rl[:2 * f]):
-            # only admissible where two candidate peaks are within FFT round-off
-            vals = np.sort(R.ravel())[::-1]
-            assert abs(vals[0] - vals[1]) < 1e-4 * scale or f > 1, (q, out[q], ref)
-            near_ties += 1
+            # admissible only where two values whose order decides the peaks
+            # are closer than the two planes' own difference allows to resolve
+            assert margin <= 2 * err, (q, margin, err, out[q], ref)
+            near_ties.append((q, margin / scale, rl[:2 * f].tolist(), locs[q, :2 * f].tolist()))
             continue
         np.testing.assert_allclose(out[q, :2], ref[:2], atol=TOL_PX)
         np.testing.assert_allclose(out[q, 3], ref[3], rtol=1e-3, atol=1e-6, equal_nan=True)
-    assert near_ties <= max(1, len(jobs) // 50)
+    print(f"{len(jobs)} windows: {len(near_ties)} near-tie peak differences {near_ties}; "
+          f"{close} windows with a decision margin below 1e-6 of the peak")
+    assert len(near_ties) <= max(1, len(jobs) // 50)
 
 
 # --- deformation ----------------------------------------------------------------------
 
-def test_deformation_matches_oracle(ws, orc, hooks, hb):
+def _deform_close(w, o):
+    """The oracle solves each B-spline line in one Thomas sweep (the system
+    Interpolations' Cubic(Line(OnGrid())) prefilter solves); the device cuts
+    the sweeps into 64-unknown segments that start 32 unknowns early from
+    zero. The neglected term is below 0.268^32 ~ 5e-19 of the value, so the
+    two agree to float rounding: at most 4 ulp of the image scale (1 here),
+    and in practice bit for bit at almost every pixel."""
+    d = np.abs(w.astype(np.float64) - o)
+    assert d.max() <= 4 * np.spacing(np.float32(1.0)), d.max()
+    print(f"deformed pixels identical to the oracle: {np.mean(w == o):.6f}, max |diff| {d.max():.3g}")
+
+
+@pytest.mark.parametrize("shape", [(96, 128), (300, 260)])
+def test_deformation_matches_oracle(ws, orc, hooks, hb, shape):
     rng = np.random.default_rng(9)
-    A = rng.uniform(size=(96, 128)).astype(np.float32)
-    B = rng.uniform(size=(96, 128)).astype(np.float32)
+    A = rng.uniform(size=shape).astype(np.float32)
+    B = rng.uniform(size=shape).astype(np.float32)
     py = np.array([16.5, 48.5, 80.5], np.float32)
     px = np.array([16.5, 48.5, 80.5, 112.5], np.float32)
     pu = np.array([[0.8 * math.sin(0.05 * a) + 0.3 * math.cos(0.04 * b) for b in px] for a in py], np.float32)
@@ -168,11 +186,14 @@ def test_deformation_matches_oracle(ws, orc, hooks, hb):
     cA = orc.prefilter(A)
     cB = orc.prefilter(B)
     oA, oB = orc.deform(cA, cB, A.shape, pu, pv, py, px)
-    assert np.array_equal(wA, oA) and np.array_equal(wB, oB)
+    _deform_close(wA, oA)
+    _deform_close(wB, oB)
     # FP64 oracle: the FP32 device deformation stays within float round-off
     dA, _ = orc.deform(orc.prefilter(A, np.float64), orc.prefilter(B, np.float64), A.shape, pu, pv, py, px,
                        dtype=np.float64)
-    assert np.abs(wA - dA).max() < 2e-5
+    # FP32 rounding of the coefficients (the prefilter amplifies white noise
+    # by about sqrt(3)) and of the 16-tap sums of each sample
+    assert np.abs(wA - dA).max() < 4e-5
     for i, yy in enumerate(gy):
         for j, xx in enumerate(gx):
             import oracle as _o
@@ -312,15 +333,40 @@ def test_uq_statistics(ws, orc, hb, hooks, pair256, w):
 
 # --- end to end ---------------------------------------------------------------------------
 
-def _compare_runs(r_dev, r_orc, tol=TOL_PX, max_flag_diff=0):
-    valid = ~(r_orc["outliers"] | r_orc["mask"]) & ~(r_dev.outliers | r_dev.mask)
+def _compare_runs(r_dev, r_orc, tol=TOL_PX):
+    """A device run against the oracle's Float32 run of the same schedule:
+    grid masks, validation flags and sweep counts identical, and every vector
+    valid in both within `tol` px (no quantile: the maximum)."""
     assert np.array_equal(r_dev.mask, r_orc["mask"])
+    assert np.all(np.isnan(r_dev.u[r_dev.mask]))
+    flips = np.argwhere(r_dev.outliers != r_orc["outliers"])
+    assert len(flips) == 0, f"outlier flags differ at {flips[:10].tolist()}"
+    assert list(r_dev.sweeps) == list(r_orc["sweeps"])
+    valid = ~(r_orc["outliers"] | r_orc["mask"])
     du = np.abs(r_dev.u - r_orc["u"])[valid]
     dv = np.abs(r_dev.v - r_orc["v"])[valid]
-    assert np.all(np.isnan(r_dev.u[r_dev.mask]))
-    nflag = int((r_dev.outliers != r_orc["outliers"]).sum())
-    assert nflag <= max_flag_diff, nflag
+    assert du.max() <= tol and dv.max() <= tol, (du.max(), dv.max())
+    # replaced outliers are medians of valid neighbours: the same tolerance
+    out = r_orc["outliers"] & ~r_orc["mask"]
+    if out.any():
+        assert np.abs(r_dev.u - r_orc["u"])[out].max() <= tol and np.abs(r_dev.v - r_orc["v"])[out].max() <= tol
+    print(f"grid {r_dev.u.shape}: flags identical, max |du| {du.max():.2e}, max |dv| {dv.max():.2e}")
     return du, dv
+
+
+def _compare_uncertainty(r_dev, r_orc, q=0.99, tol=1e-3):
+    """Uncertainty: the same finite cells, and all but 1 % within `tol`.
+    finalize_uncertainty (src/uncertainty.jl:162-179) takes a ring of the
+    covariance sums only while its largest entry reaches 0.05 S00; where a
+    ring sits at that threshold, float round-off of the sums decides whether
+    it counts and sigma jumps, so the comparison is by quantile."""
+    fin = np.isfinite(r_dev.uncertainty_u)
+    assert np.array_equal(fin, np.isfinite(r_orc["uncertainty_u"]))
+    assert np.array_equal(np.isfinite(r_dev.uncertainty_v), np.isfinite(r_orc["uncertainty_v"]))
+    if fin.any():
+        assert np.quantile(np.abs(r_dev.uncertainty_u - r_orc["uncertainty_u"])[fin], q) < tol
+        fv = np.isfinite(r_dev.uncertainty_v)
+        assert np.quantile(np.abs(r_dev.uncertainty_v - r_orc["uncertainty_v"])[fv], q) < tol
 
 
 def test_run_piv_config0(hb, orc, ws):
@@ -329,9 +375,7 @@ def test_run_piv_config0(hb, orc, ws):
     p = hb.PIVParameters(window_size=32, overlap=16)
     r = hb.run_piv(A, B, p, workspace=ws)
     o = orc.run_piv(A, B, p)
-    du, dv = _compare_runs(r, o)
-    assert du.max() <= TOL_PX and dv.max() <= TOL_PX
-    assert np.array_equal(r.outliers, o["outliers"])
+    _compare_runs(r, o)
     assert hb.rms_error(r, flow) < 0.1
 
 
@@ -342,13 +386,9 @@ def test_run_piv_config1(hb, orc, ws):
                                      final=dict(max_iterations=3, uncertainty=True))
     r = hb.run_piv(A, B, passes, workspace=ws)
     o = orc.run_piv(A, B, passes, nthreads=8)
-    du, dv = _compare_runs(r, o, max_flag_diff=2)
-    assert np.quantile(du, 0.999) <= TOL_PX and np.quantile(dv, 0.999) <= TOL_PX
+    _compare_runs(r, o)
+    _compare_uncertainty(r, o)
     assert hb.rms_error(r, flow) <= 0.05
-    both = np.isfinite(r.uncertainty_u) & np.isfinite(o["uncertainty_u"])
-    assert both.mean() > 0.95
-    assert np.quantile(np.abs(r.uncertainty_u - o["uncertainty_u"])[both], 0.99) < 1e-3
-    assert list(r.sweeps) == list(o["sweeps"])
 
 
 def test_run_piv_iterated_equals_repeated(hb, ws):
@@ -368,8 +408,7 @@ def test_run_piv_mask_and_shear(hb, orc, ws):
     passes = hb.multipass_parameters([64, 32, 16, 16], padding=True, apodization="gauss")
     r = hb.run_piv(A, B, passes, mask=mask, workspace=ws)
     o = orc.run_piv(A, B, passes, mask=mask)
-    du, dv = _compare_runs(r, o, max_flag_diff=1)
-    assert du.max() <= TOL_PX and dv.max() <= TOL_PX
+    _compare_runs(r, o)
     assert r.mask.any()
 
 
@@ -384,3 +423,37 @@ def test_run_piv_device_inputs(hb, ws):
     dB = torch.from_numpy(np.ascontiguousarray(B.T)).cuda().T
     r_dev = hb.run_piv(dA, dB, p, workspace=ws)
     assert np.array_equal(r_host.u, r_dev.u) and np.array_equal(r_host.v, r_dev.v)
+
+
+# --- the mixed batch's second schedule: [48, 24], padded, Gaussian, 3 sweeps, UQ ----------
+
+def _cut(a, n=1024):
+    return np.asfortranarray(a[:n, :n])
+
+
+@pytest.mark.parametrize("shape", [(512, 512), (768, 1024), (2048, 2048)], ids=["512", "768x1024", "2048cut"])
+def test_run_piv_48_24_against_oracle(hb, orc, ws, shape):
+    """The [48, 24] schedule of the mixed batch (48- and 96-point transforms in
+    the first pass, 48-point in the final one, up to three sweeps,
+    uncertainty) end to end against the oracle's Float32 run, on the first
+    pair of each image size of the batch (a 1024 x 1024 cut of the 2048^2
+    pair). The device's deviation from the oracle's FP64 run is also the
+    Float32 algorithm's own: it is bounded by the deviation of the oracle's
+    Float32 run from its FP64 run (plus the 1e-3 px parity tolerance)."""
+    syn = hb.synthetic
+    sp = next(s for s in syn.config3_pairs() if s["shape"] == shape)
+    A, B = syn.particle_pair(sp["shape"], sp["flow"], seed=sp["seed"])
+    if shape[0] > 1024:
+        A, B = _cut(A), _cut(B)
+    passes = hb.multipass_parameters([48, 24], padding=True, apodization="gauss",
+                                     final=dict(max_iterations=3, uncertainty=True))
+    r = hb.run_piv(A, B, passes, workspace=ws)
+    o = orc.run_piv(A, B, passes, nthreads=8)
+    _compare_runs(r, o)
+    _compare_uncertainty(r, o)
+    o64 = orc.run_piv(A, B, passes, nthreads=8, dtype=np.float64)
+    ok = ~(r.outliers | o64["outliers"] | r.mask)
+    e_dev = np.maximum(np.abs(r.u - o64["u"]), np.abs(r.v - o64["v"]))[ok]
+    e_f32 = np.maximum(np.abs(o["u"] - o64["u"]), np.abs(o["v"] - o64["v"]))[ok]
+    print(f"deviation from FP64: device {e_dev.max():.3g} px, Float32 oracle {e_f32.max():.3g} px")
+    assert e_dev.max() <= e_f32.max() + TOL_PX

@@ -10,7 +10,7 @@ is the parity target, with the tolerances of the equal-area parity tests.
 import numpy as np
 import pytest
 
-from helpers import shear_pair
+from helpers import plane_decision_margin, shear_pair
 
 pytestmark = pytest.mark.gpu
 
@@ -59,7 +59,7 @@ def test_search_planes_and_peaks(ws, orc, hb, hooks, far_pair, kw):
     n = planes.shape[1]
     assert n == (2 * s if p.padding else s)
     phase = p.correlation_method == "phase"
-    near_ties = 0
+    near_ties = []
     for q, (gi, gj, rs, cs) in enumerate(jobs):
         sa = A[rs - 1:rs - 1 + w, cs - 1:cs - 1 + w]
         sb = B[rs - 1 - m:rs - 1 + w + m, cs - 1 - m:cs - 1 + w + m]
@@ -83,22 +83,28 @@ def test_search_planes_and_peaks(ws, orc, hb, hooks, far_pair, kw):
         ref, rl = orc.analyze_plane(R, p.n_peaks, p.peak_finder, p.subpixel_method)
         f = int(ref[4])
         if int(out[q, 4]) != f or not np.array_equal(locs[q, :2 * f], rl[:2 * f]):
-            vals = np.sort(R.ravel())[::-1]
-            assert abs(vals[0] - vals[1]) < (4e-3 if phase else 1e-4) * scale or f > 1, (q, out[q], ref)
-            near_ties += 1
+            # admissible only where two values whose order decides the peaks
+            # are closer than the two planes' own difference allows to resolve
+            err = float(np.abs(planes[q] - R).max())
+            margin = plane_decision_margin(R, rl[:2 * f], locs[q, :2 * int(out[q, 4])], p.n_peaks, p.peak_finder)
+            assert margin <= 2 * err, (q, margin, err, out[q], ref)
+            near_ties.append((q, margin / scale, rl[:2 * f].tolist(), locs[q, :2 * f].tolist()))
             continue
         np.testing.assert_allclose(out[q, :2], ref[:2], atol=TOL_PX)
         np.testing.assert_allclose(out[q, 3], ref[3], rtol=1e-3, atol=1e-6, equal_nan=True)
+    print(f"{len(jobs)} windows: {len(near_ties)} near-tie peak differences {near_ties}")
     # phase planes carry round-off of 1e-3 of the peak, so more candidate
     # peaks are tied within it
-    assert near_ties <= max(1, len(jobs) // (20 if phase else 50))
+    assert len(near_ties) <= max(1, len(jobs) // (20 if phase else 50))
 
 
-def _compare(r, o, tol=TOL_PX, max_flag_diff=0):
+def _compare(r, o, tol=TOL_PX):
+    """Grid masks and outlier flags identical; every vector within tol px."""
     assert np.array_equal(r.mask, o["mask"])
-    valid = ~(o["outliers"] | o["mask"]) & ~(r.outliers | r.mask)
-    assert np.abs(r.u - o["u"])[valid].max() <= tol and np.abs(r.v - o["v"])[valid].max() <= tol
-    assert int((r.outliers != o["outliers"]).sum()) <= max_flag_diff
+    flips = np.argwhere(r.outliers != o["outliers"])
+    assert len(flips) == 0, f"outlier flags differ at {flips[:10].tolist()}"
+    ok = ~o["mask"]
+    assert np.abs(r.u - o["u"])[ok].max() <= tol and np.abs(r.v - o["v"])[ok].max() <= tol
 
 
 def test_search_run_piv_large_shift(hb, orc, ws, far_pair):
@@ -121,7 +127,7 @@ def test_search_multipass_mask_and_uncertainty(hb, orc, ws):
                                uncertainty=True, max_iterations=2)]
     r = hb.run_piv(A, B, passes, mask=mask, workspace=ws)
     o = orc.run_piv(A, B, passes, mask=mask)
-    _compare(r, o, max_flag_diff=1)
+    _compare(r, o)
     assert r.mask.any()
     both = np.isfinite(r.uncertainty_u) & np.isfinite(o["uncertainty_u"])
     assert both.any()
@@ -149,9 +155,8 @@ def test_search_ensemble(hb, orc, ws):
     p = hb.PIVParameters(window_size=16, search_area_size=32, overlap=8)
     e = hb.run_piv_ensemble(pairs, p, workspace=ws)
     o = orc.run_ensemble(pairs, [p], nthreads=8)
+    _compare(e, o)
     both = ~(e.outliers | o["outliers"])
-    assert np.quantile(np.abs(e.u - o["u"])[both], 0.99) <= TOL_PX
-    assert np.quantile(np.abs(e.v - o["v"])[both], 0.99) <= TOL_PX
     assert np.quantile(np.hypot(e.u - 5.7, e.v - 4.9)[both], 0.95) < 0.15
 
 

@@ -100,12 +100,21 @@ def test_backend_scope_check(hb):
     ok = hb.multipass_parameters([64, 32, 16], padding=True, apodization="gauss", final=dict(uncertainty=True))
     hb.check_backend_params(ok)
     hb.check_backend_params([hb.PIVParameters(window_size=16, search_area_size=48, overlap=8)])
+    # the reference's effort=:high preset (128 px padded windows, 256 x 256
+    # planes) and any other window or search-area shape whose FFT lengths
+    # factor into primes up to 61: the general-shape kernel
+    hb.check_backend_params(hb.effort_schedule("high"))
+    for kw in [dict(window_size=16, search_area_size=40, overlap=8),
+               dict(window_size=16, search_area_size=(48, 32), overlap=8),
+               dict(window_size=(32, 16), overlap=(8, 8), padding=True, uncertainty=True),
+               dict(window_size=20, overlap=10, uncertainty=True),
+               dict(window_size=128, overlap=64, padding=True, apodization="gauss", uncertainty=True),
+               dict(window_size=(56, 44), overlap=(28, 22), correlation_method="phase")]:
+        hb.check_backend_params([hb.PIVParameters(**kw)])
     for kw, msg in [(dict(subpixel_method="gauss2d"), "gauss2d"),
-                    (dict(window_size=16, search_area_size=40, overlap=8), "search area 40"),
-                    (dict(window_size=16, search_area_size=(48, 32), overlap=8), "square search areas"),
                     (dict(keep_correlation_planes=True), "keep_correlation_planes"),
-                    (dict(window_size=(32, 16), overlap=(8, 8)), "square"),
-                    (dict(window_size=20, overlap=10), "no correlation kernel"),
+                    (dict(window_size=67, overlap=10), "prime factors of at most 61"),
+                    (dict(window_size=(1200, 1200), overlap=(600, 600), padding=True), "FFT plane of 2400 x 2400"),
                     (dict(n_peaks=9), "at most 8"),
                     (dict(uod_neighborhood=5), "uod_neighborhood")]:
         with pytest.raises(hb.ArgumentError, match=msg):
