@@ -277,6 +277,70 @@ def adjoint_bench(hb, ws, torch, stream, dev_time, reps):
             "windows": int(((A.shape[0] - 16) // 8 + 1) * ((A.shape[1] - 16) // 8 + 1))}
 
 
+def timeseries_leg(hb, ws, torch, dev_time, npairs=8, reps=3, cut_check=True):
+    """The large-frame time series: chained 4096^2 frames (12-bit counts in
+    UInt16, 0.01 ppp, noise 0.05, Poiseuille 6 px), passes [128, 64, 32, 16]
+    with the final pass at 75 % overlap, three sweeps and uncertainty; a
+    bounded run of `npairs` chained pairs (frames resident on the device,
+    UInt16 converted on the device) in the batched and the plain per-pair
+    form, final-pass vectors/s of each; the RMS error against the flow; and
+    the device's deviation from the oracle's FP64 run on a 1024^2 cut.
+    Beside it, the reference's effort = :high preset ([128, 64, 32] padded,
+    2 sweeps, uncertainty) on one 4096^2 pair, ms per pair, the case the
+    reference publishes for its own GPU path."""
+    syn = hb.synthetic
+    frames, flow = syn.config4_frames(npairs + 1, seed=1004)
+    passes = hb.multipass_parameters([128, 64, 32]) + [
+        hb.PIVParameters(window_size=16, overlap=12, max_iterations=3, uncertainty=True)]
+    dev16 = [torch.from_numpy(np.ascontiguousarray(f.T)).cuda().T for f in frames]
+    dev32 = [(t.float() / 65535.0) for t in dev16]  # value / 65535, as the batched form converts UInt16
+    pairs16 = [(dev16[k], dev16[k + 1]) for k in range(npairs)]
+    runner = hb.BatchRunner(pairs16, passes, workspace=ws)
+    runner.run(read=False)
+    ms_b = dev_time(lambda: runner.run(read=False), reps)
+    runner.run()
+    res = runner.results(copy=True)
+    runner.close()
+    nvec = sum(int(r.u.size - r.mask.sum()) for r in res)
+
+    def plain():
+        for k in range(npairs):
+            hb.run_piv(dev32[k], dev32[k + 1], passes, workspace=ws)
+    plain()
+    ms_p = dev_time(plain, 1)
+    X, Y = np.meshgrid(res[0].x, res[0].y)
+    ut, vt = flow(X, Y)
+    ok = ~(res[0].outliers | res[0].mask)
+    rms = float(np.sqrt(np.mean((res[0].u - ut)[ok] ** 2 + (res[0].v - vt)[ok] ** 2)))
+    out = {"config": f"{npairs} chained 4096x4096 UInt16 pairs, [128,64,32] + 16 px at 75 % overlap, 3 sweeps + UQ",
+           "final_pass_vectors": nvec,
+           "batched": {"value": nvec / (ms_b / 1e3), "unit": UNIT, "ms_per_pair": ms_b / npairs},
+           "plain": {"value": nvec / (ms_p / 1e3), "unit": UNIT, "ms_per_pair": ms_p / npairs},
+           "batched_speedup": ms_p / ms_b, "rms_px_pair0": rms, "outlier_fraction_pair0": float(res[0].outliers.mean())}
+    # effort = :high on one 4096^2 pair (the reference's published 4096^2 case)
+    hi = hb.effort_schedule("high")
+    A, B = dev32[0], dev32[1]
+    hb.run_piv(A, B, hi, workspace=ws)
+    ms_hi = dev_time(lambda: hb.run_piv(A, B, hi, workspace=ws), reps)
+    out["effort_high_4096"] = {
+        "ms_per_pair": ms_hi, "schedule": "[128,64,32] padded + gauss, 2 sweeps per pass, UQ in the final pass",
+        "reference_published_s_per_pair": {"RTX 2000 Ada, Float32, batch 8192": 2.98,
+                                           "RX 6800 XT, Float32, steady state": 3.29}}
+    if cut_check:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        a = np.asfortranarray(frames[0][:1024, :1024].astype(np.float32) / np.float32(65535))
+        b = np.asfortranarray(frames[1][:1024, :1024].astype(np.float32) / np.float32(65535))
+        r = hb.run_piv(a, b, passes, workspace=ws)
+        o = oracle.run_piv(a, b, passes, nthreads=os.cpu_count() or 1, dtype=np.float64)
+        ok = ~(r.outliers | r.mask | o["outliers"] | o["mask"])
+        d = np.concatenate([np.abs(r.u - o["u"])[ok], np.abs(r.v - o["v"])[ok]]).astype(np.float64)
+        out["fp64_oracle_error_1024_cut"] = {"components": int(d.size), "max_abs_px": float(d.max()),
+                                             "rms_px": float(np.sqrt(np.mean(d * d)))}
+    return out
+
+
 # ---------------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
@@ -290,6 +354,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison step")
     ap.add_argument("--limit", type=int, default=None, help="use only the first N pairs (debugging)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default correlation CTA shapes")
+    ap.add_argument("--no-timeseries", action="store_true", help="skip the 4096^2 time-series leg")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -420,6 +485,9 @@ def main():
     # ---- differentiation: loss + adjoint gradient over the full predictor field
     adj = adjoint_bench(hb, ws, torch, stream, dev_time, max(args.steps, 5))
 
+    # ---- the large-frame time series (4096^2 UInt16 chained pairs)
+    ts = None if args.no_timeseries else timeseries_leg(hb, ws, torch, dev_time, cut_check=rank == 0)
+
     # ---- roofline of the dominant kernel (the fused correlation)
     c = prof["correlate"]
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
@@ -467,6 +535,7 @@ def main():
                                 "peak": hbm_peak, "unit": "GB/s"},
             "kernel_share": shares,
             "adjoint": adj,
+            "timeseries_4096": ts,
             "autotune": {k.split("|", 1)[1]: {"variant": e["variant"], "ms": [round(m, 4) for m in e["ms"]]}
                          for k, e in tuned.items()},
             "clocks": clk.summary(sm_max),

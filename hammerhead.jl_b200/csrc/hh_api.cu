@@ -981,6 +981,12 @@ static void drop_plans(hh_ctx* ctx) {  // batched graphs captured with an older 
   ctx->bplans.clear();
 }
 
+extern "C" hh_status hh_debug_fail_alloc(hh_ctx* ctx, int64_t after) {
+  if (!ctx) return fail(nullptr, HH_ERR_ARG, "context is NULL");
+  ctx->fail_alloc_after = after < 0 ? -1 : after;
+  return HH_OK;
+}
+
 extern "C" int32_t hh_corr_fused(const hh_pass_desc* p) { return p && corr_special(*p) ? 1 : 0; }
 
 extern "C" hh_status hh_set_corr_variant(hh_ctx* ctx, int32_t fft_size_, int32_t window, int32_t variant) {

@@ -97,7 +97,7 @@ static void free_plan(void* vp) {
 
 template <class T> static hh_status plan_alloc(hh_ctx* ctx, BPlan& P, size_t count, T** out) {
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+  cudaError_t e = ctx_malloc(ctx, &p, std::max<size_t>(count, 1) * sizeof(T));
   if (e != cudaSuccess)
     return fail(ctx, HH_ERR_OOM, std::string("device allocation of ") + std::to_string(count * sizeof(T)) +
                                      " bytes for the batched plan failed: " + cudaGetErrorString(e));
@@ -392,7 +392,7 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
     for (auto& c : S.classes) {
       c.njobs = (int64_t)c.hjobs.size() / 4;
       void* d = nullptr;
-      HH_CK(cudaMalloc(&d, std::max<size_t>(c.hjobs.size(), 1) * sizeof(int32_t)));
+      HH_CK(ctx_malloc(ctx, &d, std::max<size_t>(c.hjobs.size(), 1) * sizeof(int32_t)));
       c.jobs = static_cast<int32_t*>(d);
       HH_CK(cudaMemcpy(c.jobs, c.hjobs.data(), c.hjobs.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
       c.hjobs.clear();

@@ -58,6 +58,10 @@ struct hh_ctx {
   const float* curB = nullptr;
   bool staged = false;
   const uint8_t* hook_mask = nullptr;  // image mask of the hook calls (hh_stage_mask), device
+  // host-side allocation-failure injection (hh_debug_fail_alloc): the
+  // allocation attempt that brings the count to zero fails with HH_ERR_OOM
+  // as a failing cudaMalloc would; negative = off
+  int64_t fail_alloc_after = -1;
   // timing of the last schedule
   std::vector<float> pass_ms;
   std::vector<int32_t> pass_sweeps;
@@ -120,6 +124,16 @@ inline std::string num(double x) {
   return o.str();
 }
 
+// cudaMalloc through the context, with the injected failure of
+// hh_debug_fail_alloc (no device call is made for an injected failure).
+inline cudaError_t ctx_malloc(hh_ctx* ctx, void** p, size_t bytes) {
+  if (ctx && ctx->fail_alloc_after >= 0 && ctx->fail_alloc_after-- == 0) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
 // Device buffer by name, grown on demand (never shrunk): a steady state of
 // equally sized calls allocates nothing.
 template <class T> hh_status buf(hh_ctx* ctx, const char* name, size_t count, T** out) {
@@ -129,7 +143,7 @@ template <class T> hh_status buf(hh_ctx* ctx, const char* name, size_t count, T*
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.bytes = 0;
-    cudaError_t e = cudaMalloc(&b.p, need);
+    cudaError_t e = ctx_malloc(ctx, &b.p, need);
     if (e != cudaSuccess)
       return fail(ctx, HH_ERR_OOM, std::string("device allocation of ") + std::to_string(need) + " bytes for " + name +
                                        " failed: " + cudaGetErrorString(e));

@@ -189,6 +189,7 @@ SIGNATURES = [
     ("hh_set_profiling", ctypes.c_int32, [_CTX, ctypes.c_int32]),
     ("hh_profile_read", ctypes.c_int32, [_CTX, ctypes.POINTER(hh_kernel_profile), ctypes.c_int32]),
     ("hh_launch_count", ctypes.c_int64, [_CTX]),
+    ("hh_debug_fail_alloc", ctypes.c_int32, [_CTX, ctypes.c_int64]),
     ("hh_field_change_noalloc", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
       ctypes.c_void_p, ctypes.c_void_p]),

@@ -216,13 +216,35 @@ def run_piv_batch(pairs, passes, *, masks=None, predictor_smoothing=True, mask_t
     `pairs`: list of (A, B) images (numpy (rows, cols) arrays, or column-major
     torch CUDA tensors); `passes`: one schedule (a PIVParameters or a list of
     them) for every pair, or one schedule per pair; `masks`: None or one mask
-    (or None) per pair."""
-    runner = BatchRunner(pairs, passes, masks=masks, predictor_smoothing=predictor_smoothing,
-                         mask_threshold=mask_threshold, workspace=workspace, graph=graph, pinned=False)
+    (or None) per pair.
+
+    A batch whose device storage does not fit (the library reports
+    HH_ERR_OOM and releases what it had allocated) is split in halves that run
+    one after the other, down to single pairs; the results are the same, as
+    every pair's result is independent of its batch. This is the bounded
+    sub-batch of the reference's device backends (the memory-aware batch cap,
+    ext/HammerheadCUDAExt.jl:147-164) taken on demand."""
+    if not pairs:
+        raise ArgumentError("pairs must not be empty")
+    n = len(pairs)
     try:
-        return runner.run().results(copy=True)
-    finally:
-        runner.close()
+        runner = BatchRunner(pairs, passes, masks=masks, predictor_smoothing=predictor_smoothing,
+                             mask_threshold=mask_threshold, workspace=workspace, graph=graph, pinned=False)
+        try:
+            return runner.run().results(copy=True)
+        finally:
+            runner.close()
+    except _lib.HammerheadError as e:
+        if e.status != _lib.HH_ERR_OOM or n == 1:
+            raise
+    uniq, index = _schedules(passes, n)
+    per_pair = [uniq[k] for k in index]
+    masks = [None] * n if masks is None else list(masks)
+    h = n // 2
+    kw = dict(predictor_smoothing=predictor_smoothing, mask_threshold=mask_threshold, workspace=workspace,
+              graph=graph)
+    return (run_piv_batch(pairs[:h], per_pair[:h], masks=masks[:h], **kw) +
+            run_piv_batch(pairs[h:], per_pair[h:], masks=masks[h:], **kw))
 
 
 def run_piv_sequence(pairs, params=None, *, preprocess=None, progress=False, on_result=None, mask=None,

@@ -381,6 +381,16 @@ hh_status hh_profile_read(hh_ctx* ctx, hh_kernel_profile* out /* HH_K_CLASSES en
 /* Kernels launched on ctx since creation (all classes, profiling or not). */
 int64_t hh_launch_count(const hh_ctx* ctx);
 
+/* Failure injection for tests of the out-of-memory path (no counterpart in
+ * the reference; host side only, no device fault): the device allocation
+ * attempt `after` calls from now (0 = the next one) through the context's
+ * arena or a batched plan fails with HH_ERR_OOM exactly as a failing
+ * cudaMalloc would, without calling it; later allocations proceed. A
+ * negative value switches the injection off. The failing call leaves the
+ * context usable: its partly built plan or buffer is released and the next
+ * call allocates again. */
+hh_status hh_debug_fail_alloc(hh_ctx* ctx, int64_t after);
+
 /* ---- Allocation-free convergence norm (no counterpart in the reference) --
  *
  * For callers that must not have the library allocate device memory: a host

@@ -325,3 +325,59 @@ def test_batch_stream_error_leaves_session_usable(hb, ws):
     for k in range(2):
         for a, b in zip(out[k], hb.run_piv_batch(good[k], sched, workspace=ws)):
             _same(a, b)
+
+
+def test_allocation_failure_leaves_context_usable(hb, ws):
+    """An injected device-allocation failure (host side, hh_debug_fail_alloc)
+    surfaces as HH_ERR_OOM; the context then runs the next call normally,
+    with the same results as before."""
+    L = hb._lib.lib()
+    syn = hb.synthetic
+    A, B = syn.particle_pair((256, 224), syn.sine_shear_flow(2.0, 160.0), seed=901)
+    passes = hb.multipass_parameters([32, 16], padding=True, final=dict(max_iterations=2, uncertainty=True))
+    w = hb.piv_workspace()
+    try:
+        ref = hb.run_piv(A, B, passes, workspace=ws)
+        L.hh_debug_fail_alloc(w.ctx, 0)  # the first allocation of the fresh context fails
+        with pytest.raises(hb.HammerheadError) as ei:
+            hb.run_piv(A, B, passes, workspace=w)
+        assert ei.value.status == hb._lib.HH_ERR_OOM
+        again = hb.run_piv(A, B, passes, workspace=w)
+        for k in ("u", "v", "uncertainty_u"):
+            assert np.array_equal(getattr(again, k), getattr(ref, k), equal_nan=True), k
+        # a failure inside a batched plan: the plan is released, the next call rebuilds it
+        pairs = [(A, B), syn.particle_pair((192, 256), syn.uniform_flow(1.5, 0.5), seed=902)]
+        runner = hb.BatchRunner(pairs, passes, workspace=w)
+        try:
+            L.hh_debug_fail_alloc(w.ctx, 3)
+            with pytest.raises(hb.HammerheadError) as ei:
+                runner.run()
+            assert ei.value.status == hb._lib.HH_ERR_OOM
+        finally:
+            runner.close()
+        L.hh_debug_fail_alloc(w.ctx, -1)
+        res = hb.run_piv_batch(pairs, passes, workspace=w)
+        assert np.array_equal(res[0].u, ref.u, equal_nan=True)
+    finally:
+        L.hh_debug_fail_alloc(w.ctx, -1)
+        w.close()
+
+
+def test_batch_splits_on_allocation_failure(hb, ws):
+    """run_piv_batch falls back to half batches when the whole batch's plan
+    cannot be allocated; the results equal the unsplit batch."""
+    L = hb._lib.lib()
+    syn = hb.synthetic
+    pairs = [syn.particle_pair((192, 192), syn.uniform_flow(0.5 * i, -0.3 * i), seed=910 + i) for i in range(4)]
+    passes = hb.multipass_parameters([32, 16], padding=True, final=dict(max_iterations=2))
+    whole = hb.run_piv_batch(pairs, passes, workspace=ws)
+    w = hb.piv_workspace()
+    try:
+        L.hh_debug_fail_alloc(w.ctx, 0)  # the first (whole-batch) plan fails; the halves succeed
+        split = hb.run_piv_batch(pairs, passes, workspace=w)
+        for a, b in zip(whole, split):
+            assert np.array_equal(a.u, b.u, equal_nan=True) and np.array_equal(a.v, b.v, equal_nan=True)
+            assert np.array_equal(a.outliers, b.outliers)
+    finally:
+        L.hh_debug_fail_alloc(w.ctx, -1)
+        w.close()
