@@ -648,29 +648,37 @@ __device__ __forceinline__ float2 cross_spectrum(float2 X, float2 Zm, int method
 // ---------------------------------------------------------------------------
 // W is the extent of the data: the window, or with SRCH the frame-B search
 // area that holds the (runtime) frame-A window at its centre. VAR selects the
-// CTA shape (windows per CTA, threads per window, register budget): 0 the
-// default, 1 the alternative the autotuner times against it (the same
-// arithmetic on another thread mapping, so the results are identical).
+// CTA shape (windows per CTA, threads per window) and register budget (CTAs
+// per SM the registers are sized for) among the four the autotuner times:
+// 0 the default shape and budget, 1 the alternative shape, 2 the default
+// shape with one CTA per SM more in the budget (fewer registers, more warps),
+// 3 the default shape with one CTA less (more registers, no spills) -- or,
+// where the default budget is one CTA, the alternative shape with one CTA
+// more. All compute the same arithmetic on another thread mapping or
+// register allocation, so the results are identical.
 template <int N, int W, bool SRCH = false, int VAR = 0> struct CorrCfg {
   static constexpr int N1 = AxisSplit<N>::N1, N2 = AxisSplit<N>::N2;
+  // budget of the default shape; shape of this variant (0 default, 1 alternative)
+  static constexpr int MINB0 = (N == 32 && W == 16) ? 3 : (N <= 48 ? 4 : (N <= 64 ? 3 : (N <= 96 ? 2 : 1)));
+  static constexpr int SH = (VAR == 1 || (VAR == 3 && MINB0 == 1)) ? 1 : 0;
   // 16 x 16 windows padded to 32: every stage of the plane has at most 16
   // lines (16 data columns, 16 canonical column items, 16 row pairs), so
   // half a warp serves a window and each warp carries two
-  static constexpr bool HALF = VAR == 0 && N == 32 && W == 16;
+  static constexpr bool HALF = SH == 0 && N == 32 && W == 16;
   // alternatives: N <= 32 one window per warp in CTAs of 4 (half-warp
   // windows) or 8 warps; N = 48 a 3-CTA register budget; N = 64 one window
   // per 256-thread CTA; N = 96 512 threads and N = 128 256 threads per window
-  static constexpr int WPC = VAR == 0 ? (HALF ? 8 : (N <= 32 ? 4 : (N <= 64 ? 2 : 1)))  // windows per CTA
-                                      : (N <= 32 ? (N == 32 && W == 16 ? 4 : 8) : (N <= 48 ? 2 : 1));
-  static constexpr int NT = VAR == 0 ? (N <= 48 ? 128 : (N <= 96 ? 256 : 512))
-                                     : (N <= 32 ? (N == 32 && W == 16 ? 128 : 256)
-                                                : (N <= 48 ? 128 : (N <= 64 ? 256 : (N <= 96 ? 512 : 256))));
+  static constexpr int WPC = SH == 0 ? (HALF ? 8 : (N <= 32 ? 4 : (N <= 64 ? 2 : 1)))  // windows per CTA
+                                     : (N <= 32 ? (N == 32 && W == 16 ? 4 : 8) : (N <= 48 ? 2 : 1));
+  static constexpr int NT = SH == 0 ? (N <= 48 ? 128 : (N <= 96 ? 256 : 512))
+                                    : (N <= 32 ? (N == 32 && W == 16 ? 128 : 256)
+                                               : (N <= 48 ? 128 : (N <= 64 ? 256 : (N <= 96 ? 512 : 256))));
   static constexpr int G = NT / WPC;  // threads per window
-  // CTAs per SM the register budget is sized for (the shared-memory limit
-  // allows at least this many)
-  static constexpr int MINB = VAR == 0 ? (HALF ? 3 : (N <= 48 ? 4 : (N <= 64 ? 3 : (N <= 96 ? 2 : 1))))
-                                       : (N <= 32 ? (N == 32 && W == 16 ? 4 : 2)
-                                                  : (N <= 48 ? 3 : (N <= 64 ? 3 : 1)));
+  // CTAs per SM the register budget is sized for
+  static constexpr int MINB_SH = SH == 0 ? MINB0
+                                         : (N <= 32 ? (N == 32 && W == 16 ? 4 : 2) : (N <= 48 ? 3 : (N <= 64 ? 3 : 1)));
+  static constexpr int MINB = VAR == 2 ? MINB0 + 1
+                                       : (VAR == 3 ? (MINB0 > 1 ? MINB0 - 1 : MINB_SH + 1) : MINB_SH);
   // the peak analysis inline (one window per CTA: its latency is the CTA's)
   static constexpr bool INLINE_ANALYSIS = N >= 96;
   // Canonical column c sits at storage column N2 (c % N1) + c / N1, and with
@@ -1351,8 +1359,12 @@ cudaError_t launch_correlate(const CorrArgs& a, int N, int W, cudaStream_t s, in
 #define X(n, w)                                                                         \
   if (N == n && W == w) {                                                              \
     if (a.win > 0 && a.win < w) return launch_nw<n, w, true, 0>(a, s, num_sms);       \
-    return a.variant == 1 ? launch_nw<n, w, false, 1>(a, s, num_sms)                   \
-                          : launch_nw<n, w, false, 0>(a, s, num_sms);                  \
+    switch (a.variant) {                                                               \
+      case 1: return launch_nw<n, w, false, 1>(a, s, num_sms);                         \
+      case 2: return launch_nw<n, w, false, 2>(a, s, num_sms);                         \
+      case 3: return launch_nw<n, w, false, 3>(a, s, num_sms);                         \
+      default: return launch_nw<n, w, false, 0>(a, s, num_sms);                        \
+    }                                                                                  \
   }
   HH_CORR_CASES(X)
 #undef X

@@ -136,6 +136,7 @@ extern "C" const char* hh_noalloc_last_error(void) { return g_noalloc_err.c_str(
 
 extern "C" hh_status hh_field_change_noalloc(const float* d_u, const float* d_v, const float* d_pu, const float* d_pv,
                                              const uint8_t* d_mask, int64_t n, float* d_change, void* stream) {
+  g_noalloc_err.clear();  // the message describes this call's failure only
   if (n > kMaxVectors)
     return fail(HH_ERR_ARG, "hh_field_change_noalloc: " + std::to_string(n) + " vectors exceed the fixed scratch of " +
                                 std::to_string(kMaxVectors) + " (HH_NOALLOC_MAX_VECTORS); use hh_field_change");

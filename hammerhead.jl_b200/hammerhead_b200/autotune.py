@@ -19,7 +19,7 @@ from . import _lib
 from ._lib import ArgumentError
 from .params import PIVParameters
 
-VARIANTS = 2  # HH_CORR_VARIANTS
+VARIANTS = 4  # HH_CORR_VARIANTS
 
 
 def _flatten(passes):

@@ -215,8 +215,9 @@ hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npair
 
 /* ---- Autotuning of the correlation kernel --------------------------------
  * The correlation kernel of each (FFT size, window) comes in
- * HH_CORR_VARIANTS CTA shapes (windows per CTA, threads per window,
- * register budget); all compute the same results. hh_autotune_correlation
+ * HH_CORR_VARIANTS variants: two CTA shapes (windows per CTA, threads per
+ * window) and, for the default shape, register budgets of one CTA per SM
+ * more and one less; all compute the same results. hh_autotune_correlation
  * times every shape on the windows of `pass` over the staged pair
  * (hh_stage_pair first), `reps` launches each, interleaved, writes the mean
  * ms per launch of each shape into variant_ms (HH_CORR_VARIANTS entries)
@@ -225,7 +226,7 @@ hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npair
  * example from a cache of earlier tuning). Both drop the context's batched
  * plans, whose graphs hold the old choice. Enlarged search areas have one
  * shape. No counterpart in the reference. */
-#define HH_CORR_VARIANTS 2
+#define HH_CORR_VARIANTS 4
 hh_status hh_autotune_correlation(hh_ctx* ctx, const hh_pass_desc* pass, int32_t reps, float* variant_ms,
                                   int32_t* best);
 hh_status hh_set_corr_variant(hh_ctx* ctx, int32_t fft_size, int32_t window, int32_t variant);
@@ -406,12 +407,16 @@ hh_status hh_debug_fail_alloc(hh_ctx* ctx, int64_t after);
  * GPU that loads the library holds until the process exits (4 MiB).
  *   - n > HH_NOALLOC_MAX_VECTORS is rejected with HH_ERR_ARG.
  *   - The first call on a device looks up the scratch address for that
- *     device (the device current at the call); make that first call before
- *     any stream capture.
+ *     device (the device current at the call) and keeps it for the life of
+ *     the process; make that first call before any stream capture. Calls
+ *     after cudaDeviceReset (or any other teardown of the device's primary
+ *     context) are not supported: the kept address belongs to the old
+ *     context.
  *   - All calls on a device share the scratch; each call rewrites the
  *     entries it reads, so nothing carries over, but calls whose kernels
  *     overlap on the GPU (different streams, no ordering) race on it.
- * Errors are reported through hh_noalloc_last_error(). */
+ * Errors are reported through hh_noalloc_last_error(), which is empty after
+ * a call that succeeded. */
 #define HH_NOALLOC_MAX_VECTORS (1 << 20)
 hh_status hh_field_change_noalloc(const float* d_u, const float* d_v, const float* d_pu, const float* d_pv,
                                   const uint8_t* d_mask, int64_t n, float* d_change, void* stream);

@@ -75,7 +75,7 @@ def test_autotune_argument_errors(hb, ws):
     from hammerhead_b200 import _lib
 
     with pytest.raises(hb.ArgumentError):
-        hb.tuning.set_variant(ws, 32, 16, 2)
+        hb.tuning.set_variant(ws, 32, 16, hb.tuning.VARIANTS)
     with pytest.raises(hb.ArgumentError):
         hb.tuning.set_variant(ws, 40, 20, 0)
     syn = hb.synthetic
@@ -83,7 +83,7 @@ def test_autotune_argument_errors(hb, ws):
     A, B = _lib.as_f32_colmajor(A), _lib.as_f32_colmajor(B)
     _lib.check(_lib.lib().hh_stage_pair(ws.ctx, _lib.fptr(A), _lib.fptr(B), 128, 128), ws.ctx)
     d = hb.PIVParameters(window_size=16, search_area_size=32, overlap=8).to_desc()
-    ms = (ctypes.c_float * 2)()
+    ms = (ctypes.c_float * hb.tuning.VARIANTS)()
     best = ctypes.c_int32()
     st = _lib.lib().hh_autotune_correlation(ws.ctx, ctypes.byref(d), 2, ms, ctypes.byref(best))
     assert st == _lib.HH_ERR_ARG

