@@ -64,6 +64,8 @@ def schedule(hb, kind, uq=True):
         return hb.multipass_parameters([64, 32, 16], padding=True, apodization="gauss", final=final)
     if kind == "48-24":
         return hb.multipass_parameters([48, 24], padding=True, apodization="gauss", final=final)
+    if kind == "high":  # the reference's effort = :high preset (256 x 256 planes in its first pass)
+        return hb.effort_schedule("high")
     raise ValueError(kind)
 
 
@@ -74,6 +76,9 @@ def make_workload(hb, name, rank=0, limit=None):
     elif name == "vortex":
         specs = [dict(shape=(1024, 1024), flow=syn.lamb_oseen_flow((512.5, 512.5), 80.0, 8.0), kind=("vortex",),
                       schedule="64-32-16", seed=1001 + 100000 * rank)]
+    elif name == "effort_high":
+        specs = [dict(shape=(2048, 2048), flow=syn.lamb_oseen_flow((1024.5, 1024.5), 160.0, 8.0), kind=("vortex",),
+                      schedule="high", seed=1005 + 100000 * rank + i) for i in range(4)]
     else:
         raise ValueError(name)
     if limit:
@@ -155,6 +160,9 @@ def _load_synthetic():
 
 
 def oracle_schedule(oracle, kind, uq=True):
+    if kind == "high":
+        return oracle.multipass([128, 64, 32], padding=True, apodization="gauss", max_iterations=2,
+                                final=dict(uncertainty=uq))
     final = dict(max_iterations=3, uncertainty=uq)
     sizes = {"64-32-16": [64, 32, 16], "48-24": [48, 24]}[kind]
     return oracle.multipass(sizes, padding=True, apodization="gauss", final=final)
@@ -180,6 +188,9 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     if args.workload == "batch64":
         specs = syn.config3_pairs(seed0=1003)
+    elif args.workload == "effort_high":
+        specs = [dict(shape=(2048, 2048), flow=syn.lamb_oseen_flow((1024.5, 1024.5), 160.0, 8.0),
+                      schedule="high", seed=1005)]
     else:
         specs = [dict(shape=(1024, 1024), flow=syn.lamb_oseen_flow((512.5, 512.5), 80.0, 8.0),
                       schedule="64-32-16", seed=1001)]
@@ -215,7 +226,9 @@ def run_reference(args):
 def workload_name(w):
     return {"batch64": "mixed batch: 64 pairs (24x 512x512, 24x 768x1024, 16x 2048x2048), shear/uniform, "
                        "[64,32,16] or [48,24] padded+gauss, final 3 sweeps + UQ",
-            "vortex": "1024x1024 Lamb-Oseen vortex, [64,32,16] padded+gauss, final 3 sweeps + UQ"}[w]
+            "vortex": "1024x1024 Lamb-Oseen vortex, [64,32,16] padded+gauss, final 3 sweeps + UQ",
+            "effort_high": "4 pairs of 2048x2048 Lamb-Oseen vortex, effort=:high ([128,64,32] padded+gauss, "
+                           "2 sweeps per pass, UQ)"}[w]
 
 
 def cpu_baseline(hb, pairs, results=None, budget_s=20.0):
@@ -354,7 +367,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="batch64", choices=["batch64", "vortex"])
+    ap.add_argument("--workload", default="batch64", choices=["batch64", "vortex", "effort_high"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", action="store_true", help="time the plain per-pair form instead of the batched one")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison step")

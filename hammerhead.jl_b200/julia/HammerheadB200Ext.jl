@@ -1,5 +1,10 @@
 # Package extension that registers `backend = :b200` in Hammerhead.jl and
-# forwards the planar WIDIM path to libhammerhead_b200.so through ccall.
+# forwards the planar WIDIM path to libhammerhead_b200.so through ccall:
+# Hammerhead's own run_piv / run_piv_ensemble drive the device through the
+# backend hooks below (piv_correlation_engines, _deform_context,
+# apply_predictor, process_windows!, uncertainty_sweep!,
+# release_piv_engines!, the ensemble trio); run_piv_b200 and
+# run_piv_ensemble_b200 run a whole schedule in one library call.
 #
 # Not runnable in this repository's environment (no Julia toolchain); it is
 # written against the backend-hook contract of docs/src/reference/backends.md
