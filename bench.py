@@ -467,6 +467,18 @@ def main():
                 hb.run_piv(dA, dB, p["passes"], workspace=ws)
         plain_step()
         plain_ms = max_over_ranks(dev_time(plain_step, 1))
+    # ---- the bound on batched / plain: the batched form of the largest pairs
+    #      alone (they carry most of the windows and already fill the GPU in
+    #      the plain form), so plain_ms / this is the most batching can give
+    big_ms = None
+    if not args.plain and not args.no_plain and args.workload == "batch64":
+        big = max(p["A"].size for p in pairs)
+        sel = [i for i, p in enumerate(pairs) if p["A"].size == big]
+        if 0 < len(sel) < len(pairs):
+            rb = hb.BatchRunner([dev[i] for i in sel], [scheds[i] for i in sel], workspace=ws)
+            rb.run(read=False)
+            big_ms = max_over_ranks(dev_time(lambda: rb.run(read=False), max(3, args.steps // 2)))
+            rb.close()
 
     # ---- kernel classes: one profiled run (events around every launch, no graph)
     L.hh_set_profiling(ws.ctx, 1)
@@ -539,7 +551,9 @@ def main():
             "pairs_per_s": len(pairs) * world / (ms_max / 1e3),
             "plain_form": None if plain_ms is None else {
                 "value": nvec_total / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
-                "batched_speedup": plain_ms / ms_max},
+                "batched_speedup": plain_ms / ms_max,
+                "largest_pairs_batched_ms": big_ms,
+                "batched_speedup_bound": (plain_ms / big_ms) if big_ms else None},
             "rms_px": rms_all,
             "fp64_oracle_error": base.pop("fp64_oracle_error") if base else None,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -41,14 +41,14 @@ __device__ __forceinline__ float2 gc_tw(const float2* tw, int t, bool inv) {
 }
 
 // One radix-r Stockham stage of a length-n line: in -> out, p = product of
-// the radices before this one. Butterfly i (k = i mod p) reads in[i + m n/r],
-// applies the twiddles exp(-+2 pi i m k / (p r)), takes the r-point DFT and
-// writes out[(i - k) r + k + q p].
-__device__ __forceinline__ void gc_stage(const float2* __restrict__ in, float2* __restrict__ out, int n, int r, int p,
-                                         const float2* tw, bool inv, int lane) {
-  const int nr = n / r, tstep = n / (p * r);
+// the radices before this one (pm = p - 1 when p is a power of two, else
+// -1), nr = n / r, tstep = n / (p r). Butterfly i (k = i mod p) reads
+// in[i + m nr], applies the twiddles exp(-+2 pi i m k / (p r)), takes the
+// r-point DFT and writes out[(i - k) r + k + q p].
+__device__ __forceinline__ void gc_stage(const float2* __restrict__ in, float2* __restrict__ out, int r, int p, int pm,
+                                         int nr, int tstep, const float2* tw, bool inv, int lane) {
   for (int i = lane; i < nr; i += 32) {
-    const int k = i % p, j0 = (i - k) * r + k;
+    const int k = pm >= 0 ? (i & pm) : i % p, j0 = (i - k) * r + k;
     if (r == 2) {
       float2 x0 = in[i], x1 = in[i + nr];
       if (k) x1 = cmul(x1, gc_tw(tw, k * tstep, inv));
@@ -71,17 +71,20 @@ __device__ __forceinline__ void gc_stage(const float2* __restrict__ in, float2* 
       out[j0 + 3 * p] = make_float2(b.x - md.x, b.y - md.y);
     } else {
       // any other radix (3, 5, 7, ...): the r outputs summed directly, the
-      // twiddled inputs kept in shared-memory order (no register array)
-      const int rstep = n / r;
+      // twiddled inputs read from shared memory (no register array); the
+      // exponent e = m q mod r is stepped, not divided
+      const int rstep = nr;  // n / r
       for (int q = 0; q < r; ++q) {
         float2 acc = make_float2(0.f, 0.f);
+        int e = 0;
         for (int m = 0; m < r; ++m) {
           float2 x = in[i + m * nr];
           if (k && m) x = cmul(x, gc_tw(tw, m * k * tstep, inv));
-          const int e = (m * q) % r;
           if (e) x = cmul(x, gc_tw(tw, e * rstep, inv));
           acc.x += x.x;
           acc.y += x.y;
+          e += q;
+          if (e >= r) e -= r;
         }
         out[j0 + q * p] = acc;
       }
@@ -98,7 +101,8 @@ __device__ __forceinline__ float2* gc_line(float2* buf0, float2* buf1, int n, co
   int p = 1;
   for (int s = 0; s < nst; ++s) {
     const int r = radix[s];
-    gc_stage(in, out, n, r, p, tw, inv, lane);
+    const int nr = n / r;  // once per stage, not per butterfly
+    gc_stage(in, out, r, p, (p & (p - 1)) == 0 ? p - 1 : -1, nr, nr / p, tw, inv, lane);
     __syncwarp();
     p *= r;
     float2* t = in;
@@ -108,18 +112,11 @@ __device__ __forceinline__ float2* gc_line(float2* buf0, float2* buf1, int n, co
   return in;
 }
 
-// Lines staged per chunk so that the two line buffers fit the shared budget.
-__host__ __device__ __forceinline__ int gc_chunk(int n, size_t budget) {
-  const size_t per = 2 * (size_t)(n + 1) * sizeof(float2);
-  int c = (int)(budget / per);
-  return c > 32 ? 32 : (c < 1 ? 1 : c);
-}
-
 __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const CorrArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int NR = a.nfr, NC = a.nfc, wr = a.wr, wc = a.wc, sr = a.sr, sc = a.sc;
   const int LDR = NR + 1, LDC = NC + 1;  // staged line strides (float2)
-  const int CR = a.gc_chunk_r, CC = a.gc_chunk_c;  // lines per chunk: columns pass (length NR), rows pass (length NC)
+  const int CC = a.gc_chunk_c;  // rows-pass lines per chunk (length NC); the columns passes use a.gc_col_warps warps
   const size_t lines_b = a.gc_smem_lines;
   float2* buf0 = reinterpret_cast<float2*>(smem_raw);
   float2* buf1 = reinterpret_cast<float2*>(smem_raw + lines_b / 2);
@@ -136,7 +133,13 @@ __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const 
   const int oar = (sr - wr) / 2, oac = (sc - wc) / 2;  // frame-A window inside the search area
   const bool search = sr != wr || sc != wc;
   const float scale = 1.0f / (float)P;
-  const ScanPlan sp = scan_plan(tid, GC_THREADS, 0, NR - 1, 0, NC - 1);
+  // rows / columns of the fftshifted plane that can be nonzero; outside this
+  // box the gain (or the kept-lag restriction) makes the plane exactly zero,
+  // so its columns skip the last inverse transform and the peak scan covers
+  // the box (plus the last pixel, the one place outside where a zero can be
+  // a regional maximum), as in the fused kernels
+  const int rlo = a.gc_box[0], rhi = a.gc_box[1], clo = a.gc_box[2], chi = a.gc_box[3];
+  const ScanPlan sp = scan_plan(tid, GC_THREADS, rlo, rhi, clo, chi);
   PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
 
   for (int64_t job = blockIdx.x; job < a.njobs; job += gridDim.x) {
@@ -172,17 +175,17 @@ __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const 
 
     // ---- 1a. means over the unmasked pixels (FP64, one rounding)
     double sa = 0.0, sb = 0.0, na = 0.0, nb = 0.0;
-    for (int e = tid; e < sr * sc; e += GC_THREADS) {
-      const int i = e % sr, j = e / sr;
-      const int64_t off = (r0 + i) + (c0 + j) * ld;
-      if (M && __ldg(M + off)) continue;
-      sb += (double)__ldg(B + off);
-      nb += 1.0;
-      if ((unsigned)(i - oar) < (unsigned)wr && (unsigned)(j - oac) < (unsigned)wc) {
-        sa += (double)__ldg(A + off);
-        na += 1.0;
+    for (int j = warp; j < sc; j += GC_WARPS)  // warps on columns, lanes down the rows
+      for (int i = lane; i < sr; i += 32) {
+        const int64_t off = (r0 + i) + (c0 + j) * ld;
+        if (M && __ldg(M + off)) continue;
+        sb += (double)__ldg(B + off);
+        nb += 1.0;
+        if ((unsigned)(i - oar) < (unsigned)wr && (unsigned)(j - oac) < (unsigned)wc) {
+          sa += (double)__ldg(A + off);
+          na += 1.0;
+        }
       }
-    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       sa += __shfl_xor_sync(0xffffffffu, sa, o);
@@ -207,50 +210,52 @@ __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const 
     const float ma = tna > 0 ? (float)(ta / tna) : 0.f, mb = tnb > 0 ? (float)(tb / tnb) : 0.f;
     const bool bad = !(isfinite(ta) && isfinite(tb));  // the window holds NaN or Inf: the reference's plane is NaN
 
-    // ---- 1b. data columns j < sc of Z, transformed along the rows axis
-    for (int j0 = 0; j0 < sc; j0 += CR) {
-      const int nl = min(CR, sc - j0);
-      for (int e = tid; e < nl * NR; e += GC_THREADS) {
-        const int l = e / NR, i = e % NR, j = j0 + l;
-        float2 z = make_float2(0.f, 0.f);
-        if (i < sr && !bad) {
-          const int64_t off = (r0 + i) + (c0 + j) * ld;
-          if (!(M && __ldg(M + off))) {
-            const int ia = i - oar, ja = j - oac;
-            const bool ina = (unsigned)ia < (unsigned)wr && (unsigned)ja < (unsigned)wc;
-            if (search) {
-              z.y = __ldg(B + off) - mb;
-              if (ina) z.x = __ldg(a.apod + ia + ja * wr) * (__ldg(A + off) - ma);
-            } else {
-              const float ap = __ldg(a.apod + i + j * wr);
-              z = make_float2(ap * (__ldg(A + off) - ma), ap * (__ldg(B + off) - mb));
+    // ---- 1b. data columns j < sc of Z, transformed along the rows axis;
+    //      each warp builds, transforms and stores its own columns
+    //      (consecutive lanes on consecutive rows), so no CTA barrier is needed
+    if (warp < a.gc_col_warps) {
+      float2* l0 = buf0 + (size_t)warp * 2 * LDR;
+      float2* l1 = l0 + LDR;
+      for (int j = warp; j < sc; j += a.gc_col_warps) {
+#pragma unroll 4
+        for (int i = lane; i < NR; i += 32) {
+          float2 z = make_float2(0.f, 0.f);
+          if (i < sr && !bad) {
+            const int64_t off = (r0 + i) + (c0 + j) * ld;
+            if (!(M && __ldg(M + off))) {
+              const int ia = i - oar, ja = j - oac;
+              const bool ina = (unsigned)ia < (unsigned)wr && (unsigned)ja < (unsigned)wc;
+              if (search) {
+                z.y = __ldg(B + off) - mb;
+                if (ina) z.x = __ldg(a.apod + ia + ja * wr) * (__ldg(A + off) - ma);
+              } else {
+                const float ap = __ldg(a.apod + i + j * wr);
+                z = make_float2(ap * (__ldg(A + off) - ma), ap * (__ldg(B + off) - mb));
+              }
             }
           }
+          l0[i] = z;
         }
-        buf0[l * LDR + i] = z;
+        __syncwarp();
+        const float2* res = gc_line(l0, l1, NR, a.gc_radix_r, a.gc_nst_r, a.twr, false, lane);
+        float2* zc = Z + (int64_t)j * NR;
+        for (int i = lane; i < NR; i += 32) zc[i] = res[i];
+        __syncwarp();
       }
-      __syncthreads();
-      for (int l = warp; l < nl; l += GC_WARPS)
-        gc_line(buf0 + l * LDR, buf1 + l * LDR, NR, a.gc_radix_r, a.gc_nst_r, a.twr, false, lane);
-      __syncthreads();
-      // every line ends in the buffer the stage count's parity gives
-      const float2* res = (a.gc_nst_r & 1) ? buf1 : buf0;
-      for (int e = tid; e < nl * NR; e += GC_THREADS) {
-        const int l = e / NR, i = e % NR;
-        Z[(int64_t)(j0 + l) * NR + i] = res[l * LDR + i];
-      }
-      __syncthreads();
     }
+    __syncthreads();
 
     // ---- 2. row pairs (r, -r): forward along columns, spectrum, inverse
     const int half = NR / 2;  // rows 0..half, each with its partner (NR - r) % NR
     const int CH = CC / 2;
     for (int h0 = 0; h0 <= half; h0 += CH) {
       const int nh = min(CH, half + 1 - h0);
-      for (int e = tid; e < 2 * nh * NC; e += GC_THREADS) {
-        const int l = e % (2 * nh), j = e / (2 * nh);
-        const int ra = h0 + (l >> 1), row = (l & 1) ? (NR - ra) % NR : ra;
-        buf0[l * LDC + j] = j < sc ? Z[(int64_t)j * NR + row] : make_float2(0.f, 0.f);
+      // lanes on the chunk's rows (consecutive rows and their partners), warps
+      // on the columns: the reads of a column are two contiguous runs
+      for (int l0 = lane; l0 < 2 * nh; l0 += 32) {
+        const int ra = h0 + (l0 >> 1), row = (l0 & 1) ? (NR - ra) % NR : ra;
+        for (int j = warp; j < NC; j += GC_WARPS)
+          buf0[l0 * LDC + j] = j < sc ? Z[(int64_t)j * NR + row] : make_float2(0.f, 0.f);
       }
       __syncthreads();
       for (int l = warp; l < 2 * nh; l += GC_WARPS)
@@ -258,53 +263,68 @@ __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const 
       __syncthreads();
       float2* fz = (a.gc_nst_c & 1) ? buf1 : buf0;  // forward rows
       float2* sz = (a.gc_nst_c & 1) ? buf0 : buf1;  // spectrum rows
-      for (int e = tid; e < 2 * nh * NC; e += GC_THREADS) {
-        const int l = e / NC, k2 = e % NC;
+      for (int l = warp; l < 2 * nh; l += GC_WARPS) {
         const int ra = h0 + (l >> 1), row = (l & 1) ? (NR - ra) % NR : ra;
         const float2* Za = fz + l * LDC;          // this row
         const float2* Zb = fz + (l ^ 1) * LDC;    // its partner row (-r)
-        const float wk = a.phasew ? __ldg(a.phasew + row + (int64_t)k2 * NR) : 1.f;
-        sz[l * LDC + k2] = cross_spectrum(Za[k2], Zb[(NC - k2) % NC], a.method, wk);
+        for (int k2 = lane; k2 < NC; k2 += 32) {
+          const float wk = a.phasew ? __ldg(a.phasew + row + (int64_t)k2 * NR) : 1.f;
+          sz[l * LDC + k2] = cross_spectrum(Za[k2], Zb[k2 == 0 ? 0 : NC - k2], a.method, wk);
+        }
       }
       __syncthreads();
       for (int l = warp; l < 2 * nh; l += GC_WARPS)
         gc_line(sz + l * LDC, fz + l * LDC, NC, a.gc_radix_c, a.gc_nst_c, a.twc, true, lane);
       __syncthreads();
       float2* iz = (a.gc_nst_c & 1) ? fz : sz;
-      for (int e = tid; e < 2 * nh * NC; e += GC_THREADS) {
-        const int l = e % (2 * nh), j = e / (2 * nh);
-        const int ra = h0 + (l >> 1);
-        const int row = (l & 1) ? (NR - ra) % NR : ra;
-        if ((l & 1) && row == ra) continue;  // a self-paired row (0, NR/2) is written once
-        Z[(int64_t)j * NR + row] = iz[l * LDC + j];
+      for (int l0 = lane; l0 < 2 * nh; l0 += 32) {
+        const int ra = h0 + (l0 >> 1), row = (l0 & 1) ? (NR - ra) % NR : ra;
+        if ((l0 & 1) && row == ra) continue;  // a self-paired row (0, NR/2) is written once
+        for (int j = warp; j < NC; j += GC_WARPS) {
+          const int js = j + NC / 2 < NC ? j + NC / 2 : j + NC / 2 - NC;
+          if (js < clo || js > chi) continue;  // a column that step 3 writes as zeros
+          Z[(int64_t)j * NR + row] = iz[l0 * LDC + j];
+        }
       }
       __syncthreads();
     }
 
-    // ---- 3. columns back, then |.| / (nr nc), fftshift, gain, kept lags
-    for (int j0 = 0; j0 < NC; j0 += CR) {
-      const int nl = min(CR, NC - j0);
-      for (int e = tid; e < nl * NR; e += GC_THREADS) {
-        const int l = e / NR, i = e % NR;
-        buf0[l * LDR + i] = Z[(int64_t)(j0 + l) * NR + i];
+    // ---- 3. columns back, then |.| / (nr nc), fftshift, gain, kept lags;
+    //      columns whose shifted position lies outside the box are zero
+    const int nbox = chi - clo + 1;
+    {
+      const float z0 = bad ? __int_as_float(0x7fc00000) : 0.f;
+      for (int c = warp; c < NC - nbox; c += GC_WARPS) {
+        float* rc = R + (int64_t)((chi + 1 + c) % NC) * NR;  // columns chi+1 .. clo-1 (wrapping)
+        for (int i = lane; i < NR; i += 32) rc[i] = z0;
       }
-      __syncthreads();
-      for (int l = warp; l < nl; l += GC_WARPS)
-        gc_line(buf0 + l * LDR, buf1 + l * LDR, NR, a.gc_radix_r, a.gc_nst_r, a.twr, true, lane);
-      __syncthreads();
-      const float2* res = (a.gc_nst_r & 1) ? buf1 : buf0;
-      for (int e = tid; e < nl * NR; e += GC_THREADS) {
-        const int l = e / NR, i = e % NR, j = j0 + l;
-        const float2 c = res[l * LDR + i];
-        const int is = (i + NR / 2) % NR, js = (j + NC / 2) % NC;  // fftshifted position
-        float v = hypotf(c.x * scale, c.y * scale);
-        if (a.gain) v *= __ldg(a.gain + is + (int64_t)js * NR);
-        if (search && !(abs(is - NR / 2) <= oar && abs(js - NC / 2) <= oac)) v = 0.f;
-        if (bad) v = __int_as_float(0x7fc00000);
-        R[is + (int64_t)js * NR] = v;
-      }
-      __syncthreads();
     }
+    //      the box's columns, one warp each: unshifted column j = (js - NC/2) mod NC
+    if (warp < a.gc_col_warps) {
+      float2* l0 = buf0 + (size_t)warp * 2 * LDR;
+      float2* l1 = l0 + LDR;
+      for (int b = warp; b < nbox; b += a.gc_col_warps) {
+        const int js = clo + b, j = (js + NC - NC / 2) % NC;
+        const float2* zc = Z + (int64_t)j * NR;
+#pragma unroll 8
+        for (int i = lane; i < NR; i += 32) l0[i] = zc[i];
+        __syncwarp();
+        const float2* res = gc_line(l0, l1, NR, a.gc_radix_r, a.gc_nst_r, a.twr, true, lane);
+        float* rc = R + (int64_t)js * NR;
+        const bool colkept = !search || abs(js - NC / 2) <= oac;
+        for (int i = lane; i < NR; i += 32) {
+          const float2 c = res[i];
+          const int is = i + NR / 2 < NR ? i + NR / 2 : i + NR / 2 - NR;  // fftshifted row
+          float v = hypotf(c.x * scale, c.y * scale);
+          if (a.gain) v *= __ldg(a.gain + is + (int64_t)js * NR);
+          if (!colkept || (search && abs(is - NR / 2) > oar)) v = 0.f;
+          if (bad) v = __int_as_float(0x7fc00000);
+          rc[is] = v;
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
 
     // ---- 4. plane out (correlation_planes / ensemble sums) and analysis
     if (a.planes) {

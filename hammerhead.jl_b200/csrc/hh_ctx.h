@@ -39,6 +39,9 @@ struct Tables {
   float* phasew = nullptr;
   // support of the gain, or the kept search lags, in fftshifted rows/columns (0, 0: whole plane)
   int box_lo = 0, box_hi = 0;
+  // the same per axis for any plane shape (fftshifted rows rlo..rhi,
+  // columns clo..chi; the whole plane when there is no gain or lag limit)
+  int rlo = 0, rhi = -1, clo = 0, chi = -1;
 };
 
 }  // namespace hhd
@@ -314,11 +317,17 @@ inline hh_status get_tables(hh_ctx* ctx, const hh_pass_desc& p, Tables& t) {
   std::vector<float> ap, gn, ph;
   apod_table(wr, wc, p.apodization, ap);
   Tables nt;
+  nt.rhi = NR - 1;
+  nt.chi = NC - 1;
   HH_CK(cudaMalloc(&nt.apod, ap.size() * sizeof(float)));
   HH_CK(cudaMemcpy(nt.apod, ap.data(), ap.size() * sizeof(float), cudaMemcpyHostToDevice));
   if (sr != wr || sc != wc) {
     // enlarged search area: no overlap gain (CrossCorrelator, src/correlators.jl:73);
     // only lags with |lag| <= (S - W) / 2 are kept (restrict_search_lags!, :347-355)
+    nt.rlo = NR / 2 - (sr - wr) / 2;
+    nt.rhi = NR / 2 + (sr - wr) / 2;
+    nt.clo = NC / 2 - (sc - wc) / 2;
+    nt.chi = NC / 2 + (sc - wc) / 2;
     if (NR == NC && sr == sc && wr == wc) {
       const int m = (sr - wr) / 2;
       nt.box_lo = NR / 2 - m;
@@ -326,6 +335,23 @@ inline hh_status get_tables(hh_ctx* ctx, const hh_pass_desc& p, Tables& t) {
     }
   } else if (p.padding) {
     gain_table(wr, wc, p.apodization, ap, gn);
+    {  // bounding rows and columns of the nonzero gain
+      int rl = NR, rh = -1, cl = NC, ch = -1;
+      for (int q = 0; q < NC; ++q)
+        for (int r = 0; r < NR; ++r)
+          if (gn[r + (size_t)q * NR] != 0.f) {
+            rl = std::min(rl, r);
+            rh = std::max(rh, r);
+            cl = std::min(cl, q);
+            ch = std::max(ch, q);
+          }
+      if (rh >= 0) {
+        nt.rlo = rl;
+        nt.rhi = rh;
+        nt.clo = cl;
+        nt.chi = ch;
+      }
+    }
     if (NR == NC) {
       // bounding box of the nonzero gain (square and centred, by symmetry)
       int lo = NR, hi = -1;
@@ -383,7 +409,8 @@ inline bool gcorr_shape_ok(const hh_pass_desc& p) {
   int8_t rr[24];
   const int NR = fft_rows(p), NC = fft_cols(p);
   return NR >= 2 && NC >= 2 && (int64_t)NR * NC <= GC_MAX_POINTS && hh::gcorr_radix_plan(NR, rr) > 0 &&
-         hh::gcorr_radix_plan(NC, rr) > 0 && 2 * (size_t)(NC + 1) * 2 * sizeof(float2) <= GC_SMEM_LINES;
+         hh::gcorr_radix_plan(NC, rr) > 0 && 2 * (size_t)(NC + 1) * 2 * sizeof(float2) <= GC_SMEM_LINES &&
+         2 * (size_t)(NR + 1) * sizeof(float2) <= GC_SMEM_LINES;
 }
 
 // Fill the general-shape fields of a correlation launch: shapes, radix
@@ -405,13 +432,21 @@ inline hh_status gcorr_setup(hh_ctx* ctx, const hh_pass_desc& p, CorrArgs& ca) {
                     std::to_string(ca.nfc));
   HH_TRY(gc_twiddles(ctx, ca.nfr, &ca.twr));
   HH_TRY(gc_twiddles(ctx, ca.nfc, &ca.twc));
-  ca.gc_chunk_r = std::max(1, std::min(32, (int)(GC_SMEM_LINES / (2 * (size_t)(ca.nfr + 1) * sizeof(float2)))));
+  // columns passes: one warp per line, two line buffers per warp, as many
+  // warps (of 16) as fit; rows pass: chunks of row pairs, two buffers each
+  ca.gc_col_warps = std::max(1, std::min(16, (int)(GC_SMEM_LINES / (2 * (size_t)(ca.nfr + 1) * sizeof(float2)))));
   ca.gc_chunk_c = std::max(2, std::min(32, (int)(GC_SMEM_LINES / (2 * (size_t)(ca.nfc + 1) * sizeof(float2)))) & ~1);
-  const size_t lines = std::max((size_t)ca.gc_chunk_r * (ca.nfr + 1), (size_t)ca.gc_chunk_c * (ca.nfc + 1));
+  const size_t lines = std::max((size_t)ca.gc_col_warps * (ca.nfr + 1), (size_t)ca.gc_chunk_c * (ca.nfc + 1));
   ca.gc_smem_lines = (int64_t)(2 * lines * sizeof(float2));
   const int64_t P = (int64_t)ca.nfr * ca.nfc;
   ca.gscr_stride = (P + (P + 1) / 2 + 31) & ~(int64_t)31;  // complex plane + real plane, 256-byte aligned slices
   ca.gscr_slices = ctx->num_sms;
+  Tables tb;
+  HH_TRY(get_tables(ctx, p, tb));
+  ca.gc_box[0] = tb.rlo;
+  ca.gc_box[1] = tb.rhi;
+  ca.gc_box[2] = tb.clo;
+  ca.gc_box[3] = tb.chi;
   return HH_OK;
 }
 inline hh_status gcorr_prepare(hh_ctx* ctx, const hh_pass_desc& p, CorrArgs& ca) {

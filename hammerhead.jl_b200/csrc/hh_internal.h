@@ -61,7 +61,7 @@ struct CorrArgs {
   // area sr x sc, FFT plane nfr x nfc; gscr holds one scratch slice of
   // gscr_stride float2 per CTA (complex plane + real plane); twr / twc the
   // twiddle tables exp(-2 pi i t / n) of the two lengths and their radix
-  // plans; lines staged per chunk and the shared bytes of the line buffers
+  // plans; the line buffers' layout and shared bytes
   int32_t wr, wc, sr, sc, nfr, nfc;
   float2* gscr;
   int64_t gscr_stride;
@@ -70,8 +70,11 @@ struct CorrArgs {
   const float2* twc;
   int8_t gc_radix_r[24], gc_radix_c[24];
   int32_t gc_nst_r, gc_nst_c;
-  int32_t gc_chunk_r, gc_chunk_c;
+  int32_t gc_col_warps, gc_chunk_c;  // warps of the columns passes (one line each); rows-pass lines per chunk
   int64_t gc_smem_lines;
+  // fftshifted rows [0], [1] and columns [2], [3] outside which the plane is
+  // zero (overlap-gain support or kept search lags; the whole plane otherwise)
+  int32_t gc_box[4];
 };
 
 // Launch the correlation kernel for FFT size N (square) and window W (the

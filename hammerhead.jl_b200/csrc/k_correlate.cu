@@ -1402,7 +1402,8 @@ size_t gcorr_smem_extra() {
 
 cudaError_t launch_correlate_general(const CorrArgs& a, cudaStream_t s) {
   if (a.njobs <= 0) return cudaSuccess;
-  if (!a.gscr || !a.twr || !a.twc || a.gscr_slices < 1 || a.gc_chunk_r < 1 || a.gc_chunk_c < 2)
+  if (!a.gscr || !a.twr || !a.twc || a.gscr_slices < 1 || a.gc_col_warps < 1 || a.gc_col_warps > GC_WARPS ||
+      a.gc_chunk_c < 2)
     return cudaErrorInvalidValue;
   const size_t sm = (size_t)a.gc_smem_lines + gcorr_smem_extra();
   static size_t attr = 0;
