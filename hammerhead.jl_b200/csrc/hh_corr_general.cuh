@@ -112,10 +112,59 @@ __device__ __forceinline__ float2* gc_line(float2* buf0, float2* buf1, int n, co
   return in;
 }
 
+// Lengths n = 16 B (B = 2, 4, 8, 16: n = 32 .. 256) are transformed in
+// registers by half a warp (hl = lane within the half): the four-step split
+// n = 16 B with input index B n1 + n2 and output index k1 + 16 k2 -- a
+// 16-point DFT over n1 per n2 (lanes n2 < B), the twiddle W_n^(n2 k1), a
+// B-point DFT over n2 per k1 (lanes k1 < 16) -- with one exchange through
+// `tmp` (row k1 padded to B + 1, so both access patterns are conflict-free).
+// The result overwrites `line`. Two lines per warp, one per half.
+template <int B, bool INV>
+__device__ __forceinline__ void gc_fft16(float2* line, float2* tmp, const float2* tw, int hl, bool act) {
+  if (act && hl < B) {
+    float2 x[16];
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) x[n1] = line[B * n1 + hl];
+    RDFT<16, INV>::run(x, 16);
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) {
+      float2 v = x[k1];
+      if (k1 && hl) v = cmul(v, gc_tw(tw, hl * k1, INV));
+      tmp[k1 * (B + 1) + hl] = v;
+    }
+  }
+  __syncwarp();
+  if (act) {
+    float2 t[B];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) t[n2] = tmp[hl * (B + 1) + n2];
+    RDFT<B, INV>::run(t, B);
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) line[hl + 16 * k2] = t[k2];
+  }
+  __syncwarp();
+}
+
+// n = 32, 64, 128 or 256: the register form applies
+__host__ __device__ __forceinline__ bool gc_reg_len(int n) { return n == 32 || n == 64 || n == 128 || n == 256; }
+
+template <bool INV>
+__device__ __forceinline__ void gc_fft16_n(float2* line, float2* tmp, int n, const float2* tw, int hl, bool act) {
+  switch (n) {
+    case 32: gc_fft16<2, INV>(line, tmp, tw, hl, act); break;
+    case 64: gc_fft16<4, INV>(line, tmp, tw, hl, act); break;
+    case 128: gc_fft16<8, INV>(line, tmp, tw, hl, act); break;
+    default: gc_fft16<16, INV>(line, tmp, tw, hl, act); break;
+  }
+}
+
 __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const CorrArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int NR = a.nfr, NC = a.nfc, wr = a.wr, wc = a.wc, sr = a.sr, sc = a.sc;
-  const int LDR = NR + 1, LDC = NC + 1;  // staged line strides (float2)
+  // staged line strides (float2): room for the register form's padded exchange
+  const int LDR = NR + 16, LDC = NC + 16;
+  const bool regR = gc_reg_len(NR), regC = gc_reg_len(NC);  // register-form lengths
+  const int hw = (threadIdx.x & 31) >> 4, hl = threadIdx.x & 15;  // half-warp, lane within it
   const int CC = a.gc_chunk_c;  // rows-pass lines per chunk (length NC); the columns passes use a.gc_col_warps warps
   const size_t lines_b = a.gc_smem_lines;
   float2* buf0 = reinterpret_cast<float2*>(smem_raw);
@@ -141,6 +190,16 @@ __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const 
   const int rlo = a.gc_box[0], rhi = a.gc_box[1], clo = a.gc_box[2], chi = a.gc_box[3];
   const ScanPlan sp = scan_plan(tid, GC_THREADS, rlo, rhi, clo, chi);
   PeakOut po{a.du, a.dv, a.ratio, a.moment, a.alt_u, a.alt_v, a.nalt, a.G, a.packed, a.locs};
+
+  // the real plane outside the box's columns is zero for every window of
+  // this launch (the box is the launch's): cleared once here, never rewritten
+  for (int c = warp; c < NC; c += GC_WARPS) {
+    const int js = c;
+    if (js >= clo && js <= chi) continue;
+    float* rc = R + (int64_t)js * NR;
+    for (int i = lane; i < NR; i += 32) rc[i] = 0.f;
+  }
+  __syncthreads();
 
   for (int64_t job = blockIdx.x; job < a.njobs; job += gridDim.x) {
     int rs, cs;
@@ -211,35 +270,47 @@ __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const 
     const bool bad = !(isfinite(ta) && isfinite(tb));  // the window holds NaN or Inf: the reference's plane is NaN
 
     // ---- 1b. data columns j < sc of Z, transformed along the rows axis;
-    //      each warp builds, transforms and stores its own columns
-    //      (consecutive lanes on consecutive rows), so no CTA barrier is needed
+    //      each warp builds, transforms and stores its own columns (two at a
+    //      time, one per half-warp, in the register form), so no CTA barrier
+    //      is needed
     if (warp < a.gc_col_warps) {
-      float2* l0 = buf0 + (size_t)warp * 2 * LDR;
-      float2* l1 = l0 + LDR;
-      for (int j = warp; j < sc; j += a.gc_col_warps) {
+      const int lpw = regR ? 2 : 1;  // lines per warp at a time
+      float2* wbuf = buf0 + (size_t)warp * 2 * lpw * LDR;
+      for (int jb = warp * lpw; jb < sc; jb += a.gc_col_warps * lpw) {
+        const int j = jb + (regR ? hw : 0);
+        const bool act = j < sc;
+        const int i0 = regR ? hl : lane, st = regR ? 16 : 32;
+        float2* l0 = wbuf + (regR ? hw * 2 * LDR : 0);
+        float2* l1 = l0 + LDR;
+        if (act) {
 #pragma unroll 4
-        for (int i = lane; i < NR; i += 32) {
-          float2 z = make_float2(0.f, 0.f);
-          if (i < sr && !bad) {
-            const int64_t off = (r0 + i) + (c0 + j) * ld;
-            if (!(M && __ldg(M + off))) {
-              const int ia = i - oar, ja = j - oac;
-              const bool ina = (unsigned)ia < (unsigned)wr && (unsigned)ja < (unsigned)wc;
-              if (search) {
-                z.y = __ldg(B + off) - mb;
-                if (ina) z.x = __ldg(a.apod + ia + ja * wr) * (__ldg(A + off) - ma);
-              } else {
-                const float ap = __ldg(a.apod + i + j * wr);
-                z = make_float2(ap * (__ldg(A + off) - ma), ap * (__ldg(B + off) - mb));
+          for (int i = i0; i < NR; i += st) {
+            float2 z = make_float2(0.f, 0.f);
+            if (i < sr && !bad) {
+              const int64_t off = (r0 + i) + (c0 + j) * ld;
+              if (!(M && __ldg(M + off))) {
+                const int ia = i - oar, ja = j - oac;
+                const bool ina = (unsigned)ia < (unsigned)wr && (unsigned)ja < (unsigned)wc;
+                if (search) {
+                  z.y = __ldg(B + off) - mb;
+                  if (ina) z.x = __ldg(a.apod + ia + ja * wr) * (__ldg(A + off) - ma);
+                } else {
+                  const float ap = __ldg(a.apod + i + j * wr);
+                  z = make_float2(ap * (__ldg(A + off) - ma), ap * (__ldg(B + off) - mb));
+                }
               }
             }
+            l0[i] = z;
           }
-          l0[i] = z;
         }
         __syncwarp();
-        const float2* res = gc_line(l0, l1, NR, a.gc_radix_r, a.gc_nst_r, a.twr, false, lane);
-        float2* zc = Z + (int64_t)j * NR;
-        for (int i = lane; i < NR; i += 32) zc[i] = res[i];
+        const float2* res = l0;
+        if (regR) gc_fft16_n<false>(l0, l1, NR, a.twr, hl, act);
+        else res = gc_line(l0, l1, NR, a.gc_radix_r, a.gc_nst_r, a.twr, false, lane);
+        if (act) {
+          float2* zc = Z + (int64_t)j * NR;
+          for (int i = i0; i < NR; i += st) zc[i] = res[i];
+        }
         __syncwarp();
       }
     }
@@ -254,15 +325,22 @@ __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const 
       // on the columns: the reads of a column are two contiguous runs
       for (int l0 = lane; l0 < 2 * nh; l0 += 32) {
         const int ra = h0 + (l0 >> 1), row = (l0 & 1) ? (NR - ra) % NR : ra;
+#pragma unroll 8
         for (int j = warp; j < NC; j += GC_WARPS)
           buf0[l0 * LDC + j] = j < sc ? Z[(int64_t)j * NR + row] : make_float2(0.f, 0.f);
       }
       __syncthreads();
-      for (int l = warp; l < 2 * nh; l += GC_WARPS)
-        gc_line(buf0 + l * LDC, buf1 + l * LDC, NC, a.gc_radix_c, a.gc_nst_c, a.twc, false, lane);
+      if (regC) {  // two lines per warp (its row pair), one per half-warp
+        const int l = 2 * warp + hw;
+        gc_fft16_n<false>(buf0 + l * LDC, buf1 + l * LDC, NC, a.twc, hl, l < 2 * nh);
+      } else {
+        for (int l = warp; l < 2 * nh; l += GC_WARPS)
+          gc_line(buf0 + l * LDC, buf1 + l * LDC, NC, a.gc_radix_c, a.gc_nst_c, a.twc, false, lane);
+      }
       __syncthreads();
-      float2* fz = (a.gc_nst_c & 1) ? buf1 : buf0;  // forward rows
-      float2* sz = (a.gc_nst_c & 1) ? buf0 : buf1;  // spectrum rows
+      // the register form leaves its result in place
+      float2* fz = (!regC && (a.gc_nst_c & 1)) ? buf1 : buf0;  // forward rows
+      float2* sz = (!regC && (a.gc_nst_c & 1)) ? buf0 : buf1;  // spectrum rows
       for (int l = warp; l < 2 * nh; l += GC_WARPS) {
         const int ra = h0 + (l >> 1), row = (l & 1) ? (NR - ra) % NR : ra;
         const float2* Za = fz + l * LDC;          // this row
@@ -273,13 +351,19 @@ __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const 
         }
       }
       __syncthreads();
-      for (int l = warp; l < 2 * nh; l += GC_WARPS)
-        gc_line(sz + l * LDC, fz + l * LDC, NC, a.gc_radix_c, a.gc_nst_c, a.twc, true, lane);
+      if (regC) {
+        const int l = 2 * warp + hw;
+        gc_fft16_n<true>(sz + l * LDC, fz + l * LDC, NC, a.twc, hl, l < 2 * nh);
+      } else {
+        for (int l = warp; l < 2 * nh; l += GC_WARPS)
+          gc_line(sz + l * LDC, fz + l * LDC, NC, a.gc_radix_c, a.gc_nst_c, a.twc, true, lane);
+      }
       __syncthreads();
-      float2* iz = (a.gc_nst_c & 1) ? fz : sz;
+      float2* iz = (!regC && (a.gc_nst_c & 1)) ? fz : sz;
       for (int l0 = lane; l0 < 2 * nh; l0 += 32) {
         const int ra = h0 + (l0 >> 1), row = (l0 & 1) ? (NR - ra) % NR : ra;
         if ((l0 & 1) && row == ra) continue;  // a self-paired row (0, NR/2) is written once
+#pragma unroll 4
         for (int j = warp; j < NC; j += GC_WARPS) {
           const int js = j + NC / 2 < NC ? j + NC / 2 : j + NC / 2 - NC;
           if (js < clo || js > chi) continue;  // a column that step 3 writes as zeros
@@ -291,28 +375,32 @@ __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const 
 
     // ---- 3. columns back, then |.| / (nr nc), fftshift, gain, kept lags;
     //      columns whose shifted position lies outside the box are zero
+    //      (those columns were cleared at the start of the launch)
     const int nbox = chi - clo + 1;
-    {
-      const float z0 = bad ? __int_as_float(0x7fc00000) : 0.f;
-      for (int c = warp; c < NC - nbox; c += GC_WARPS) {
-        float* rc = R + (int64_t)((chi + 1 + c) % NC) * NR;  // columns chi+1 .. clo-1 (wrapping)
-        for (int i = lane; i < NR; i += 32) rc[i] = z0;
-      }
-    }
     //      the box's columns, one warp each: unshifted column j = (js - NC/2) mod NC
     if (warp < a.gc_col_warps) {
-      float2* l0 = buf0 + (size_t)warp * 2 * LDR;
-      float2* l1 = l0 + LDR;
-      for (int b = warp; b < nbox; b += a.gc_col_warps) {
-        const int js = clo + b, j = (js + NC - NC / 2) % NC;
-        const float2* zc = Z + (int64_t)j * NR;
+      const int lpw = regR ? 2 : 1;
+      float2* wbuf = buf0 + (size_t)warp * 2 * lpw * LDR;
+      for (int bb = warp * lpw; bb < nbox; bb += a.gc_col_warps * lpw) {
+        const int b = bb + (regR ? hw : 0);
+        const bool act = b < nbox;
+        const int i0 = regR ? hl : lane, st = regR ? 16 : 32;
+        float2* l0 = wbuf + (regR ? hw * 2 * LDR : 0);
+        float2* l1 = l0 + LDR;
+        const int js = clo + (act ? b : 0), j = (js + NC - NC / 2) % NC;
+        if (act) {
+          const float2* zc = Z + (int64_t)j * NR;
 #pragma unroll 8
-        for (int i = lane; i < NR; i += 32) l0[i] = zc[i];
+          for (int i = i0; i < NR; i += st) l0[i] = zc[i];
+        }
         __syncwarp();
-        const float2* res = gc_line(l0, l1, NR, a.gc_radix_r, a.gc_nst_r, a.twr, true, lane);
+        const float2* res = l0;
+        if (regR) gc_fft16_n<true>(l0, l1, NR, a.twr, hl, act);
+        else res = gc_line(l0, l1, NR, a.gc_radix_r, a.gc_nst_r, a.twr, true, lane);
         float* rc = R + (int64_t)js * NR;
         const bool colkept = !search || abs(js - NC / 2) <= oac;
-        for (int i = lane; i < NR; i += 32) {
+        if (act)
+        for (int i = i0; i < NR; i += st) {
           const float2 c = res[i];
           const int is = i + NR / 2 < NR ? i + NR / 2 : i + NR / 2 - NR;  // fftshifted row
           float v = hypotf(c.x * scale, c.y * scale);
@@ -327,9 +415,12 @@ __global__ void __launch_bounds__(GC_THREADS, 1) correlate_general_kernel(const 
     __syncthreads();
 
     // ---- 4. plane out (correlation_planes / ensemble sums) and analysis
-    if (a.planes) {
+    if (a.planes) {  // a window holding NaN or Inf has a NaN plane, as in the reference
       float* dst = a.planes + job * P;
-      for (int64_t e = tid; e < P; e += GC_THREADS) dst[e] = a.accumulate ? dst[e] + R[e] : R[e];
+      for (int64_t e = tid; e < P; e += GC_THREADS) {
+        const float v = bad ? __int_as_float(0x7fc00000) : R[e];
+        dst[e] = a.accumulate ? dst[e] + v : v;
+      }
     }
     if (!a.accumulate) {
       analyze_group(R, NR, NC, NR, K, a.npeaks, a.finder, a.subpixel, tid, GC_THREADS, red, true, s_vals, s_locs,

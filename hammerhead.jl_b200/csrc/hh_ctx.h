@@ -404,13 +404,16 @@ constexpr size_t GC_SMEM_LINES = 192 * 1024;
 // planes the general kernel accepts (complex + real plane per CTA slice)
 constexpr int64_t GC_MAX_POINTS = (int64_t)1 << 22;
 
+// FFT lengths the general kernel transforms in registers (16 x B, two lines per warp)
+inline bool gc_reg_length(int n) { return n == 32 || n == 64 || n == 128 || n == 256; }
+
 // Is the pass's FFT shape one the general kernel can run?
 inline bool gcorr_shape_ok(const hh_pass_desc& p) {
   int8_t rr[24];
   const int NR = fft_rows(p), NC = fft_cols(p);
   return NR >= 2 && NC >= 2 && (int64_t)NR * NC <= GC_MAX_POINTS && hh::gcorr_radix_plan(NR, rr) > 0 &&
-         hh::gcorr_radix_plan(NC, rr) > 0 && 2 * (size_t)(NC + 1) * 2 * sizeof(float2) <= GC_SMEM_LINES &&
-         2 * (size_t)(NR + 1) * sizeof(float2) <= GC_SMEM_LINES;
+         hh::gcorr_radix_plan(NC, rr) > 0 && 2 * (size_t)(NC + 16) * 2 * sizeof(float2) <= GC_SMEM_LINES &&
+         2 * 2 * (size_t)(NR + 16) * sizeof(float2) <= GC_SMEM_LINES;
 }
 
 // Fill the general-shape fields of a correlation launch: shapes, radix
@@ -432,11 +435,15 @@ inline hh_status gcorr_setup(hh_ctx* ctx, const hh_pass_desc& p, CorrArgs& ca) {
                     std::to_string(ca.nfc));
   HH_TRY(gc_twiddles(ctx, ca.nfr, &ca.twr));
   HH_TRY(gc_twiddles(ctx, ca.nfc, &ca.twc));
-  // columns passes: one warp per line, two line buffers per warp, as many
-  // warps (of 16) as fit; rows pass: chunks of row pairs, two buffers each
-  ca.gc_col_warps = std::max(1, std::min(16, (int)(GC_SMEM_LINES / (2 * (size_t)(ca.nfr + 1) * sizeof(float2)))));
-  ca.gc_chunk_c = std::max(2, std::min(32, (int)(GC_SMEM_LINES / (2 * (size_t)(ca.nfc + 1) * sizeof(float2)))) & ~1);
-  const size_t lines = std::max((size_t)ca.gc_col_warps * (ca.nfr + 1), (size_t)ca.gc_chunk_c * (ca.nfc + 1));
+  // columns passes: per warp one line (two, one per half-warp, for the
+  // register-form lengths 32..256), two buffers per line, as many warps (of
+  // 16) as fit; rows pass: chunks of row pairs, two buffers each. Lines are
+  // staged with 16 elements of padding (the register form's exchange).
+  const size_t ldr = (size_t)ca.nfr + 16, ldc = (size_t)ca.nfc + 16;
+  const int lpw = gc_reg_length(ca.nfr) ? 2 : 1;
+  ca.gc_col_warps = std::max(1, std::min(16, (int)(GC_SMEM_LINES / (2 * lpw * ldr * sizeof(float2)))));
+  ca.gc_chunk_c = std::max(2, std::min(32, (int)(GC_SMEM_LINES / (2 * ldc * sizeof(float2)))) & ~1);
+  const size_t lines = std::max((size_t)ca.gc_col_warps * lpw * ldr, (size_t)ca.gc_chunk_c * ldc);
   ca.gc_smem_lines = (int64_t)(2 * lines * sizeof(float2));
   const int64_t P = (int64_t)ca.nfr * ca.nfc;
   ca.gscr_stride = (P + (P + 1) / 2 + 31) & ~(int64_t)31;  // complex plane + real plane, 256-byte aligned slices

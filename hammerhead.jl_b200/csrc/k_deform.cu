@@ -152,58 +152,6 @@ __device__ __forceinline__ float bspline_eval(const float* C, int64_t nr, int64_
   return s;
 }
 
-// The samples of a quad of consecutive rows (pixels j = 0..3 of one column):
-// when all four lie inside the image, share one tap column base and their
-// tap rows follow each other (the usual case: the displacement varies
-// slowly), the 7 x 4 coefficients their 4 x 4 tap blocks cover are loaded
-// once and each sample is summed from registers, in the order and with the
-// arithmetic of bspline_eval, so the results are identical; any other quad
-// takes bspline_eval per sample. nv = samples to evaluate (the quad's end may
-// lie past the image).
-__device__ __forceinline__ void bspline_eval4(const float* C, int64_t nr, int64_t nc, const float* yy, const float* xx,
-                                              int nv, float* out) {
-  int64_t iy[4], ix[4];
-  bool fast = nv == 4;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const bool in = !(yy[j] < 1.f || yy[j] > (float)nr || xx[j] < 1.f || xx[j] > (float)nc);
-    fast = fast && in;
-    iy[j] = (int64_t)floorf(yy[j]);
-    if (iy[j] > nr - 1) iy[j] = nr - 1;
-    ix[j] = (int64_t)floorf(xx[j]);
-    if (ix[j] > nc - 1) ix[j] = nc - 1;
-  }
-#pragma unroll
-  for (int j = 1; j < 4; ++j) fast = fast && ix[j] == ix[0] && iy[j] == iy[0] + j;
-  if (!fast) {
-#pragma unroll
-    for (int j = 0; j < 4; ++j) out[j] = j < nv ? bspline_eval(C, nr, nc, yy[j], xx[j]) : 0.f;
-    return;
-  }
-  const int64_t ld = nr + 2;
-  const float* base = C + (iy[0] - 1) + (ix[0] - 1) * ld;
-  float patch[7][4];
-#pragma unroll
-  for (int r = 0; r < 7; ++r)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) patch[r][b] = __ldg(base + r + b * ld);
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    float wy[4], wx[4];
-    cubw(FS(yy[j], (float)iy[j]), wy);
-    cubw(FS(xx[j], (float)ix[j]), wx);
-    float s = 0.f;
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      float t = 0.f;
-#pragma unroll
-      for (int b = 0; b < 4; ++b) t = FA(t, FM(wx[b], patch[a + j][b]));
-      s = FA(s, FM(wy[a], t));
-    }
-    out[j] = s;
-  }
-}
-
 __global__ void __launch_bounds__(256) deform_kernel(const float* __restrict__ CA, const float* __restrict__ CB,
                                                      int64_t nr, int64_t nc, const float* __restrict__ pu,
                                                      const float* __restrict__ pv, PredGrid g, float* wA, float* wB) {
@@ -758,14 +706,12 @@ __global__ void __launch_bounds__(256) b_deform_kernel(const BPair* __restrict__
       c = l0 / nr;
     }
     float wa[4], wb[4];
-    float ya[4], xa[4], yb[4], xb[4];  // the quad's sample points in frames A and B
     int ix = 0;
     float dx = 0.f;
     int64_t cx = -1;  // column whose x interpolation (ix, dx) is held
-    const int nv = l0 + 4 <= npx ? 4 : (int)(npx - l0);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      ya[j] = xa[j] = yb[j] = xb[j] = 0.f;
+      wa[j] = wb[j] = 0.f;
       if (l0 + j < npx) {
         int64_t rj = r + j, cj = c;
         while (rj >= nr) {  // the quad wraps to the next column
@@ -782,14 +728,10 @@ __global__ void __launch_bounds__(256) b_deform_kernel(const BPair* __restrict__
         lin_axis(R, g.y0, g.ysp, g.gny, iy, dy);
         const float du2 = FM(bilinear_at(fu, g, iy, dy, ix, dx), 0.5f);
         const float dv2 = FM(bilinear_at(fv, g, iy, dy, ix, dx), 0.5f);
-        ya[j] = FS(R, dv2);
-        xa[j] = FS(Cc, du2);
-        yb[j] = FA(R, dv2);
-        xb[j] = FA(Cc, du2);
+        wa[j] = bspline_eval(b.coefA, nr, nc, FS(R, dv2), FS(Cc, du2));
+        wb[j] = bspline_eval(b.coefB, nr, nc, FA(R, dv2), FA(Cc, du2));
       }
     }
-    bspline_eval4(b.coefA, nr, nc, ya, xa, nv, wa);
-    bspline_eval4(b.coefB, nr, nc, yb, xb, nv, wb);
     if (l0 + 3 < npx) {
       *reinterpret_cast<float4*>(b.warpA + l0) = make_float4(wa[0], wa[1], wa[2], wa[3]);
       *reinterpret_cast<float4*>(b.warpB + l0) = make_float4(wb[0], wb[1], wb[2], wb[3]);
