@@ -39,6 +39,7 @@ scaling, no collective on the data path); only the timing max and the
 vector counts are reduced.
 """
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -530,6 +531,10 @@ def main():
         per_window = {ln.split()[0]: float(ln.split()[1]) for ln in open(tpath)
                       if ln.strip() and not ln.startswith("#")}["dram_bytes_per_window"]
         traffic = per_window * c["units"] / max(c["launches"], 1)
+    general = any(not L.hh_corr_fused(ctypes.byref(p.to_desc())) for sc in scheds for p in sc)
+    corr_label = ("correlate_kernel + correlate_general_kernel (window FFT correlation + peak analysis; "
+                  "the general-shape kernel serves the passes without a fused kernel)" if general else
+                  "correlate_kernel (fused window FFT correlation + peak analysis)")
     shares = {k: round(v["ms"] / max(sum(x["ms"] for x in prof.values()), 1e-9), 4) for k, v in prof.items()}
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     d = prof["deform"]
@@ -560,7 +565,7 @@ def main():
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": (achieved / fp32_peak) if achieved else None, "traffic": traffic,
-                         "kernel": "correlate_kernel (fused window FFT correlation + peak analysis)",
+                         "kernel": corr_label,
                          "peak_source": f"148 SMs x 128 FP32 lanes x 2 FLOP x {sm_max:.0f} MHz (no FP32 entry in "
                                         "MEASURED_PEAKS.json)",
                          "launches": c["launches"], "ms_per_launch": c["ms"] / max(c["launches"], 1)},
