@@ -139,4 +139,16 @@ template <> struct AxisSplit<64> { static constexpr int N1 = 16, N2 = 4; };
 template <> struct AxisSplit<96> { static constexpr int N1 = 12, N2 = 8; };
 template <> struct AxisSplit<128> { static constexpr int N1 = 16, N2 = 8; };
 
+// The alternative split the autotuner times against AxisSplit: a shorter
+// in-register radix and a longer second pass (one more exchange through
+// shared memory for N <= 32, fewer live registers per item).
+template <int N> struct AxisSplitAlt;
+template <> struct AxisSplitAlt<16> { static constexpr int N1 = 4, N2 = 4; };
+template <> struct AxisSplitAlt<24> { static constexpr int N1 = 6, N2 = 4; };
+template <> struct AxisSplitAlt<32> { static constexpr int N1 = 8, N2 = 4; };
+template <> struct AxisSplitAlt<48> { static constexpr int N1 = 12, N2 = 4; };
+template <> struct AxisSplitAlt<64> { static constexpr int N1 = 8, N2 = 8; };
+template <> struct AxisSplitAlt<96> { static constexpr int N1 = 8, N2 = 12; };
+template <> struct AxisSplitAlt<128> { static constexpr int N1 = 8, N2 = 16; };
+
 }  // namespace hh

@@ -649,15 +649,20 @@ __device__ __forceinline__ float2 cross_spectrum(float2 X, float2 Zm, int method
 // W is the extent of the data: the window, or with SRCH the frame-B search
 // area that holds the (runtime) frame-A window at its centre. VAR selects the
 // CTA shape (windows per CTA, threads per window) and register budget (CTAs
-// per SM the registers are sized for) among the four the autotuner times:
-// 0 the default shape and budget, 1 the alternative shape, 2 the default
-// shape with one CTA per SM more in the budget (fewer registers, more warps),
-// 3 the default shape with one CTA less (more registers, no spills) -- or,
-// where the default budget is one CTA, the alternative shape with one CTA
-// more. All compute the same arithmetic on another thread mapping or
-// register allocation, so the results are identical.
+// per SM the registers are sized for) and FFT split among the five the
+// autotuner times: 0 the default shape and budget, 1 the alternative shape,
+// 2 the default shape with one CTA per SM more in the budget (fewer
+// registers, more warps), 3 the default shape with one CTA less (more
+// registers, no spills) -- or, where the default budget is one CTA, the
+// alternative shape with one CTA more. Variants 0-3 compute the same
+// arithmetic on another thread mapping or register allocation, so their
+// results are identical. Variant 4 splits each axis's DFT differently
+// (AxisSplitAlt), so its planes differ from variant 0's by rounding.
 template <int N, int W, bool SRCH = false, int VAR = 0> struct CorrCfg {
-  static constexpr int N1 = AxisSplit<N>::N1, N2 = AxisSplit<N>::N2;
+  // variant 4: the alternative FFT split (AxisSplitAlt) in the default shape and budget
+  static constexpr bool ALT = VAR == 4;
+  static constexpr int N1 = ALT ? AxisSplitAlt<N>::N1 : AxisSplit<N>::N1;
+  static constexpr int N2 = ALT ? AxisSplitAlt<N>::N2 : AxisSplit<N>::N2;
   // budget of the default shape; shape of this variant (0 default, 1 alternative)
   static constexpr int MINB0 = (N == 32 && W == 16) ? 3 : (N <= 48 ? 4 : (N <= 64 ? 3 : (N <= 96 ? 2 : 1)));
   static constexpr int SH = (VAR == 1 || (VAR == 3 && MINB0 == 1)) ? 1 : 0;
@@ -1363,6 +1368,7 @@ cudaError_t launch_correlate(const CorrArgs& a, int N, int W, cudaStream_t s, in
       case 1: return launch_nw<n, w, false, 1>(a, s, num_sms);                         \
       case 2: return launch_nw<n, w, false, 2>(a, s, num_sms);                         \
       case 3: return launch_nw<n, w, false, 3>(a, s, num_sms);                         \
+      case 4: return launch_nw<n, w, false, 4>(a, s, num_sms);                         \
       default: return launch_nw<n, w, false, 0>(a, s, num_sms);                        \
     }                                                                                  \
   }

@@ -1,8 +1,9 @@
-"""Autotuning of the correlation kernel's CTA shape.
+"""Autotuning of the correlation kernel's CTA shape and FFT split.
 
 Every (FFT size, window) of the correlation kernel is built in
-HH_CORR_VARIANTS CTA shapes (windows per CTA, threads per window, register
-budget) that compute the same results. `autotune` times them on the
+HH_CORR_VARIANTS variants: CTA shapes (windows per CTA, threads per window,
+register budget) that compute the same results, and an alternative split
+of each axis's DFT whose results differ by rounding. `autotune` times them on the
 workspace's device (hh_autotune_correlation) for every pass class of a
 schedule and makes the fastest the workspace's choice; the choices are kept
 in a JSON cache keyed by device and (FFT size, window, peaks), so later runs
@@ -19,7 +20,7 @@ from . import _lib
 from ._lib import ArgumentError
 from .params import PIVParameters
 
-VARIANTS = 4  # HH_CORR_VARIANTS
+VARIANTS = 5  # HH_CORR_VARIANTS
 
 
 def _flatten(passes):

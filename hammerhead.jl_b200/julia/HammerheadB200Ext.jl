@@ -526,7 +526,7 @@ function autotune_b200!(ctx::Context, imgA::AbstractMatrix{<:Real}, imgB::Abstra
         w = p.window_size[1]
         n = p.padding ? 2w : w
         any(o -> o[1] == n && o[2] == w, out) && continue
-        ms = zeros(Float32, 4)  # HH_CORR_VARIANTS
+        ms = zeros(Float32, 5)  # HH_CORR_VARIANTS
         best = Ref{Int32}(0)
         check(ccall((:hh_autotune_correlation, LIB), Int32,
                     (Ptr{Cvoid}, Ref{PassDesc}, Int32, Ptr{Float32}, Ref{Int32}),

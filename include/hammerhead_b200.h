@@ -217,7 +217,9 @@ hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npair
  * The correlation kernel of each (FFT size, window) comes in
  * HH_CORR_VARIANTS variants: two CTA shapes (windows per CTA, threads per
  * window) and, for the default shape, register budgets of one CTA per SM
- * more and one less; all compute the same results. hh_autotune_correlation
+ * more and one less (variants 0-3, identical results), and the default
+ * shape with another split of each axis's DFT into an in-register radix and
+ * a second pass (variant 4, results differ by rounding). hh_autotune_correlation
  * times every shape on the windows of `pass` over the staged pair
  * (hh_stage_pair first), `reps` launches each, interleaved, writes the mean
  * ms per launch of each shape into variant_ms (HH_CORR_VARIANTS entries)
@@ -226,7 +228,7 @@ hh_status hh_run_ensemble(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npair
  * example from a cache of earlier tuning). Both drop the context's batched
  * plans, whose graphs hold the old choice. Enlarged search areas have one
  * shape. No counterpart in the reference. */
-#define HH_CORR_VARIANTS 4
+#define HH_CORR_VARIANTS 5
 hh_status hh_autotune_correlation(hh_ctx* ctx, const hh_pass_desc* pass, int32_t reps, float* variant_ms,
                                   int32_t* best);
 hh_status hh_set_corr_variant(hh_ctx* ctx, int32_t fft_size, int32_t window, int32_t variant);

@@ -87,3 +87,26 @@ def plane_decision_margin(R, locs_a, locs_b, k, finder="regionalmax", excl=2):
         if np.isfinite(nb):
             gaps.append(abs(R64[r - 1, c - 1] - nb))
     return min(gaps) if gaps else np.inf
+
+
+def compare_runs(r, o, tol=1e-3, all_sweeps=True):
+    """A device run against the oracle's Float32 run of the same schedule:
+    grid masks, validation flags and sweep counts identical, every unmasked
+    vector within `tol` px (the maximum, no quantile), and the uncertainty
+    finite on the same cells with 99 % of it within 1e-3 px (a ring of the
+    covariance sums that sits at finalize_uncertainty's 0.05 S00 threshold,
+    src/uncertainty.jl:162-179, is decided by round-off). all_sweeps=False
+    compares the final pass's sweep count only."""
+    assert np.array_equal(r.mask, o["mask"])
+    flips = np.argwhere(r.outliers != o["outliers"])
+    assert len(flips) == 0, f"outlier flags differ at {flips[:10].tolist()}"
+    # the batched form reports the final pass's sweep count only
+    assert list(r.sweeps) == list(o["sweeps"]) if all_sweeps else r.sweeps[-1] == o["sweeps"][-1]
+    ok = ~o["mask"]
+    du, dv = np.abs(r.u - o["u"])[ok], np.abs(r.v - o["v"])[ok]
+    assert du.max() <= tol and dv.max() <= tol, (du.max(), dv.max())
+    fin = np.isfinite(r.uncertainty_u)
+    assert np.array_equal(fin, np.isfinite(o["uncertainty_u"]))
+    if fin.any():
+        assert np.quantile(np.abs(r.uncertainty_u - o["uncertainty_u"])[fin], 0.99) < 1e-3
+    return du.max(), dv.max()
