@@ -41,61 +41,61 @@ __device__ __forceinline__ uint32_t fkey(float v) {
   return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
 
-struct TopK {
-  uint32_t hi[KMAX];
-  uint32_t lo[KMAX];
+// Per-thread list of the best keys seen, descending, in KC register slots
+// (KC >= K: 4 when the pass keeps at most 4 peaks, else KMAX).
+template <int KC> struct TopK {
+  uint32_t hi[KC];
+  uint32_t lo[KC];
   int cnt;
   uint32_t thr;  // key of the K-th entry once the list is full, else 0
   __device__ __forceinline__ void init() {
     cnt = 0;
     thr = 0u;
 #pragma unroll
-    for (int m = 0; m < KMAX; ++m) hi[m] = lo[m] = 0u;
+    for (int m = 0; m < KC; ++m) hi[m] = lo[m] = 0u;
   }
   // the K-th (last retained) key, read with unrolled selects so the arrays
   // stay in registers for a run-time K
   __device__ __forceinline__ uint32_t last_hi(int K) const {
     uint32_t v = 0u;
 #pragma unroll
-    for (int m = 0; m < KMAX; ++m) v = (m == K - 1) ? hi[m] : v;
+    for (int m = 0; m < KC; ++m) v = (m == K - 1) ? hi[m] : v;
     return v;
   }
   __device__ __forceinline__ uint32_t last_lo(int K) const {
     uint32_t v = 0u;
 #pragma unroll
-    for (int m = 0; m < KMAX; ++m) v = (m == K - 1) ? lo[m] : v;
+    for (int m = 0; m < KC; ++m) v = (m == K - 1) ? lo[m] : v;
     return v;
   }
-  // insert keeping (hi, lo) descending; K <= KMAX entries retained. Valid
-  // keys are nonzero and empty slots hold 0, so the new key bubbles down
-  // through compare-and-select steps (no data-dependent indexing: the list
-  // stays in registers).
+  // insert keeping (hi, lo) descending; K <= KC entries retained. Valid keys
+  // are nonzero and empty slots hold 0, so the slots the new key beats are a
+  // suffix of the first K: the first of them takes the new key, the others
+  // their predecessor, and a key that beats none changes nothing. The
+  // comparisons are independent of one another (no data-dependent indexing:
+  // the list stays in registers).
   __device__ __forceinline__ void insert(uint32_t h, uint32_t l, int K) {
-    if (cnt == K) {
-      const uint32_t lh = last_hi(K), ll = last_lo(K);
-      if (!(h > lh || (h == lh && l > ll))) return;
-    }
-    uint32_t ch = h, cl = l;
+    bool b[KC];
 #pragma unroll
-    for (int m = 0; m < KMAX; ++m) {
-      const bool in = m < K;
-      const bool better = in && (ch > hi[m] || (ch == hi[m] && cl > lo[m]));
-      const uint32_t th = hi[m], tl = lo[m];
-      hi[m] = better ? ch : th;
-      lo[m] = better ? cl : tl;
-      ch = better ? th : ch;
-      cl = better ? tl : cl;
+    for (int m = 0; m < KC; ++m) b[m] = m < K && (h > hi[m] || (h == hi[m] && l > lo[m]));
+#pragma unroll
+    for (int m = KC - 1; m >= 0; --m) {
+      const int q = m > 0 ? m - 1 : 0;
+      const bool prev = m > 0 && b[q];
+      const uint32_t ph = prev ? hi[q] : h, pl = prev ? lo[q] : l;
+      hi[m] = b[m] ? ph : hi[m];
+      lo[m] = b[m] ? pl : lo[m];
     }
     if (cnt < K) ++cnt;
     if (cnt == K) thr = last_hi(K);
   }
   __device__ __forceinline__ void pop() {
 #pragma unroll
-    for (int m = 0; m + 1 < KMAX; ++m) {
+    for (int m = 0; m + 1 < KC; ++m) {
       hi[m] = hi[m + 1];
       lo[m] = lo[m + 1];
     }
-    hi[KMAX - 1] = lo[KMAX - 1] = 0u;
+    hi[KC - 1] = lo[KC - 1] = 0u;
     if (cnt > 0) --cnt;
     thr = 0u;
   }
@@ -167,7 +167,8 @@ __device__ __forceinline__ void group_argmax(uint32_t hi, uint32_t lo, uint32_t*
 // group's part of one), by K shuffle rounds (keys are unique, so exactly one
 // lane pops each winner): lane m receives the m-th best in (mh, ml);
 // returns how many exist (the same in every lane).
-__device__ __forceinline__ int warp_topk(TopK& tk, int K, int lane, uint32_t& mh, uint32_t& ml, unsigned mask) {
+template <class TK>
+__device__ __forceinline__ int warp_topk(TK& tk, int K, int lane, uint32_t& mh, uint32_t& ml, unsigned mask) {
   int n = 0;
   mh = ml = 0u;
   for (int round = 0; round < K; ++round) {
@@ -401,6 +402,9 @@ __device__ void peak_outputs(const Src& src, int nr, int nc, int K, int npeaks, 
 // group size do not change), so the integer divisions are done once:
 // column strips of rps rows, S strips per column; this thread's first
 // strip is column c, rows [r0, r1).
+#ifndef HH_SPEC_BATCH
+#define HH_SPEC_BATCH 4  // spectrum items per thread whose loads are issued together (N <= 32)
+#endif
 struct ScanPlan {
   int rlo, rhi, clo, chi;
   int bw, S, rps;
@@ -421,6 +425,7 @@ __device__ __forceinline__ ScanPlan scan_plan(int gtid, int gsize, int rlo, int 
   return sp;
 }
 
+template <int KC>
 __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
                                              int subpixel, int gtid, int gsize, uint32_t* red, bool active,
                                              float* s_vals, int* s_locs, int64_t grid_id, int64_t job,
@@ -440,7 +445,7 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
     // the pixel above) must not exceed the value, later ones (the right
     // column and the pixel below) must stay below it; fmaxf drops NaN
     // neighbours, which never block in the reference either.
-    TopK tk;
+    TopK<KC> tk;
     tk.init();
     if (scan) {
       const int bw = sp.bw, S = sp.S, rps = sp.rps;
@@ -515,7 +520,7 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
       }
       grp_sync(bar, gsize);
       if (gwarp == 0) {
-        TopK tg;
+        TopK<KC> tg;
         tg.init();
         for (int e = lane; e < nwarps * K; e += 32) {
           const uint32_t h = red[2 * e], l = red[2 * e + 1];
@@ -621,8 +626,12 @@ __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int l
                                            float* s_vals, int* s_locs, int64_t grid_id, int64_t job,
                                            const PeakOut* o, bool poison, int bar, const ScanPlan sp,
                                            float* rec, int64_t rec_stride) {
-  analyze_body(R, nr, nc, ldr, K, npeaks, finder, subpixel, gtid, gsize, red, active, s_vals, s_locs, grid_id, job, o,
-               poison, bar, sp, rec, rec_stride);
+  if (K <= 4)
+    analyze_body<4>(R, nr, nc, ldr, K, npeaks, finder, subpixel, gtid, gsize, red, active, s_vals, s_locs, grid_id, job,
+                    o, poison, bar, sp, rec, rec_stride);
+  else
+    analyze_body<KMAX>(R, nr, nc, ldr, K, npeaks, finder, subpixel, gtid, gsize, red, active, s_vals, s_locs, grid_id,
+                       job, o, poison, bar, sp, rec, rec_stride);
 }
 
 // S(k) = conj(FA(k)) FB(k) of the packed transform Z = F(a + i b), from
@@ -1013,26 +1022,52 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
     //      place (for N <= 32 every canonical column is done here: folding
     //      the spectrum into the single-pass inverse costs more registers
     //      than the separate pass costs time).
+    if (N2 == 1) {
+      // items (row ap, canonical column c) in batches of SB per thread: the
+      // batch's operands are loaded before any of its results is stored (no
+      // item reads a cell another item writes: column -c is read only, and a
+      // self-paired column's rows ap and -ap belong to one item)
+      constexpr int SB = HH_SPEC_BATCH, NIT = NC * N;
 #pragma unroll 1
-    for (int it = gt; it < (N2 == 1 ? NC : 2) * N; it += G) {
-      const int ap = it % N, c = N2 == 1 ? it / N : (it / N) * H;
-      int aq, bq, bp, kp;
-      if (N2 == 1) {
-        aq = c;
-        bq = (N - c) % N;
-        bp = (N - ap) % N;
-        kp = ap;
-      } else {
-        aq = bq = s_canon[c];
-        bp = s_neg[ap];
-        kp = s_freq[ap];
+      for (int it0 = gt; it0 < NIT; it0 += SB * G) {
+        float2 xa[SB], xb[SB];
+        int ia[SB], ib[SB];
+        bool on[SB], self[SB];
+        float wk[SB];
+#pragma unroll
+        for (int u = 0; u < SB; ++u) {
+          const int it = it0 + u * G;
+          const int ap = it % N, c = it / N, bq = (N - c) % N, bp = (N - ap) % N;
+          self[u] = c == bq;
+          on[u] = it < NIT && !(self[u] && ap > bp);  // a self pair is done by its upper row
+          ia[u] = c * LD + ap;
+          ib[u] = bq * LD + bp;
+          wk[u] = on[u] && a.method == 1 ? __ldg(a.phasew + c * N + ap) : 1.f;
+          if (on[u]) {
+            xa[u] = P[ia[u]];
+            xb[u] = P[ib[u]];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < SB; ++u)
+          if (on[u]) {
+            const float2 S = cross_spectrum(xa[u], xb[u], a.method, wk[u]);
+            P[ia[u]] = S;
+            if (self[u]) P[ib[u]] = make_float2(S.x, -S.y);
+          }
       }
-      const bool self = aq == bq;
-      if (self && ap > bp) continue;  // its partner row does this pair
-      const float wk = a.method == 1 ? __ldg(a.phasew + c * N + kp) : 1.f;
-      const float2 S = cross_spectrum(P[aq * LD + ap], P[bq * LD + bp], a.method, wk);
-      P[aq * LD + ap] = S;
-      if (self) P[aq * LD + bp] = make_float2(S.x, -S.y);
+    } else {
+      // the two self-paired columns kq = 0 and N/2 (storage order)
+#pragma unroll 1
+      for (int it = gt; it < 2 * N; it += G) {
+        const int ap = it % N, c = (it / N) * H;
+        const int aq = s_canon[c], bp = s_neg[ap], kp = s_freq[ap];
+        if (ap > bp) continue;  // its partner row does this pair
+        const float wk = a.method == 1 ? __ldg(a.phasew + c * N + kp) : 1.f;
+        const float2 S = cross_spectrum(P[aq * LD + ap], P[aq * LD + bp], a.method, wk);
+        P[aq * LD + ap] = S;
+        P[aq * LD + bp] = make_float2(S.x, -S.y);
+      }
     }
     grp_sync(bar, G);
     //      (ii) for N > 32 every other canonical column forms its spectrum
@@ -1233,9 +1268,12 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
     //      needed only when the outputs are formed here, not from a record)
     const bool defer = a.rec && a.finder == 0;
     uint32_t* gred = red + w * (G / 32) * 2 * KMAX;
-    if (C::INLINE_ANALYSIS)
-      analyze_body(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
-                   s_locs + w * 2 * KMAX, gid, job, defer ? nullptr : &pw, bad, bar, sp, a.rec, a.njobs);
+    if (C::INLINE_ANALYSIS && K <= 4)
+      analyze_body<4>(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
+                      s_locs + w * 2 * KMAX, gid, job, defer ? nullptr : &pw, bad, bar, sp, a.rec, a.njobs);
+    else if (C::INLINE_ANALYSIS)
+      analyze_body<KMAX>(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
+                         s_locs + w * 2 * KMAX, gid, job, defer ? nullptr : &pw, bad, bar, sp, a.rec, a.njobs);
     else
       analyze_group(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
                     s_locs + w * 2 * KMAX, gid, job, defer ? nullptr : &pw, bad, bar, sp, a.rec, a.njobs);
