@@ -33,6 +33,27 @@
 namespace hh {
 
 // ---------------------------------------------------------------------------
+// Global loads with L1 eviction hints. The shared-memory carveout leaves a
+// small L1, and the window pixels, read once per window, would otherwise
+// push out the small per-class tables (apodization, overlap gain, phase
+// filter) that every window reads: the pixels stream past L1, the tables
+// are kept. Inputs are read-only for the kernel's lifetime (.nc).
+__device__ __forceinline__ float ld_stream(const float* p) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ uint8_t ld_stream(const uint8_t* p) {
+  unsigned short v;
+  asm("ld.global.nc.L1::no_allocate.u8 %0, [%1];" : "=h"(v) : "l"(p));
+  return (uint8_t)v;
+}
+__device__ __forceinline__ float ld_keep(const float* p) {
+  float v;
+  asm("ld.global.nc.L1::evict_last.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+
 // Peak keys: larger key = larger value, ties broken by smaller column-major
 // index (the reference's first-in-scan-order rule).
 __device__ __forceinline__ uint32_t fkey(float v) {
@@ -402,9 +423,6 @@ __device__ void peak_outputs(const Src& src, int nr, int nc, int K, int npeaks, 
 // group size do not change), so the integer divisions are done once:
 // column strips of rps rows, S strips per column; this thread's first
 // strip is column c, rows [r0, r1).
-#ifndef HH_SPEC_BATCH
-#define HH_SPEC_BATCH 4  // spectrum items per thread whose loads are issued together (N <= 32)
-#endif
 struct ScanPlan {
   int rlo, rhi, clo, chi;
   int bw, S, rps;
@@ -720,10 +738,16 @@ template <int N, int W, bool SRCH = false, int VAR = 0> struct CorrCfg {
   // writes) do not meet in one bank
   static constexpr int PS = N * LD + (HALF ? 8 : 0);
   static constexpr size_t PLANE_B = (size_t)PS * sizeof(float2);
+  // the overlap gain table in shared memory for FFT sizes up to 48, where
+  // it fits beside the CTAs' planes without costing a CTA per SM (read from
+  // L1 instead, it was a third of the last inverse pass at 32 points);
+  // larger sizes read it from global memory with an L1 keep hint
+  static constexpr bool GSM = N <= 48;
   static constexpr size_t smem() {
     return WPC * PLANE_B + WPC * (G / 32) * NPART * sizeof(double) + N * sizeof(float2) +
            WPC * (G / 32) * 2 * KMAX * sizeof(uint32_t) +
-           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int)) + 3 * N * sizeof(int) + 64;
+           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int)) + 3 * N * sizeof(int) + 64 +
+           (GSM ? (size_t)N * N * sizeof(float) : 0);
   }
   static_assert(W == N || 2 * W == N, "window must equal the FFT size or half of it");
   static_assert((G >= 32 && G % 32 == 0) || G == 16, "a window group is whole warps or half a warp");
@@ -749,9 +773,12 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
   int* s_freq = reinterpret_cast<int*>(s_locs + WPC * 2 * KMAX);
   int* s_neg = s_freq + N;
   int* s_canon = s_neg + N;
+  float* s_gain = reinterpret_cast<float*>(s_canon + N);  // N x N when C::GSM
 
   const int tid = threadIdx.x;
   const int K = a.npeaks > 2 ? a.npeaks : 2;
+  if (C::GSM && a.gain)
+    for (int m = tid; m < N * N; m += NT) s_gain[m] = a.gain[m];
   if (N2 > 1) {
     for (int m = tid; m < N; m += NT) {
       double sn, cs;
@@ -845,8 +872,8 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
           const int p = e % W, q = e / W;
           const bool ina = (unsigned)(p - oa) < (unsigned)wa && (unsigned)(q - oa) < (unsigned)wa;
           const int64_t off = (r0 + p) + (c0 + q) * ld;
-          z[i] = make_float2(ina ? __ldg(A + off) : 0.f, __ldg(B + off));
-          mk[i] = M ? __ldg(M + off) != 0 : false;
+          z[i] = make_float2(ina ? ld_stream(A + off) : 0.f, ld_stream(B + off));
+          mk[i] = M ? ld_stream(M + off) != 0 : false;
           if (!mk[i]) {
             sb += (double)z[i].y;
             nb += 1.0;
@@ -893,7 +920,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
           float2 v = make_float2(0.f, 0.f);
           if (!(mk[i] || bad)) {
             v.y = z[i].y - mb;
-            if (ina) v.x = __ldg(a.apod + (p - oa) + (q - oa) * wa) * (z[i].x - ma);
+            if (ina) v.x = ld_keep(a.apod + (p - oa) + (q - oa) * wa) * (z[i].x - ma);
           }
           P[q * LD + p] = v;
         }
@@ -910,8 +937,8 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
         if (e < W * W) {
           const int p = e % W, q = e / W;
           const int64_t off = (int64_t)(rs + p) + (int64_t)(cs + q) * ld;
-          z[i] = make_float2(__ldg(A + off), __ldg(B + off));
-          mk[i] = M ? __ldg(M + off) != 0 : false;
+          z[i] = make_float2(ld_stream(A + off), ld_stream(B + off));
+          mk[i] = M ? ld_stream(M + off) != 0 : false;
           if (!mk[i]) {
             sa += (double)z[i].x;
             sb += (double)z[i].y;
@@ -948,7 +975,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
         const int e = gt + i * G;
         if (e < W * W) {
           const int p = e % W, q = e / W;
-          const float ap = __ldg(a.apod + e);
+          const float ap = ld_keep(a.apod + e);
           P[q * LD + p] = (mk[i] || bad) ? make_float2(0.f, 0.f) : make_float2(ap * (z[i].x - ma), ap * (z[i].y - mb));
         }
       }
@@ -1027,7 +1054,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
       // batch's operands are loaded before any of its results is stored (no
       // item reads a cell another item writes: column -c is read only, and a
       // self-paired column's rows ap and -ap belong to one item)
-      constexpr int SB = HH_SPEC_BATCH, NIT = NC * N;
+      constexpr int SB = 4, NIT = NC * N;  // (batches of 8 were slower: registers)
 #pragma unroll 1
       for (int it0 = gt; it0 < NIT; it0 += SB * G) {
         float2 xa[SB], xb[SB];
@@ -1042,7 +1069,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
           on[u] = it < NIT && !(self[u] && ap > bp);  // a self pair is done by its upper row
           ia[u] = c * LD + ap;
           ib[u] = bq * LD + bp;
-          wk[u] = on[u] && a.method == 1 ? __ldg(a.phasew + c * N + ap) : 1.f;
+          wk[u] = on[u] && a.method == 1 ? ld_keep(a.phasew + c * N + ap) : 1.f;
           if (on[u]) {
             xa[u] = P[ia[u]];
             xb[u] = P[ib[u]];
@@ -1063,7 +1090,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
         const int ap = it % N, c = (it / N) * H;
         const int aq = s_canon[c], bp = s_neg[ap], kp = s_freq[ap];
         if (ap > bp) continue;  // its partner row does this pair
-        const float wk = a.method == 1 ? __ldg(a.phasew + c * N + kp) : 1.f;
+        const float wk = a.method == 1 ? ld_keep(a.phasew + c * N + kp) : 1.f;
         const float2 S = cross_spectrum(P[aq * LD + ap], P[aq * LD + bp], a.method, wk);
         P[aq * LD + ap] = S;
         P[aq * LD + bp] = make_float2(S.x, -S.y);
@@ -1100,7 +1127,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
           x[k2] = L[k2];
           if (aq != bq) {
             const int pos = N2 * k1 + k2;
-            const float wk = a.method == 1 ? __ldg(a.phasew + c * N + s_freq[pos]) : 1.f;
+            const float wk = a.method == 1 ? ld_keep(a.phasew + c * N + s_freq[pos]) : 1.f;
             x[k2] = cross_spectrum(x[k2], Lb[s_neg[pos]], a.method, wk);
           }
         }
@@ -1216,8 +1243,8 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
             const int qs = (N2 * n1 + n2 + H) % N;
             float r0 = fabsf(x[n1].x) * scale, r1 = fabsf(x[n1].y) * scale;
             if (a.gain) {
-              r0 *= __ldg(a.gain + qs * N + ps0);
-              r1 *= hasb ? __ldg(a.gain + qs * N + ps1) : 0.f;
+              r0 *= C::GSM ? s_gain[qs * N + ps0] : ld_keep(a.gain + qs * N + ps0);
+              r1 *= hasb ? (C::GSM ? s_gain[qs * N + ps1] : ld_keep(a.gain + qs * N + ps1)) : 0.f;
             }
             if (SRCH && (qs < blo || qs > bhi)) r0 = r1 = 0.f;  // lags outside the search range
             rv[i][0][n1] = r0;
