@@ -738,17 +738,22 @@ template <int N, int W, bool SRCH = false, int VAR = 0> struct CorrCfg {
   // writes) do not meet in one bank
   static constexpr int PS = N * LD + (HALF ? 8 : 0);
   static constexpr size_t PLANE_B = (size_t)PS * sizeof(float2);
-  // the overlap gain table in shared memory for FFT sizes up to 48, where
-  // it fits beside the CTAs' planes without costing a CTA per SM (read from
-  // L1 instead, it was a third of the last inverse pass at 32 points);
-  // larger sizes read it from global memory with an L1 keep hint
-  static constexpr bool GSM = N <= 48;
-  static constexpr size_t smem() {
-    return WPC * PLANE_B + WPC * (G / 32) * NPART * sizeof(double) + N * sizeof(float2) +
-           WPC * (G / 32) * 2 * KMAX * sizeof(uint32_t) +
-           WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int)) + 3 * N * sizeof(int) + 64 +
-           (GSM ? (size_t)N * N * sizeof(float) : 0);
+  static constexpr size_t BASE_B = WPC * PLANE_B + WPC * (G / 32) * NPART * sizeof(double) + N * sizeof(float2) +
+                                   WPC * (G / 32) * 2 * KMAX * sizeof(uint32_t) +
+                                   WPC * (KMAX * sizeof(float) + 2 * KMAX * sizeof(int)) + 3 * N * sizeof(int) + 64;
+  // CTAs per SM that shared memory allows (228 KB per SM, 1 KB of it
+  // reserved per CTA), capped by the register budget
+  static constexpr int occ(size_t b) {
+    return (int)((228 * 1024) / (b + 1024)) < MINB ? (int)((228 * 1024) / (b + 1024)) : MINB;
   }
+  // The overlap gain table (N x N) is read by every window; from global
+  // memory its L1 lines are flushed by the window pixels (it took a third of
+  // the last inverse pass at 32 points, half of it at 128). It goes to shared
+  // memory where that costs no CTA per SM: every size but 64 points. (The
+  // apodization window in shared memory as well was no faster.)
+  static constexpr size_t GAIN_B = (size_t)N * N * sizeof(float);
+  static constexpr bool GSM = occ(BASE_B + GAIN_B) >= occ(BASE_B);
+  static constexpr size_t smem() { return BASE_B + (GSM ? GAIN_B : 0); }
   static_assert(W == N || 2 * W == N, "window must equal the FFT size or half of it");
   static_assert((G >= 32 && G % 32 == 0) || G == 16, "a window group is whole warps or half a warp");
   static_assert(N * LDR <= 2 * N * LD, "real plane must fit in the complex plane");
@@ -779,6 +784,7 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
   const int K = a.npeaks > 2 ? a.npeaks : 2;
   if (C::GSM && a.gain)
     for (int m = tid; m < N * N; m += NT) s_gain[m] = a.gain[m];
+
   if (N2 > 1) {
     for (int m = tid; m < N; m += NT) {
       double sn, cs;
@@ -1049,7 +1055,52 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
     //      place (for N <= 32 every canonical column is done here: folding
     //      the spectrum into the single-pass inverse costs more registers
     //      than the separate pass costs time).
-    if (N2 == 1) {
+    if constexpr (N2 == 1 && G <= N && N % G == 0) {
+      // each thread owns rows ap = gt + j G (j < N / G) of every canonical
+      // column; the columns are unrolled, so every address is the row's base
+      // plus a constant, and CB columns' operands are loaded before any of
+      // their results is stored (no item reads a cell another item writes:
+      // column -c is read only, and a self-paired column's rows ap and -ap
+      // belong to one item)
+      constexpr int RPT = G <= N ? N / G : 1, CB = RPT >= 2 ? 2 : 4;
+      int ra[RPT], rb[RPT];
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) {
+        ra[j] = gt + j * G;
+        rb[j] = (N - ra[j]) % N;
+      }
+#pragma unroll
+      for (int c0 = 0; c0 < NC; c0 += CB) {
+        float2 xa[CB][RPT], xb[CB][RPT];
+        float wk[CB][RPT];
+#pragma unroll
+        for (int u = 0; u < CB; ++u) {
+          const int c = c0 + u, cb = (N - c) % N;
+          if (c < NC) {
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) {
+              if (c == cb && ra[j] > rb[j]) continue;  // a self pair is done by its upper row
+              xa[u][j] = P[c * LD + ra[j]];
+              xb[u][j] = P[cb * LD + rb[j]];
+              wk[u][j] = a.method == 1 ? ld_keep(a.phasew + c * N + ra[j]) : 1.f;
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < CB; ++u) {
+          const int c = c0 + u, cb = (N - c) % N;
+          if (c < NC) {
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) {
+              if (c == cb && ra[j] > rb[j]) continue;
+              const float2 S = cross_spectrum(xa[u][j], xb[u][j], a.method, wk[u][j]);
+              P[c * LD + ra[j]] = S;
+              if (c == cb) P[c * LD + rb[j]] = make_float2(S.x, -S.y);
+            }
+          }
+        }
+      }
+    } else if constexpr (N2 == 1) {
       // items (row ap, canonical column c) in batches of SB per thread: the
       // batch's operands are loaded before any of its results is stored (no
       // item reads a cell another item writes: column -c is read only, and a
