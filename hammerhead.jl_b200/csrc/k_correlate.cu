@@ -1172,14 +1172,18 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
         const int aq = s_canon[c], bq = s_neg[aq];
         float2* L = P + aq * LD + N2 * k1;
         const float2* Lb = P + bq * LD;
+        // slot N2 k1 + k2 holds frequency k1 + N1 k2; its negation sits at
+        // slot N2 (N1 - k1) + N2 - 1 - k2 (k1 > 0), or N2 - k2 (k1 = 0, k2 > 0),
+        // or 0: the row base is per item, the offsets constants
+        const int nb0 = k1 == 0 ? N2 : N2 * (N1 - k1) + N2 - 1;
         float2 x[N2];
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) {
           x[k2] = L[k2];
           if (aq != bq) {
-            const int pos = N2 * k1 + k2;
-            const float wk = a.method == 1 ? ld_keep(a.phasew + c * N + s_freq[pos]) : 1.f;
-            x[k2] = cross_spectrum(x[k2], Lb[s_neg[pos]], a.method, wk);
+            const int neg = (k1 == 0 && k2 == 0) ? 0 : nb0 - k2;
+            const float wk = a.method == 1 ? ld_keep(a.phasew + c * N + k1 + N1 * k2) : 1.f;
+            x[k2] = cross_spectrum(x[k2], Lb[neg], a.method, wk);
           }
         }
         RDFT<N2, true>::run(x, N2);
