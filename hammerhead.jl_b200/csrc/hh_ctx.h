@@ -366,6 +366,24 @@ inline hh_status get_tables(hh_ctx* ctx, const hh_pass_desc& p, Tables& t) {
         nt.box_hi = hi;
       }
     }
+    // after the table: a flag word and, for a square table whose values
+    // depend only on |lag| along each axis (a symmetric apodization window),
+    // its quarter q[a + b (N/2 + 1)] = gain at lags (-a, -b) for kernels that
+    // keep the quarter in shared memory; the flag is 1 when the quarter is exact
+    std::vector<float> gq;
+    if (NR == NC) {
+      const int H = NR / 2, HQ = H + 1;
+      gq.assign((size_t)HQ * HQ, 0.f);
+      for (int b = 0; b <= H; ++b)
+        for (int a = 0; a <= H; ++a) gq[a + (size_t)b * HQ] = gn[(H - a) + (size_t)(H - b) * NR];
+      bool sym = true;
+      for (int c = 0; c < NC && sym; ++c)
+        for (int r = 0; r < NR && sym; ++r)
+          sym = gn[r + (size_t)c * NR] == gq[std::abs(r - H) + (size_t)std::abs(c - H) * HQ];
+      if (!sym) gq.clear();
+    }
+    gn.push_back(gq.empty() ? 0.f : 1.f);
+    gn.insert(gn.end(), gq.begin(), gq.end());
     HH_CK(cudaMalloc(&nt.gain, gn.size() * sizeof(float)));
     HH_CK(cudaMemcpy(nt.gain, gn.data(), gn.size() * sizeof(float), cudaMemcpyHostToDevice));
   }

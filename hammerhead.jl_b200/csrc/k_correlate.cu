@@ -751,9 +751,14 @@ template <int N, int W, bool SRCH = false, int VAR = 0> struct CorrCfg {
   // the last inverse pass at 32 points, half of it at 128). It goes to shared
   // memory where that costs no CTA per SM: every size but 64 points. (The
   // apodization window in shared memory as well was no faster.)
+  // Where the full table would cost a CTA (64 points), its quarter does not:
+  // the gain of a symmetric apodization depends only on |lag| along each
+  // axis, and the table builder appends the quarter when that holds exactly.
   static constexpr size_t GAIN_B = (size_t)N * N * sizeof(float);
+  static constexpr size_t GQ_B = (size_t)(N / 2 + 1) * (N / 2 + 1) * sizeof(float);
   static constexpr bool GSM = occ(BASE_B + GAIN_B) >= occ(BASE_B);
-  static constexpr size_t smem() { return BASE_B + (GSM ? GAIN_B : 0); }
+  static constexpr bool QSM = !GSM && occ(BASE_B + GQ_B) >= occ(BASE_B);
+  static constexpr size_t smem() { return BASE_B + (GSM ? GAIN_B : (QSM ? GQ_B : 0)); }
   static_assert(W == N || 2 * W == N, "window must equal the FFT size or half of it");
   static_assert((G >= 32 && G % 32 == 0) || G == 16, "a window group is whole warps or half a warp");
   static_assert(N * LDR <= 2 * N * LD, "real plane must fit in the complex plane");
@@ -784,6 +789,10 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
   const int K = a.npeaks > 2 ? a.npeaks : 2;
   if (C::GSM && a.gain)
     for (int m = tid; m < N * N; m += NT) s_gain[m] = a.gain[m];
+  // the quarter table (word N^2 of the gain buffer says whether it follows)
+  const bool gq = C::QSM && a.gain && a.gain[N * N] != 0.f;
+  if (gq)
+    for (int m = tid; m < (N / 2 + 1) * (N / 2 + 1); m += NT) s_gain[m] = a.gain[N * N + 1 + m];
 
   if (N2 > 1) {
     for (int m = tid; m < N; m += NT) {
@@ -1298,8 +1307,17 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
             const int qs = (N2 * n1 + n2 + H) % N;
             float r0 = fabsf(x[n1].x) * scale, r1 = fabsf(x[n1].y) * scale;
             if (a.gain) {
-              r0 *= C::GSM ? s_gain[qs * N + ps0] : ld_keep(a.gain + qs * N + ps0);
-              r1 *= hasb ? (C::GSM ? s_gain[qs * N + ps1] : ld_keep(a.gain + qs * N + ps1)) : 0.f;
+              if (C::GSM) {
+                r0 *= s_gain[qs * N + ps0];
+                r1 *= hasb ? s_gain[qs * N + ps1] : 0.f;
+              } else if (gq) {
+                const int bq = abs(qs - H) * (H + 1);
+                r0 *= s_gain[abs(ps0 - H) + bq];
+                r1 *= hasb ? s_gain[abs(ps1 - H) + bq] : 0.f;
+              } else {
+                r0 *= ld_keep(a.gain + qs * N + ps0);
+                r1 *= hasb ? ld_keep(a.gain + qs * N + ps1) : 0.f;
+              }
             }
             if (SRCH && (qs < blo || qs > bhi)) r0 = r1 = 0.f;  // lags outside the search range
             rv[i][0][n1] = r0;
