@@ -10,6 +10,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "hh_batch.h"
 #include "hh_internal.h"
 
@@ -56,14 +58,21 @@ static UQOffsets make_offsets() {
   return o;
 }
 
+// finalize_uncertainty (src/uncertainty.jl:162-179). The doubled covariance
+// sums enter S00 one ring at a time (each ring summed in its own order, then
+// added), the arithmetic of the lane-parallel form uq_finalize_seg, so every
+// kernel gives a window the same sigma from the same statistics.
 __device__ __forceinline__ float uq_finalize(const double* s, const UQOffsets& o) {
   const double C0 = s[0], Cp = s[1], Cm = s[2], S00 = s[3];
   double s2 = S00;
   for (int ring = 0; ring < 4; ++ring) {
-    double mx = -INFINITY;
-    for (int k = o.ring_start[ring]; k < o.ring_start[ring + 1]; ++k) mx = fmax(mx, s[4 + k]);
+    double mx = -INFINITY, rsum = 0.0;
+    for (int k = o.ring_start[ring]; k < o.ring_start[ring + 1]; ++k) {
+      mx = fmax(mx, s[4 + k]);
+      rsum = fma(2.0, s[4 + k], rsum);
+    }
     if (mx < __dmul_rn(0.05, S00)) break;
-    for (int k = o.ring_start[ring]; k < o.ring_start[ring + 1]; ++k) s2 = __dadd_rn(s2, __dmul_rn(2.0, s[4 + k]));
+    s2 = __dadd_rn(s2, rsum);
   }
   const double sdc = sqrt(fmax(s2, 0.0));
   const double Cpm = __dadd_rn(Cp, Cm) / 2.0;
@@ -244,13 +253,19 @@ __global__ void __launch_bounds__(UQ_THREADS) uq_kernel(const UQArgs a, const UQ
 // Register form for windows up to 32 px: two warps per window, one per
 // component (u: the window as stored, v: its transpose). Lane c owns column c
 // of the component's W x (W-1) difference field dC for every row in
-// registers, so the smoothing along the columns and the 40 half-plane
-// covariance sums are register FMAs plus one shuffle per neighbour column
-// and row; the per-lane partial sums are combined through shared memory in
-// a fixed order. Same FP32 operations as uq_kernel, FP64 sums.
+// registers, so the smoothing along the columns is register arithmetic plus
+// one shuffle per row. The mean-free smoothed field then goes to shared
+// memory (one column per lane, zero columns past the last), and each lane
+// reads its neighbour columns there in 16-byte row pairs for the 40
+// half-plane covariance sums, which are register FMAs. The per-lane partial
+// sums are combined across the window's lanes by transposed shuffle sums
+// (each exchange halves the values a lane holds), so no shared memory holds
+// per-lane partials. Same FP32 operations as uq_kernel, FP64 sums.
 // When dC has at most 16 columns (W <= 17) a warp serves two windows, one
 // per 16-lane segment (shuffles of width 16), so no lane idles for want of
-// a column.
+// a column. Window means are one warp's job per window (all 32 lanes), and
+// finalize_uncertainty is spread over the first lanes of each window (ring
+// maxima and sums on lanes 0-3, one logarithm each on lanes 0-2).
 constexpr int UQW_THREADS = 128;  // two warp pairs (u, v)
 
 template <int W> struct UQWCfg {
@@ -259,18 +274,33 @@ template <int W> struct UQWCfg {
   static constexpr int WPW = M <= 16 ? 2 : 1;  // windows per warp
   static constexpr int SEG = 32 / WPW;         // lanes per window
   static constexpr int NWIN = 2 * WPW;         // windows per CTA
+  // the smoothed field of one window component: column c at c * DLD doubles.
+  // DLD = W + 2 is 2 mod 4 (W is a multiple of 4), so the 16-byte row pairs
+  // that 8 consecutive lanes read from 8 consecutive columns fall in distinct
+  // bank groups. Columns SEG .. SEG+3 stay zero: the lag partners of the last
+  // lanes.
+  static constexpr int DLD = W + 2;
+  static constexpr int DCOLS = SEG + 4;
+  static constexpr size_t dd_bytes = (size_t)DCOLS * DLD * sizeof(double);
   // window buffers of consecutive slots start 16 banks apart (64 bytes mod
   // 128), so the two windows of a warp do not meet in one bank
   static constexpr size_t win_raw = 2 * (size_t)LD * W * sizeof(float) + (size_t)W * W;
   static constexpr size_t win_bytes = (win_raw + 127) / 128 * 128 + 64;
-  static constexpr size_t part_bytes = (44 * 33 + 44 * WPW) * sizeof(double);  // per warp: partials + totals
   // the next windows are copied in (cp.async) while the current ones are
   // reduced, into a second set of buffers (timed: faster up to 16 px, no
-  // gain at 24 px, and at 32 px the buffers would cost a CTA per SM)
+  // gain at 24 px)
   static constexpr bool PREFETCH = W <= 16;
   static constexpr int NBUF = PREFETCH ? 2 : 1;
-  static constexpr size_t smem() { return NBUF * NWIN * win_bytes + 4 * part_bytes + sizeof(UQOffsets) + 16; }
-  static constexpr int MINB = 3;  // CTAs per SM the register budget is sized for
+  static constexpr size_t up128(size_t x) { return (x + 127) / 128 * 128; }
+  // shared memory: smoothed fields (4 warps x WPW), totals (4 x WPW x 44),
+  // window buffers, window means, apodization, offset tables
+  static constexpr size_t off_tot = up128(4 * WPW * dd_bytes);
+  static constexpr size_t off_win = up128(off_tot + 4 * WPW * 44 * sizeof(double));
+  static constexpr size_t off_mean = up128(off_win + NBUF * NWIN * win_bytes);
+  static constexpr size_t off_apod = up128(off_mean + NWIN * 2 * sizeof(float));
+  static constexpr size_t off_offs = up128(off_apod + (size_t)W * W * sizeof(float));
+  static constexpr size_t smem() { return off_offs + sizeof(UQOffsets) + 16; }
+  static constexpr int MINB = W <= 24 ? 4 : 3;  // CTAs per SM the register budget is sized for
 };
 
 // sum over the lanes of one SEG-lane segment
@@ -278,6 +308,72 @@ template <int SEG> __device__ __forceinline__ double seg_sum(double v) {
 #pragma unroll
   for (int o = SEG / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+
+// Transposed segment sum: N values per lane, summed over the lanes of a
+// segment in log2(SEG) exchanges. At the exchange with the lane at xor O,
+// the lower lane keeps the first half of its values and sends the second,
+// the upper lane the reverse, and each adds what it receives; so the values
+// a lane holds halve at every step. On return the lane holds the totals of
+// values base + i in v[i] for i < n (n <= tsum_slots(N, SEG)).
+constexpr int tsum_slots(int n, int seg) { return seg <= 1 ? n : tsum_slots((n + 1) / 2, seg / 2); }
+template <int N, int O> __device__ __forceinline__ void seg_tsum(double* v, int c, int& base, int& n) {
+  if constexpr (O > 0) {
+    constexpr int H = (N + 1) / 2;
+    const bool up = (c & O) != 0;
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+      const double lo = v[i];
+      const double hi = i + H < N ? v[i + H] : 0.0;
+      const double send = up ? lo : hi;
+      const double keep = up ? hi : lo;
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+    }
+    if (up) {
+      base += H;
+      n = n > H ? n - H : 0;
+    } else {
+      n = n < H ? n : H;
+    }
+    seg_tsum<H, O / 2>(v, c, base, n);
+  }
+}
+
+// finalize_uncertainty (src/uncertainty.jl:162-179) of one window component
+// from its 44 statistics in ring order (shared memory, visible to the
+// segment), spread over the segment's first lanes: lane j < 4 forms ring
+// j+1's maximum and doubled sum, lanes 0, 1, 2 one logarithm each. The
+// result is valid on every lane of the segment.
+template <int SEG> __device__ __forceinline__ float uq_finalize_seg(const double* s, const UQOffsets& o, int c) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lb = (int)(threadIdx.x & 31) & ~(SEG - 1);  // the segment's first lane
+  double mx = -INFINITY, rsum = 0.0;
+  if (c < 4)
+    for (int k = o.ring_start[c]; k < o.ring_start[c + 1]; ++k) {
+      const double x = s[4 + k];
+      mx = fmax(mx, x);
+      rsum = fma(2.0, x, rsum);
+    }
+  const double C0 = s[0], Cp = s[1], Cm = s[2], S00 = s[3];
+  const double thr = __dmul_rn(0.05, S00);
+  double s2 = S00;
+  bool go = true;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const double m = __shfl_sync(FULL, mx, lb + j);
+    const double t = __shfl_sync(FULL, rsum, lb + j);
+    go = go && !(m < thr);  // a ring below 5 % of S00 ends the sum (NaN does not)
+    if (go) s2 = __dadd_rn(s2, t);
+  }
+  const double sdc = sqrt(fmax(s2, 0.0));
+  const double Cpm = __dmul_rn(__dadd_rn(Cp, Cm), 0.5);
+  const double lo = __dsub_rn(Cpm, __dmul_rn(sdc, 0.5)), hi = __dadd_rn(Cpm, __dmul_rn(sdc, 0.5));
+  const double lg = log(c == 0 ? C0 : (c == 1 ? hi : lo));
+  const double lC0 = __shfl_sync(FULL, lg, lb), lhi = __shfl_sync(FULL, lg, lb + 1), llo = __shfl_sync(FULL, lg, lb + 2);
+  if (!(C0 > 0 && lo > 0)) return __int_as_float(0x7fc00000);
+  const double denom = __dsub_rn(__dsub_rn(__dmul_rn(2.0, lC0), lhi), llo);
+  if (!(denom > 0)) return __int_as_float(0x7fc00000);
+  return (float)(__dsub_rn(lhi, llo) / __dmul_rn(2.0, denom));
 }
 
 // Where window `job` comes from: on = the window is estimated in this launch.
@@ -325,21 +421,31 @@ __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wa
 template <int W>
 __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(const UQArgs a, const UQOffsets o) {
   using C = UQWCfg<W>;
-  constexpr int LD = C::LD, M = C::M, WPW = C::WPW, SEG = C::SEG, NWIN = C::NWIN;
+  constexpr int LD = C::LD, M = C::M, WPW = C::WPW, SEG = C::SEG, NWIN = C::NWIN, DLD = C::DLD;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* part_all = reinterpret_cast<double*>(smem_raw);  // [warp][44][33] + totals
-  unsigned char* wbase = smem_raw + 4 * C::part_bytes;
+  unsigned char* wbase = smem_raw + C::off_win;
+  float* means = reinterpret_cast<float*>(smem_raw + C::off_mean);  // per window slot: (mean A, mean B)
+  float* sap = reinterpret_cast<float*>(smem_raw + C::off_apod);    // the apodization window
   // the offset tables in shared memory (indexed at run time; a parameter
   // struct indexed that way would be copied to local memory)
-  UQOffsets& so = *reinterpret_cast<UQOffsets*>(wbase + C::NBUF * NWIN * C::win_bytes);
+  UQOffsets& so = *reinterpret_cast<UQOffsets*>(smem_raw + C::off_offs);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) so = o;
-  __syncthreads();
   const int comp = warp & 1, seg = lane / SEG, c = lane % SEG;
   const int slot = (warp >> 1) * WPW + seg;  // window of this lane
   const int ts = comp * SEG + c;             // this lane among the 2*SEG threads of its window
-  double* part = part_all + warp * (C::part_bytes / sizeof(double));
+  double* dsm = reinterpret_cast<double*>(smem_raw + (size_t)(warp * WPW + seg) * C::dd_bytes);  // this segment's field
+  double* tot = reinterpret_cast<double*>(smem_raw + C::off_tot) + (warp * WPW + seg) * 44;      // its 44 totals
+  if (tid == 0) so = o;
+  for (int k = tid; k < W * W; k += UQW_THREADS) sap[k] = __ldg(a.apod + k);
+  {  // the zero columns past each segment's lanes (never written again)
+    double* d0 = reinterpret_cast<double*>(smem_raw + (size_t)(warp * WPW) * C::dd_bytes);
+    for (int k = lane; k < WPW * 4 * DLD; k += 32) {
+      const int g = k / (4 * DLD), e = k % (4 * DLD);
+      d0[(size_t)g * (C::dd_bytes / sizeof(double)) + SEG * DLD + e] = 0.0;
+    }
+  }
+  __syncthreads();
   const int64_t stride = (int64_t)gridDim.x * NWIN;
   // copies the window's pixels into buffer set `ph` asynchronously
   auto prefetch = [&](const UQSrc& q0, int ph) {
@@ -354,19 +460,22 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
       }
   };
   int iter = 0;
+  int64_t base = (int64_t)blockIdx.x * NWIN;
+  // the source of this lane's window in the current iteration; the next
+  // iteration's is looked up once, for its prefetch, and carried over
+  UQSrc src = uq_src(a, base + slot);
   if (C::PREFETCH) {
-    const int64_t base0 = (int64_t)blockIdx.x * NWIN;
-    if (base0 < a.njobs) prefetch(uq_src(a, base0 + slot), 0);
+    prefetch(src, 0);
     cp_async_commit();
   }
-  for (int64_t base = (int64_t)blockIdx.x * NWIN; base < a.njobs; base += stride, ++iter) {
+  for (; base < a.njobs; base += stride, ++iter) {
     const int64_t job = base + slot;
     const int ph = C::PREFETCH ? (iter & 1) : 0;
     float* wa = reinterpret_cast<float*>(wbase + (ph * NWIN + slot) * C::win_bytes);  // W x W, column stride LD
     float* wb = wa + LD * W;
     uint8_t* mf = reinterpret_cast<uint8_t*>(wb + LD * W);
     // ---- the window's source (uniform within the window's lanes)
-    const UQSrc src = uq_src(a, job);
+    const UQSrc nxt = uq_src(a, base + stride + slot);
     const bool on = src.on;
     const float* A = src.A;
     const float* B = src.B;
@@ -382,7 +491,7 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
       // the next windows go to the other buffer set while these are reduced
       // (that set was last read in the previous iteration, before its final
       // barrier); then wait for this set's copies, issued one group earlier
-      if (base + stride < a.njobs) prefetch(uq_src(a, base + stride + slot), ph ^ 1);
+      prefetch(nxt, ph ^ 1);  // nothing for a window past the last job (nxt.on is false)
       cp_async_commit();
       cp_async_wait_prev();
       if (run)
@@ -414,32 +523,41 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
       }
     }
     __syncthreads();
-    // ---- window means (load_uncertainty_windows!), FP64, computed by each warp
-    float ma = 0.f, mb = 0.f;
-    if (run) {
+    // ---- window means (load_uncertainty_windows!), FP64: warp s sums window
+    //      slot s over all its lanes (a slot whose window is off and was not
+    //      loaded yields a value nobody reads)
+    if (warp < NWIN) {
+      const float* pa = reinterpret_cast<const float*>(wbase + (ph * NWIN + warp) * C::win_bytes);
+      const float* pb = pa + LD * W;
+      const uint8_t* pm = reinterpret_cast<const uint8_t*>(pb + LD * W);
       double sa = 0.0, sb = 0.0, cnt = 0.0;
-      for (int k = c; k < W * W; k += SEG)
-        if (!mf[k]) {
+#pragma unroll 4
+      for (int k = lane; k < W * W; k += 32)
+        if (!pm[k]) {
           const int p = k % W, q = k / W;
-          sa += (double)wa[p + q * LD];
-          sb += (double)wb[p + q * LD];
+          sa += (double)pa[p + q * LD];
+          sb += (double)pb[p + q * LD];
           cnt += 1.0;
         }
-      sa = seg_sum<SEG>(sa);
-      sb = seg_sum<SEG>(sb);
-      cnt = seg_sum<SEG>(cnt);
-      ma = cnt > 0 ? (float)(sa / cnt) : 0.f;
-      mb = cnt > 0 ? (float)(sb / cnt) : 0.f;
+      sa = seg_sum<32>(sa);
+      sb = seg_sum<32>(sb);
+      cnt = seg_sum<32>(cnt);
+      if (lane == 0) {
+        means[2 * warp] = cnt > 0 ? (float)(sa / cnt) : 0.f;
+        means[2 * warp + 1] = cnt > 0 ? (float)(sb / cnt) : 0.f;
+      }
     }
-    __syncthreads();  // every read of the raw values precedes the apodized writes
-    if (run)
+    __syncthreads();  // the means are visible, and every read of the raw values precedes the apodized writes
+    if (run) {
+      const float ma = means[2 * slot], mb = means[2 * slot + 1];
       for (int k = ts; k < W * W; k += 2 * SEG) {
         const int p = k % W, q = k / W;
-        const float ap = __ldg(a.apod + k);
+        const float ap = sap[k];
         const float va = wa[p + q * LD], vb = wb[p + q * LD];
         wa[p + q * LD] = mf[k] ? 0.f : __fmul_rn(ap, __fsub_rn(va, ma));
         wb[p + q * LD] = mf[k] ? 0.f : __fmul_rn(ap, __fsub_rn(vb, mb));
       }
+    }
     __syncthreads();
     if (run) {
       // ---- this component's dC column (lane c < M), and the C0 / C+ / C- sums
@@ -476,87 +594,76 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
       const double mu = seg_sum<SEG>(msum) / (double)(W * M);
 #pragma unroll
       for (int r = 0; r < W; ++r) dd[r] = col ? dd[r] - mu : 0.0;
-      // ---- S00 and the covariance sums: acc[dc][dr + 4] pairs (r, c) with
-      //      (r + dr, c + dc). Two neighbour columns at a time, so only 18
-      //      accumulators are live; each group's per-lane partials go to
-      //      shared [stat][lane] in natural order.
-      part[0 * 33 + lane] = s0;
-      part[1 * 33 + lane] = s1;
-      part[2 * 33 + lane] = s2;
+      // this lane's column of the field into shared memory (lanes past M
+      // store zeros), for the neighbour-column reads of the covariance sums
+#pragma unroll
+      for (int r = 0; r < W; r += 2) *reinterpret_cast<double2*>(dsm + c * DLD + r) = make_double2(dd[r], dd[r + 1]);
+      // sums the per-lane partials v[0..N) of statistics first .. first+N-1
+      // (natural order) over the window's lanes; the lanes holding totals
+      // store them in ring order
+      auto reduce_store = [&](double* v, auto n_tag, int first) {
+        constexpr int N = decltype(n_tag)::value;
+        int b = 0, n = N;
+        seg_tsum<N, SEG / 2>(v, c, b, n);
+#pragma unroll
+        for (int i = 0; i < tsum_slots(N, SEG); ++i)
+          if (i < n) {
+            const int st = first + b + i;
+            const int ri = st < 4 ? st : 4 + so.nat2ring[st - 4];
+            tot[ri] = v[i];
+            if (on && a.stats) {
+              if (a.accumulate) a.stats[job * 88 + comp * 44 + ri] += v[i];
+              else a.stats[job * 88 + comp * 44 + ri] = v[i];
+            }
+          }
+      };
+      // ---- C0, C+, C-, S00 and the lag-(dr, 0) sums (registers only)
       {
-        double sq = 0.0, acc0[4] = {0.0, 0.0, 0.0, 0.0};
+        double g1[8] = {s0, s1, s2, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int r = 0; r < W; ++r) {
-          sq = fma(dd[r], dd[r], sq);
+          g1[3] = fma(dd[r], dd[r], g1[3]);
 #pragma unroll
           for (int dr = 1; dr <= 4; ++dr)
-            if (r + dr < W) acc0[dr - 1] = fma(dd[r], dd[r + dr], acc0[dr - 1]);
+            if (r + dr < W) g1[3 + dr] = fma(dd[r], dd[r + dr], g1[3 + dr]);
         }
-        part[3 * 33 + lane] = sq;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) part[(4 + i) * 33 + lane] = acc0[i];
+        reduce_store(g1, std::integral_constant<int, 8>{}, 0);
       }
+      __syncwarp();  // the segment's columns are in shared memory
+      // ---- the covariance sums of columns dc = 1..4: acc[9 i + dr + 4]
+      //      pairs (r, c) with (r + dr, c + dc), dc = dg + i. Two neighbour
+      //      columns at a time, so only 18 accumulators are live; a neighbour
+      //      column past the window is one of the zero columns.
 #pragma unroll
       for (int dg = 1; dg <= 3; dg += 2) {
-        double acc[2][9];
+        double acc[18];
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-          for (int jj = 0; jj < 9; ++jj) acc[i][jj] = 0.0;
+        for (int jj = 0; jj < 18; ++jj) acc[jj] = 0.0;
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
-          const int dc = dg + i;
-          const bool ok = c + dc < M;
+          const double* xc = dsm + (c + dg + i) * DLD;
 #pragma unroll
-          for (int r2 = 0; r2 < W; ++r2) {
-            double x = __shfl_down_sync(FULL, dd[r2], dc, SEG);
-            x = ok ? x : 0.0;
+          for (int r2 = 0; r2 < W; r2 += 2) {
+            const double2 x2 = *reinterpret_cast<const double2*>(xc + r2);
 #pragma unroll
-            for (int dr = -4; dr <= 4; ++dr) {
-              const int r0 = r2 - dr;
-              if (r0 >= 0 && r0 < W) acc[i][dr + 4] = fma(dd[r0], x, acc[i][dr + 4]);
+            for (int h = 0; h < 2; ++h) {
+              const double x = h ? x2.y : x2.x;
+#pragma unroll
+              for (int dr = -4; dr <= 4; ++dr) {
+                const int r0 = r2 + h - dr;
+                if (r0 >= 0 && r0 < W) acc[9 * i + dr + 4] = fma(dd[r0], x, acc[9 * i + dr + 4]);
+              }
             }
           }
         }
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-          for (int jj = 0; jj < 9; ++jj) part[(8 + 9 * (dg - 1 + i) + jj) * 33 + lane] = acc[i][jj];
+        reduce_store(acc, std::integral_constant<int, 18>{}, 8 + 9 * (dg - 1));
       }
-      __syncwarp();
-      // ---- per window and statistic, the sum of the M column lanes' partials
-      //      in lane order (the other lanes hold zeros)
-      double* tot = part + 44 * 33;
-      bool on_s[WPW];
-      int64_t job_s[WPW];
-#pragma unroll
-      for (int g = 0; g < WPW; ++g) {
-        on_s[g] = __shfl_sync(FULL, on, g * SEG);
-        job_s[g] = base + (warp >> 1) * WPW + g;
-      }
-      for (int j = lane; j < 44 * WPW; j += 32) {
-        const int g = j / 44, st = j % 44;
-        double t = 0.0;
-        for (int l = 0; l < (WPW == 1 ? 32 : M); ++l) t += part[st * 33 + g * SEG + l];
-        const int ri = st < 4 ? st : 4 + so.nat2ring[st - 4];
-        tot[g * 44 + ri] = t;
-        bool og = on_s[0];
-        int64_t jg = job_s[0];
-#pragma unroll
-        for (int h = 1; h < WPW; ++h)
-          if (g == h) {
-            og = on_s[h];
-            jg = job_s[h];
-          }
-        if (og && a.stats) {
-          if (a.accumulate) a.stats[jg * 88 + comp * 44 + ri] += t;
-          else a.stats[jg * 88 + comp * 44 + ri] = t;
-        }
-      }
-      __syncwarp();
-      if (c == 0 && on && a.unc_u) (comp == 0 ? a.unc_u : a.unc_v)[gid] = uq_finalize(tot + seg * 44, so);
+      __syncwarp();  // the totals are visible to the segment
+      const float sg = uq_finalize_seg<SEG>(tot, so, c);
+      if (c == 0 && on && a.unc_u) (comp == 0 ? a.unc_u : a.unc_v)[gid] = sg;
     }
-    __syncthreads();  // the window buffers are reused by the next iteration
+    src = nxt;
+    __syncthreads();  // the window buffers and fields are reused by the next iteration
   }
 }
 
