@@ -287,17 +287,18 @@ template <int W> struct UQWCfg {
   static constexpr size_t win_raw = 2 * (size_t)LD * W * sizeof(float) + (size_t)W * W;
   static constexpr size_t win_bytes = (win_raw + 127) / 128 * 128 + 64;
   // the next windows are copied in (cp.async) while the current ones are
-  // reduced, into a second set of buffers (timed: faster up to 16 px, no
-  // gain at 24 px)
-  static constexpr bool PREFETCH = W <= 16;
+  // reduced, into a second set of buffers (at 32 px the second set would
+  // cost a CTA per SM)
+  static constexpr bool PREFETCH = W <= 24;
   static constexpr int NBUF = PREFETCH ? 2 : 1;
   static constexpr size_t up128(size_t x) { return (x + 127) / 128 * 128; }
   // shared memory: smoothed fields (4 warps x WPW), totals (4 x WPW x 44),
-  // window buffers, window means, apodization, offset tables
+  // window buffers, per-warp sums for the window means, apodization, offset
+  // tables
   static constexpr size_t off_tot = up128(4 * WPW * dd_bytes);
   static constexpr size_t off_win = up128(off_tot + 4 * WPW * 44 * sizeof(double));
   static constexpr size_t off_mean = up128(off_win + NBUF * NWIN * win_bytes);
-  static constexpr size_t off_apod = up128(off_mean + NWIN * 2 * sizeof(float));
+  static constexpr size_t off_apod = up128(off_mean + 4 * 3 * sizeof(double));
   static constexpr size_t off_offs = up128(off_apod + (size_t)W * W * sizeof(float));
   static constexpr size_t smem() { return off_offs + sizeof(UQOffsets) + 16; }
   static constexpr int MINB = W <= 24 ? 4 : 3;  // CTAs per SM the register budget is sized for
@@ -425,7 +426,7 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* wbase = smem_raw + C::off_win;
-  float* means = reinterpret_cast<float*>(smem_raw + C::off_mean);  // per window slot: (mean A, mean B)
+  double* msum = reinterpret_cast<double*>(smem_raw + C::off_mean);  // per warp: its share of (sum A, sum B, count)
   float* sap = reinterpret_cast<float*>(smem_raw + C::off_apod);    // the apodization window
   // the offset tables in shared memory (indexed at run time; a parameter
   // struct indexed that way would be copied to local memory)
@@ -523,16 +524,19 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
       }
     }
     __syncthreads();
-    // ---- window means (load_uncertainty_windows!), FP64: warp s sums window
-    //      slot s over all its lanes (a slot whose window is off and was not
-    //      loaded yields a value nobody reads)
-    if (warp < NWIN) {
-      const float* pa = reinterpret_cast<const float*>(wbase + (ph * NWIN + warp) * C::win_bytes);
+    // ---- window means (load_uncertainty_windows!), FP64: MW = 4 / NWIN warps
+    //      per window slot, each summing its share of the pixels over all its
+    //      lanes (a slot whose window is off and was not loaded yields values
+    //      nobody reads)
+    {
+      constexpr int MW = 4 / NWIN;
+      const int s = warp / MW, h = warp % MW;
+      const float* pa = reinterpret_cast<const float*>(wbase + (ph * NWIN + s) * C::win_bytes);
       const float* pb = pa + LD * W;
       const uint8_t* pm = reinterpret_cast<const uint8_t*>(pb + LD * W);
       double sa = 0.0, sb = 0.0, cnt = 0.0;
 #pragma unroll 4
-      for (int k = lane; k < W * W; k += 32)
+      for (int k = h * 32 + lane; k < W * W; k += 32 * MW)
         if (!pm[k]) {
           const int p = k % W, q = k / W;
           sa += (double)pa[p + q * LD];
@@ -543,13 +547,22 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
       sb = seg_sum<32>(sb);
       cnt = seg_sum<32>(cnt);
       if (lane == 0) {
-        means[2 * warp] = cnt > 0 ? (float)(sa / cnt) : 0.f;
-        means[2 * warp + 1] = cnt > 0 ? (float)(sb / cnt) : 0.f;
+        msum[3 * warp] = sa;
+        msum[3 * warp + 1] = sb;
+        msum[3 * warp + 2] = cnt;
       }
     }
-    __syncthreads();  // the means are visible, and every read of the raw values precedes the apodized writes
+    __syncthreads();  // the sums are visible, and every read of the raw values precedes the apodized writes
     if (run) {
-      const float ma = means[2 * slot], mb = means[2 * slot + 1];
+      constexpr int MW = 4 / NWIN;
+      double sa = 0.0, sb = 0.0, cnt = 0.0;
+#pragma unroll
+      for (int h = 0; h < MW; ++h) {
+        sa += msum[3 * (slot * MW + h)];
+        sb += msum[3 * (slot * MW + h) + 1];
+        cnt += msum[3 * (slot * MW + h) + 2];
+      }
+      const float ma = cnt > 0 ? (float)(sa / cnt) : 0.f, mb = cnt > 0 ? (float)(sb / cnt) : 0.f;
       for (int k = ts; k < W * W; k += 2 * SEG) {
         const int p = k % W, q = k / W;
         const float ap = sap[k];
@@ -580,7 +593,7 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
       }
       // ---- (1,2,1)/4 smoothing along the columns, and its mean
       double dd[W];
-      double msum = 0.0;
+      double fs[2] = {0.0, 0.0};  // two interleaved partial sums (shorter dependency chains)
 #pragma unroll
       for (int r = 0; r < W; ++r) {
         const float left = __shfl_up_sync(FULL, dcol[r], 1, SEG);
@@ -589,9 +602,10 @@ __global__ void __launch_bounds__(UQW_THREADS, UQWCfg<W>::MINB) uq_warp_kernel(c
         const float rr = c < M - 1 ? right : dcol[r];
         const float v = __fmul_rn(0.25f, __fadd_rn(__fadd_rn(l, __fmul_rn(2.0f, dcol[r])), rr));
         dd[r] = (double)v;
-        if (col) msum += dd[r];
+        if (col) fs[r & 1] += dd[r];
       }
-      const double mu = seg_sum<SEG>(msum) / (double)(W * M);
+      constexpr double inv_n = 1.0 / (double)(W * M);  // the mean as a product (a division costs a long chain)
+      const double mu = seg_sum<SEG>(fs[0] + fs[1]) * inv_n;
 #pragma unroll
       for (int r = 0; r < W; ++r) dd[r] = col ? dd[r] - mu : 0.0;
       // this lane's column of the field into shared memory (lanes past M
