@@ -307,7 +307,10 @@ def timeseries_leg(hb, ws, torch, dev_time, npairs=8, reps=3, cut_check=True):
     the device's deviation from the oracle's FP64 run on a 1024^2 cut.
     Beside it, the reference's effort = :high preset ([128, 64, 32] padded,
     2 sweeps, uncertainty) on one 4096^2 pair, ms per pair, the case the
-    reference publishes for its own GPU path."""
+    reference publishes for its own GPU path; and the sum-of-correlation
+    ensemble (run_piv_ensemble) over the same pairs and schedule, ms per
+    pair, with its deviation from the oracle's FP64 ensemble of two pairs
+    on the 1024^2 cut."""
     syn = hb.synthetic
     frames, flow = syn.config4_frames(npairs + 1, seed=1004)
     passes = hb.multipass_parameters([128, 64, 32]) + [
@@ -346,6 +349,18 @@ def timeseries_leg(hb, ws, torch, dev_time, npairs=8, reps=3, cut_check=True):
         "ms_per_pair": ms_hi, "schedule": "[128,64,32] padded + gauss, 2 sweeps per pass, UQ in the final pass",
         "reference_published_s_per_pair": {"RTX 2000 Ada, Float32, batch 8192": 2.98,
                                            "RX 6800 XT, Float32, steady state": 3.29}}
+    # the sum-of-correlation ensemble (run_piv_ensemble) over the same chained
+    # UInt16 pairs and schedule: one field from all pairs' summed planes
+    hb.run_piv_ensemble(pairs16, passes, workspace=ws)
+    ms_e = dev_time(lambda: hb.run_piv_ensemble(pairs16, passes, workspace=ws), reps)
+    e = hb.run_piv_ensemble(pairs16, passes, workspace=ws)
+    X, Y = np.meshgrid(e.x, e.y)
+    ut, vt = flow(X, Y)
+    ok = ~(e.outliers | e.mask)
+    out["ensemble"] = {
+        "ms_per_pair": ms_e / npairs, "pairs_per_s": npairs / (ms_e / 1e3), "field_vectors": int(e.u.size - e.mask.sum()),
+        "rms_px": float(np.sqrt(np.mean((e.u - ut)[ok] ** 2 + (e.v - vt)[ok] ** 2))),
+        "outlier_fraction": float(e.outliers.mean())}
     if cut_check:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
@@ -358,6 +373,15 @@ def timeseries_leg(hb, ws, torch, dev_time, npairs=8, reps=3, cut_check=True):
         d = np.concatenate([np.abs(r.u - o["u"])[ok], np.abs(r.v - o["v"])[ok]]).astype(np.float64)
         out["fp64_oracle_error_1024_cut"] = {"components": int(d.size), "max_abs_px": float(d.max()),
                                              "rms_px": float(np.sqrt(np.mean(d * d)))}
+        # the ensemble of the first two chained pairs on the same cut
+        c2 = [np.asfortranarray(frames[k][:1024, :1024].astype(np.float32) / np.float32(65535)) for k in range(3)]
+        cp = [(c2[0], c2[1]), (c2[1], c2[2])]
+        re_ = hb.run_piv_ensemble(cp, passes, workspace=ws)
+        oe = oracle.run_ensemble(cp, passes, nthreads=os.cpu_count() or 1, dtype=np.float64)
+        ok = ~(re_.outliers | re_.mask | oe["outliers"] | oe["mask"])
+        d = np.concatenate([np.abs(re_.u - oe["u"])[ok], np.abs(re_.v - oe["v"])[ok]]).astype(np.float64)
+        out["ensemble"]["fp64_oracle_error_1024_cut_2_pairs"] = {
+            "components": int(d.size), "max_abs_px": float(d.max()), "rms_px": float(np.sqrt(np.mean(d * d)))}
     return out
 
 
