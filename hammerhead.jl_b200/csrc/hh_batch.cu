@@ -50,8 +50,19 @@ struct BPlan {
   // device storage
   std::vector<void*> allocs;
   BPair* d_tables = nullptr;
-  BPair* h_tables = nullptr;  // pinned upload staging
-  uint8_t* h_gmask = nullptr; // pinned grid-mask staging (nslots * gcap), when masks
+  // Pinned upload staging of the descriptor tables and grid masks, two sets
+  // used in turn. A kernel reads a set from host memory when the stream
+  // reaches the call's upload, so with asynchronous calls (HH_BATCH_ASYNC)
+  // the next call fills the other set, and a set is refilled only after the
+  // event recorded behind its last upload has completed.
+  BPair* h_tables_set[2] = {nullptr, nullptr};
+  uint8_t* h_gmask_set[2] = {nullptr, nullptr};  // nslots * gcap each, when masks
+  cudaEvent_t upload_ev[2] = {nullptr, nullptr};
+  int upload_set = 0;
+  // recorded behind the last asynchronous call's read-back; the plan's
+  // storage is released only after it completes
+  cudaEvent_t done_ev = nullptr;
+  bool async_pending = false;
   int32_t* d_done = nullptr;
   int32_t* d_sweeps = nullptr;
   int32_t* d_slot_sweeps = nullptr;  // nslots x npairs: sweeps run by each pair in each slot
@@ -84,14 +95,22 @@ struct BPlan {
 static void free_plan(void* vp) {
   BPlan* P = static_cast<BPlan*>(vp);
   if (!P) return;
+  // work of an asynchronous call may still read the plan's storage
+  if (P->async_pending && P->done_ev) cudaEventSynchronize(P->done_ev);
+  for (cudaEvent_t e : P->upload_ev)
+    if (e) cudaEventSynchronize(e);
   if (P->exec) cudaGraphExecDestroy(P->exec);
   if (P->graph) cudaGraphDestroy(P->graph);
   for (void* a : P->allocs) cudaFree(a);
   for (auto& S : P->slots)
     for (auto& c : S.classes)
       if (c.jobs) cudaFree(c.jobs);
-  if (P->h_tables) cudaFreeHost(P->h_tables);
-  if (P->h_gmask) cudaFreeHost(P->h_gmask);
+  for (int i = 0; i < 2; ++i) {
+    if (P->h_tables_set[i]) cudaFreeHost(P->h_tables_set[i]);
+    if (P->h_gmask_set[i]) cudaFreeHost(P->h_gmask_set[i]);
+    if (P->upload_ev[i]) cudaEventDestroy(P->upload_ev[i]);
+  }
+  if (P->done_ev) cudaEventDestroy(P->done_ev);
   delete P;
 }
 
@@ -257,11 +276,13 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
   float** rf[] = {&r.u, &r.v, &r.ratio, &r.moment, &r.unc_u, &r.unc_v};
   for (float** f : rf) HH_TRY(plan_alloc(ctx, P, R, f));
   HH_TRY(plan_alloc(ctx, P, R, &r.outl));
-  if (any_mask) {
-    HH_TRY(plan_alloc(ctx, P, (size_t)nslots * G, &P.d_gmask));
-    HH_CK(cudaMallocHost(&P.h_gmask, std::max<size_t>((size_t)nslots * G, 1)));
+  for (int i = 0; i < 2; ++i) {
+    if (any_mask) HH_CK(cudaMallocHost(&P.h_gmask_set[i], std::max<size_t>((size_t)nslots * G, 1)));
+    HH_CK(cudaMallocHost(&P.h_tables_set[i], sizeof(BPair) * std::max<size_t>((size_t)nslots * npairs, 1)));
+    HH_CK(cudaEventCreateWithFlags(&P.upload_ev[i], cudaEventDisableTiming));
   }
-  HH_CK(cudaMallocHost(&P.h_tables, sizeof(BPair) * (size_t)nslots * npairs));
+  HH_CK(cudaEventCreateWithFlags(&P.done_ev, cudaEventDisableTiming));
+  if (any_mask) HH_TRY(plan_alloc(ctx, P, (size_t)nslots * G, &P.d_gmask));
   P.final_gmask.assign(R, 0);
   // descriptor tables and job classes, slot by slot
   P.tables.assign((size_t)nslots * npairs, BPair{});
@@ -629,6 +650,11 @@ static hh_status stage_inputs(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs,
   cudaStream_t s = ctx->stream;
   const int np = P.npairs;
   const bool any_mask = P.d_gmask != nullptr;
+  // this call's staging set: the upload that last read it must have run
+  const int set = P.upload_set;
+  HH_CK(cudaEventSynchronize(P.upload_ev[set]));
+  BPair* h_tables = P.h_tables_set[set];
+  uint8_t* h_gmask = P.h_gmask_set[set];
   bool any_u16 = false;
   for (int p = 0; p < np; ++p) any_u16 |= pairs[p].format != HH_PIX_F32;
   if ((!device_inputs || any_u16) && !P.stageA) {
@@ -693,7 +719,7 @@ static hh_status stage_inputs(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs,
         Grid gm;
         HH_TRY(make_grid(ctx, q.nr, q.nc, ps[k], hm, thr, gm));
         if (gm.any_mask) {
-          memcpy(P.h_gmask + (size_t)k * P.gcap + b.goff, gm.gmask.data(), gm.gmask.size());
+          memcpy(h_gmask + (size_t)k * P.gcap + b.goff, gm.gmask.data(), gm.gmask.size());
           b.gmask = P.d_gmask + (size_t)k * P.gcap + b.goff;
         }
         if (k == P.npass[p] - 1) memcpy(P.final_gmask.data() + b.roff, gm.gmask.data(), gm.gmask.size());
@@ -706,9 +732,11 @@ static hh_status stage_inputs(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs,
   // the tables and grid masks are read from their page-locked staging by a
   // kernel: an upload through the copy engine would queue behind frame
   // copies that a caller streams in on another stream meanwhile
-  memcpy(P.h_tables, P.tables.data(), sizeof(BPair) * P.tables.size());
-  HH_CK(hh::launch_host_read_copy(P.d_tables, P.h_tables, sizeof(BPair) * P.tables.size(), s));
-  if (any_mask) HH_CK(hh::launch_host_read_copy(P.d_gmask, P.h_gmask, (size_t)P.nslots * P.gcap, s));
+  memcpy(h_tables, P.tables.data(), sizeof(BPair) * P.tables.size());
+  HH_CK(hh::launch_host_read_copy(P.d_tables, h_tables, sizeof(BPair) * P.tables.size(), s));
+  if (any_mask) HH_CK(hh::launch_host_read_copy(P.d_gmask, h_gmask, (size_t)P.nslots * P.gcap, s));
+  HH_CK(cudaEventRecord(P.upload_ev[set], s));
+  P.upload_set = set ^ 1;
   return HH_OK;
 }
 
@@ -794,7 +822,14 @@ hh_status hh_run_batched(hh_ctx* ctx, const hh_batch_pair* pairs, int32_t npairs
     }
     if (out->offsets) out->offsets[npairs] = R;
   }
+  if ((flags & HH_BATCH_ASYNC) && !ctx->prof) {
+    // the caller waits on the context stream before it reads the results
+    HH_CK(cudaEventRecord(P->done_ev, s));
+    P->async_pending = true;
+    return HH_OK;
+  }
   HH_CK(cudaStreamSynchronize(s));
+  P->async_pending = false;
   if (ctx->prof) HH_TRY(recharge_live(ctx, *P));
   return flush_profile(ctx);
 }

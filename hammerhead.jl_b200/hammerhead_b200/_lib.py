@@ -119,6 +119,7 @@ class hh_batch_result(ctypes.Structure):
 
 HH_BATCH_DEVICE_INPUTS = 1
 HH_BATCH_NO_GRAPH = 2
+HH_BATCH_ASYNC = 4
 HH_PIX_F32 = 0
 HH_PIX_U16 = 1
 HH_PIX_U16_RAW = 2

@@ -127,7 +127,8 @@ class BatchRunner:
         self.out = {k: self._buffer(R, np.float32, pinned) for k in _FIELDS}
         self.outliers = self._buffer(R, np.uint8, pinned)
         self.gmask = np.zeros(R, np.uint8)
-        self.sweeps = np.zeros(n, np.int32)
+        self.sweeps = self._buffer(n, np.int32, pinned)
+        self.sweeps[...] = 0
         self.result = _lib.hh_batch_result(
             _lib.i32ptr(self.ny), _lib.i32ptr(self.nx), self.offsets.ctypes.data_as(_lib._I64),
             *[_lib.fptr(self.out[k]) for k in _FIELDS], _lib.u8ptr(self.outliers), _lib.u8ptr(self.gmask),
@@ -147,8 +148,8 @@ class BatchRunner:
             try:
                 import torch
                 if torch.cuda.is_available():
-                    t = torch.empty(max(n, 1), dtype={np.float32: torch.float32, np.uint8: torch.uint8}[dtype],
-                                    pin_memory=True)
+                    t = torch.empty(max(n, 1), dtype={np.float32: torch.float32, np.uint8: torch.uint8,
+                                                      np.int32: torch.int32}[dtype], pin_memory=True)
                     self._keep.append(t)
                     return t.numpy()[:n]
             except Exception:  # noqa: BLE001 -- no CUDA torch: pageable buffers
@@ -160,12 +161,17 @@ class BatchRunner:
         """Final-pass vectors of the batch (grid cells not masked)."""
         return int(self.offsets[-1] - self.gmask.sum())
 
-    def run(self, read=True):
+    def run(self, read=True, wait=True):
         """Analyse the whole batch once; results land in the runner's buffers
-        (read=False leaves them on the device, for timing the device work)."""
+        (read=False leaves them on the device, for timing the device work).
+        wait=False returns once the run and its read-back are queued on the
+        workspace's stream (HH_BATCH_ASYNC): wait on that stream (for example
+        through an event recorded on it, see `stream`) before reading the
+        results or changing the images."""
         L = _lib.lib()
+        flags = self.flags | (0 if wait else _lib.HH_BATCH_ASYNC)
         st = L.hh_run_batched(self.ws.ctx, self.pairs, self.npairs, self.descs, _lib.i32ptr(self.offsets_in),
-                              len(self.schedules), self.mask_threshold, self.smoothing, self.flags,
+                              len(self.schedules), self.mask_threshold, self.smoothing, flags,
                               ctypes.byref(self.result) if read else None)
         _lib.check(st, self.ws.ctx)
         return self
@@ -466,12 +472,18 @@ def run_piv_batch_stream(batches, passes, *, masks=None, predictor_smoothing=Tru
         stage_host[key].numpy()[...] = xt.astype(nd, copy=False)
         return stage_host[key]
 
-    def stage(batch, slot):
+    def stage(batch, slot, after):
+        """Queue the copies of `batch` into device set `slot` on the copy
+        stream, behind `after` (the event behind the analysis that last read
+        that set, or None)."""
         batch = list(batch)
         if len(batch) != n:
             raise DimensionMismatch(f"every batch must hold {n} pairs, got {len(batch)}")
+        events[slot].synchronize()  # the last copies out of this set's staging buffers are done
         srcs = [(host_tensor(a, j, 0, slot), host_tensor(b, j, 1, slot)) for j, (a, b) in enumerate(batch)]
         with torch.cuda.stream(copy_stream):
+            if after is not None:
+                copy_stream.wait_event(after)
             for (da, db), (ha, hb_) in zip(dev[slot], srcs):
                 da.copy_(ha, non_blocking=True)
                 db.copy_(hb_, non_blocking=True)
@@ -482,7 +494,8 @@ def run_piv_batch_stream(batches, passes, *, masks=None, predictor_smoothing=Tru
     conv = [None, None]  # result conversion of the batch last analysed by each runner
     runners = sess["runners"]
 
-    def collect(k, slot):
+    def collect(k, slot, done):
+        done.synchronize()  # the run and read-back of batch k have finished
         res = runners[slot].results(copy=True)
         if on_batch is not None:
             on_batch(k, res)
@@ -490,7 +503,9 @@ def run_piv_batch_stream(batches, passes, *, masks=None, predictor_smoothing=Tru
 
     try:
         with cf.ThreadPoolExecutor(max_workers=1) as pool, cf.ThreadPoolExecutor(max_workers=1) as post:
-            fut = pool.submit(stage, first, 0)
+            lib_stream = torch.cuda.ExternalStream(ws.stream())
+            done = [None, None]  # the event behind each runner's last queued run
+            fut = pool.submit(stage, first, 0, None)
             if runners is None:  # prepared while the first batch is copied in
                 runners = [BatchRunner([(a.T, b.T) for a, b in dev[s]], passes, masks=sess["masks"],
                                        predictor_smoothing=predictor_smoothing, mask_threshold=mask_threshold,
@@ -503,7 +518,9 @@ def run_piv_batch_stream(batches, passes, *, masks=None, predictor_smoothing=Tru
             while fut is not None:
                 slot = k % 2
                 fut.result()
-                events[slot].synchronize()
+                # the library stream waits for batch k's frames; the host does
+                # not, so the device runs the queued batches back to back
+                lib_stream.wait_event(events[slot])
                 if conv[slot] is not None:  # this runner's buffers still hold batch k-2
                     out.append(conv[slot].result())
                     conv[slot] = None
@@ -518,11 +535,14 @@ def run_piv_batch_stream(batches, passes, *, masks=None, predictor_smoothing=Tru
                 # releases the interpreter lock: the helper threads then do
                 # their Python work while the device runs, instead of holding
                 # the lock while this thread prepares the call
-                fut = pool.submit(stage, nxt, 1 - slot) if nxt is not None else None
+                fut = pool.submit(stage, nxt, 1 - slot, done[1 - slot]) if nxt is not None else None
                 if pend is not None:
                     conv[pend[1]] = post.submit(collect, *pend)
-                runners[slot].run()
-                pend = (k, slot)
+                runners[slot].run(wait=False)
+                ev = torch.cuda.Event()
+                ev.record(lib_stream)
+                done[slot] = ev
+                pend = (k, slot, ev)
                 k += 1
             if pend is not None:
                 conv[pend[1]] = post.submit(collect, *pend)
@@ -531,6 +551,8 @@ def run_piv_batch_stream(batches, passes, *, masks=None, predictor_smoothing=Tru
                     out.append(conv[j % 2].result())
                     conv[j % 2] = None
     finally:
+        if ws.__dict__.get("_ctx") is not None:
+            torch.cuda.ExternalStream(ws.stream()).synchronize()  # no queued run still reads the frames
         if own:
             for r in runners or ():
                 r.close()

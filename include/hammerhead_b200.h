@@ -191,6 +191,14 @@ typedef struct hh_batch_result {
 
 #define HH_BATCH_DEVICE_INPUTS 1 /* A, B, mask are device pointers */
 #define HH_BATCH_NO_GRAPH 2      /* launch directly instead of replaying a captured graph */
+/* Return once the run and its read-back are queued on the context stream
+ * (hh_ctx_stream) instead of after they finish: the result arrays in *out
+ * (page-locked host memory, or the copies are not asynchronous) and device
+ * inputs must stay untouched until the caller has waited on that stream, for
+ * example through an event recorded on it after the call. Calls on one
+ * context run in call order; a call may fill its host staging while an
+ * earlier call is still queued. Ignored while profiling. */
+#define HH_BATCH_ASYNC 4
 
 /* Final grid sizes and result offsets of a batch (host-only). */
 hh_status hh_batch_grid(const hh_batch_pair* pairs, int32_t npairs, const hh_pass_desc* passes,

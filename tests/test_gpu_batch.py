@@ -239,6 +239,37 @@ def test_batch_stream_equals_batch(hb, ws):
             _same(a, b)
 
 
+def test_batch_stream_long_async(hb, ws):
+    # seven batches of new images: the stream queues each run without a host
+    # wait (HH_BATCH_ASYNC), so runs, copies and the plan's two upload
+    # staging sets are reused several times while earlier runs are still
+    # queued; every batch must still equal its own batch call bit for bit
+    s1, s2 = _schedules(hb)
+    sched = [s1, s2, s2]
+    batches = [_mixed(hb, n=3, seed=1100 + 10 * k)[0] for k in range(7)]
+    out = hb.run_piv_batch_stream(batches, sched, workspace=ws)
+    assert len(out) == 7
+    for k in range(7):
+        for a, b in zip(out[k], hb.run_piv_batch(batches[k], sched, workspace=ws)):
+            _same(a, b)
+
+
+def test_batch_runner_async_run(hb, ws):
+    # run(wait=False) returns with the run queued; after a wait on the
+    # workspace's stream the results equal a synchronous run's
+    import torch
+
+    s1, s2 = _schedules(hb)
+    pairs = _mixed(hb, n=4, seed=1200)[0]
+    sync_res = hb.run_piv_batch(pairs, [s1, s2, s1, s2], workspace=ws)
+    runner = hb.BatchRunner(pairs, [s1, s2, s1, s2], workspace=ws)
+    runner.run(wait=False)
+    torch.cuda.ExternalStream(ws.stream()).synchronize()
+    for a, b in zip(runner.results(copy=True), sync_res):
+        _same(a, b)
+    assert list(runner.sweeps) == [r.sweeps[-1] for r in sync_res]
+
+
 def test_batch_stream_uint16(hb, ws):
     # UInt16 frames keep their pixel type on the device and are converted
     # there, in a stream exactly as in one batch call
