@@ -443,7 +443,75 @@ __device__ __forceinline__ ScanPlan scan_plan(int gtid, int gsize, int rlo, int 
   return sp;
 }
 
-template <int KC>
+// One column strip of the regional-maximum scan (src/localmax.jl:3-19): the
+// 3x3 neighbourhood rolls down the strip in registers, rows r - 1 (t) and r
+// (m) of the left, centre and right columns (3 loads per pixel). Earlier
+// neighbours in column-major order (the left column and the pixel above)
+// must not exceed the value, later ones (the right column and the pixel
+// below) must stay below it; fmaxf drops NaN neighbours, which never block
+// in the reference either.
+struct StripScan {
+  const float* Cl;
+  const float* Cc;
+  const float* Cr;
+  bool hl, hr;
+  int c, r1;
+  float lt, ct, rt, lm, cm, rm;
+  __device__ __forceinline__ void init(const float* R, int ldr, int nc, int c_, int r0, int r1_) {
+    const float NaNf = __int_as_float(0x7fc00000);
+    c = c_;
+    r1 = r1_;
+    hl = c > 0;
+    hr = c < nc - 1;
+    Cc = R + c * ldr;
+    Cl = hl ? Cc - ldr : Cc;
+    Cr = hr ? Cc + ldr : Cc;
+    lt = ct = rt = NaNf;
+    if (r0 > 0) {
+      lt = hl ? Cl[r0 - 1] : NaNf;
+      ct = Cc[r0 - 1];
+      rt = hr ? Cr[r0 - 1] : NaNf;
+    }
+    lm = hl ? Cl[r0] : NaNf;
+    cm = Cc[r0];
+    rm = hr ? Cr[r0] : NaNf;
+  }
+  // rows rb0 + 1 .. rb0 + SU of the three columns (NaN past the plane)
+  template <int SU> __device__ __forceinline__ void load(int rb0, int nr, float* l, float* m, float* r) const {
+    const float NaNf = __int_as_float(0x7fc00000);
+#pragma unroll
+    for (int u = 0; u < SU; ++u) {
+      const int rr = rb0 + 1 + u;
+      const bool ok = rr < nr;
+      l[u] = ok && hl ? Cl[rr] : NaNf;
+      m[u] = ok ? Cc[rr] : NaNf;
+      r[u] = ok && hr ? Cr[rr] : NaNf;
+    }
+  }
+  // tests row r (the centre value cm) and rolls down one row. Without TIES a
+  // full list rejects a key equal to its K-th: the strips of a thread reach
+  // the list in index order, so a later index cannot win the tie.
+  template <bool TIES, class TK>
+  __device__ __forceinline__ void step(int r, float lb, float cb, float rbv, int nr, TK& tk, int K) {
+    const float v = cm;
+    if (r < r1 && !isnan(v)) {
+      const uint32_t h = fkey(v);
+      if (TIES ? h >= tk.thr : h > tk.thr) {
+        const float e = fmaxf(fmaxf(lt, lm), fmaxf(lb, ct));
+        const float l = fmaxf(fmaxf(rt, rm), fmaxf(rbv, cb));
+        if (!(e > v) && !(l >= v)) tk.insert(h, ~(uint32_t)(r + c * nr), K);
+      }
+    }
+    lt = lm;
+    ct = cm;
+    rt = rm;
+    lm = lb;
+    cm = cb;
+    rm = rbv;
+  }
+};
+
+template <int KC, bool PAIRS>
 __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
                                              int subpixel, int gtid, int gsize, uint32_t* red, bool active,
                                              float* s_vals, int* s_locs, int64_t grid_id, int64_t job,
@@ -458,64 +526,67 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
   int nfound = 0;
   if (finder == 0) {
     // regional maxima (src/localmax.jl:3-19): each thread walks column strips
-    // top to bottom keeping the 3x3 neighbourhood in registers (3 loads per
-    // pixel). Earlier neighbours in column-major order (the left column and
-    // the pixel above) must not exceed the value, later ones (the right
-    // column and the pixel below) must stay below it; fmaxf drops NaN
-    // neighbours, which never block in the reference either.
+    // of the box top to bottom (StripScan), keeping its K best in registers
     TopK<KC> tk;
     tk.init();
     if (scan) {
-      const int bw = sp.bw, S = sp.S, rps = sp.rps;
-      const float NaNf = __int_as_float(0x7fc00000);
-      for (int strip = gtid; strip < bw * S; strip += gsize) {
-        int c = sp.c, r0 = sp.r0, r1 = sp.r1;
+      const int bw = sp.bw, S = sp.S, rps = sp.rps, ns = bw * S;
+      // blocks of SU rows: the next SU rows of the three columns are loaded
+      // together, so the loads of a block overlap instead of each row
+      // waiting on its own
+      constexpr int SU = 2;
+      // strip `strip` of the box; an empty strip inside the box when it has
+      // no rows (its addresses stay valid)
+      auto strip_at = [&](int strip, int& c, int& r0, int& r1) {
+        c = sp.c;
+        r0 = sp.r0;
+        r1 = sp.r1;
         if (strip != gtid) {  // a further strip: only when the box is wider than the group
           c = clo + strip % bw;
           r0 = rlo + (strip / bw) * rps;
           r1 = min(rhi + 1, r0 + rps);
         }
-        if (r0 >= r1) continue;
-        const bool hl = c > 0, hr = c < nc - 1;
-        const float* Cc = R + c * ldr;
-        const float* Cl = hl ? Cc - ldr : Cc;
-        const float* Cr = hr ? Cc + ldr : Cc;
-        float lt = NaNf, ct = NaNf, rt = NaNf;  // row r - 1
-        if (r0 > 0) {
-          lt = hl ? Cl[r0 - 1] : NaNf;
-          ct = Cc[r0 - 1];
-          rt = hr ? Cr[r0 - 1] : NaNf;
+        if (strip >= ns || r0 >= r1) {
+          c = clo;
+          r0 = r1 = rlo;
         }
-        float lm = hl ? Cl[r0] : NaNf, cm = Cc[r0], rm = hr ? Cr[r0] : NaNf;  // row r
-        // blocks of SU rows: the next SU rows of the three columns are loaded
-        // together, so the loads of a block overlap instead of each row
-        // waiting on its own
-        constexpr int SU = 2;
-        for (int rb0 = r0; rb0 < r1; rb0 += SU) {
-          float lb[SU], cb[SU], rbv[SU];  // rows rb0 + 1 .. rb0 + SU
+      };
+      if (PAIRS && ns > gsize) {
+        // Two strips per thread at a time, their rows interleaved, so the
+        // two strips' loads and tests are independent chains. Their pixels
+        // then reach the list out of index order, so a key equal to the
+        // list's K-th goes to the insert's full (key, index) comparison.
+        for (int sa = gtid; sa < ns; sa += 2 * gsize) {
+          int ca, ra0, ra1, cb0, rb0, rb1;
+          strip_at(sa, ca, ra0, ra1);
+          strip_at(sa + gsize, cb0, rb0, rb1);
+          StripScan A, B;
+          A.init(R, ldr, nc, ca, ra0, ra1);
+          B.init(R, ldr, nc, cb0, rb0, rb1);
+          const int nrow = max(ra1 - ra0, rb1 - rb0);
+          for (int rb = 0; rb < nrow; rb += SU) {
+            float al[SU], ac[SU], ar[SU], bl[SU], bc[SU], br[SU];  // rows + 1 .. + SU
+            A.load<SU>(ra0 + rb, nr, al, ac, ar);
+            B.load<SU>(rb0 + rb, nr, bl, bc, br);
 #pragma unroll
-          for (int u = 0; u < SU; ++u) {
-            const int rr = rb0 + 1 + u;
-            const bool ok = rr < nr;
-            lb[u] = ok && hl ? Cl[rr] : NaNf;
-            cb[u] = ok ? Cc[rr] : NaNf;
-            rbv[u] = ok && hr ? Cr[rr] : NaNf;
-          }
-#pragma unroll
-          for (int u = 0; u < SU; ++u) {
-            const int r = rb0 + u;
-            const float v = cm;
-            if (r < r1 && !isnan(v)) {
-              const uint32_t h = fkey(v);
-              // a later index cannot win a tie, so a full list rejects h <= last
-              if (h > tk.thr) {
-                const float e = fmaxf(fmaxf(lt, lm), fmaxf(lb[u], ct));
-                const float l = fmaxf(fmaxf(rt, rm), fmaxf(rbv[u], cb[u]));
-                if (!(e > v) && !(l >= v)) tk.insert(h, ~(uint32_t)(r + c * nr), K);
-              }
+            for (int u = 0; u < SU; ++u) {
+              A.template step<true>(ra0 + rb + u, al[u], ac[u], ar[u], nr, tk, K);
+              B.template step<true>(rb0 + rb + u, bl[u], bc[u], br[u], nr, tk, K);
             }
-            lt = lm; ct = cm; rt = rm;
-            lm = lb[u]; cm = cb[u]; rm = rbv[u];
+          }
+        }
+      } else {
+        for (int strip = gtid; strip < ns; strip += gsize) {
+          int c, r0, r1;
+          strip_at(strip, c, r0, r1);
+          if (r0 >= r1) continue;
+          StripScan A;
+          A.init(R, ldr, nc, c, r0, r1);
+          for (int rb0 = r0; rb0 < r1; rb0 += SU) {
+            float lb[SU], cb[SU], rbv[SU];  // rows rb0 + 1 .. rb0 + SU
+            A.load<SU>(rb0, nr, lb, cb, rbv);
+#pragma unroll
+            for (int u = 0; u < SU; ++u) A.template step<false>(rb0 + u, lb[u], cb[u], rbv[u], nr, tk, K);
           }
         }
       }
@@ -639,16 +710,20 @@ __device__ __forceinline__ void analyze_body(const float* R, int nr, int nc, int
 
 // The analysis as a call: small planes keep it out of line (the kernel's
 // transform stages then keep their registers); large planes inline it.
+// PAIRS: walk two column strips per thread at a time, for groups with more
+// strips than threads (half-warp groups of 32-point planes); elsewhere the
+// second strip's registers would only add spills.
+template <bool PAIRS = false>
 __device__ __noinline__ void analyze_group(const float* R, int nr, int nc, int ldr, int K, int npeaks, int finder,
                                            int subpixel, int gtid, int gsize, uint32_t* red, bool active,
                                            float* s_vals, int* s_locs, int64_t grid_id, int64_t job,
                                            const PeakOut* o, bool poison, int bar, const ScanPlan sp,
                                            float* rec, int64_t rec_stride) {
   if (K <= 4)
-    analyze_body<4>(R, nr, nc, ldr, K, npeaks, finder, subpixel, gtid, gsize, red, active, s_vals, s_locs, grid_id, job,
+    analyze_body<4, PAIRS>(R, nr, nc, ldr, K, npeaks, finder, subpixel, gtid, gsize, red, active, s_vals, s_locs, grid_id, job,
                     o, poison, bar, sp, rec, rec_stride);
   else
-    analyze_body<KMAX>(R, nr, nc, ldr, K, npeaks, finder, subpixel, gtid, gsize, red, active, s_vals, s_locs, grid_id,
+    analyze_body<KMAX, PAIRS>(R, nr, nc, ldr, K, npeaks, finder, subpixel, gtid, gsize, red, active, s_vals, s_locs, grid_id,
                        job, o, poison, bar, sp, rec, rec_stride);
 }
 
@@ -1369,13 +1444,13 @@ __global__ void __launch_bounds__(CorrCfg<N, W, SRCH, VAR>::NT, CorrCfg<N, W, SR
     const bool defer = a.rec && a.finder == 0;
     uint32_t* gred = red + w * (G / 32) * 2 * KMAX;
     if (C::INLINE_ANALYSIS && K <= 4)
-      analyze_body<4>(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
+      analyze_body<4, false>(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
                       s_locs + w * 2 * KMAX, gid, job, defer ? nullptr : &pw, bad, bar, sp, a.rec, a.njobs);
     else if (C::INLINE_ANALYSIS)
-      analyze_body<KMAX>(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
+      analyze_body<KMAX, false>(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
                          s_locs + w * 2 * KMAX, gid, job, defer ? nullptr : &pw, bad, bar, sp, a.rec, a.njobs);
     else
-      analyze_group(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
+      analyze_group<C::HALF>(Rw, N, N, LDR, K, a.npeaks, a.finder, a.subpixel, gt, G, gred, true, s_vals + w * KMAX,
                     s_locs + w * 2 * KMAX, gid, job, defer ? nullptr : &pw, bad, bar, sp, a.rec, a.njobs);
     grp_sync(bar, G);  // the plane is reused by the group's next window
   }
