@@ -503,7 +503,7 @@ def run_piv_batch_stream(batches, passes, *, masks=None, predictor_smoothing=Tru
 
     try:
         with cf.ThreadPoolExecutor(max_workers=1) as pool, cf.ThreadPoolExecutor(max_workers=1) as post:
-            lib_stream = torch.cuda.ExternalStream(ws.stream())
+            lib_stream = torch.cuda.ExternalStream(ws.stream(), device=torch.device("cuda", ws.device))
             done = [None, None]  # the event behind each runner's last queued run
             fut = pool.submit(stage, first, 0, None)
             if runners is None:  # prepared while the first batch is copied in
@@ -552,7 +552,8 @@ def run_piv_batch_stream(batches, passes, *, masks=None, predictor_smoothing=Tru
                     conv[j % 2] = None
     finally:
         if ws.__dict__.get("_ctx") is not None:
-            torch.cuda.ExternalStream(ws.stream()).synchronize()  # no queued run still reads the frames
+            # no queued run still reads the frames
+            torch.cuda.ExternalStream(ws.stream(), device=torch.device("cuda", ws.device)).synchronize()
         if own:
             for r in runners or ():
                 r.close()

@@ -264,7 +264,7 @@ def test_batch_runner_async_run(hb, ws):
     sync_res = hb.run_piv_batch(pairs, [s1, s2, s1, s2], workspace=ws)
     runner = hb.BatchRunner(pairs, [s1, s2, s1, s2], workspace=ws)
     runner.run(wait=False)
-    torch.cuda.ExternalStream(ws.stream()).synchronize()
+    torch.cuda.ExternalStream(ws.stream(), device=torch.device("cuda", ws.device)).synchronize()
     for a, b in zip(runner.results(copy=True), sync_res):
         _same(a, b)
     assert list(runner.sweeps) == [r.sweeps[-1] for r in sync_res]
