@@ -34,6 +34,29 @@ def test_library_exports_header(hb):
     assert L.hh_version().startswith(b"hammerhead_b200")
 
 
+def header_constants():
+    """Integer constants of the header: #define NAME value and enum members."""
+    txt = open(os.path.join(ROOT, "include", "hammerhead_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    out = {k: int(v) for k, v in re.findall(r"#define\s+(HH_[A-Z0-9_]+)\s+(\d+)\b", txt)}
+    for body in re.findall(r"enum\s*\{(.*?)\}", txt, flags=re.S):
+        out.update({k: int(v) for k, v in re.findall(r"\b(HH_[A-Z0-9_]+)\s*=\s*(\d+)", body)})
+    return out
+
+
+def test_python_constants_match_header(hb):
+    # the host layer mirrors the header's status codes, flags and pixel
+    # formats by value: each HH_* integer it defines equals the header's
+    from hammerhead_b200 import _lib
+
+    hdr = header_constants()
+    mirrored = {k: v for k, v in vars(_lib).items() if k.startswith("HH_") and isinstance(v, int)}
+    assert {"HH_OK", "HH_ERR_OOM", "HH_BATCH_ASYNC", "HH_PIX_U16"} <= set(mirrored)
+    for k, v in mirrored.items():
+        assert k in hdr, f"{k} is not in the header"
+        assert hdr[k] == v, (k, hdr[k], v)
+
+
 def test_struct_layout(hb):
     from hammerhead_b200 import _lib
     import oracle
