@@ -174,7 +174,6 @@ static std::string plan_key(const hh_batch_pair* pairs, int npairs, const hh_pas
   return k;
 }
 
-static int64_t nseg_host(int64_t n) { return n >= 5 ? (n - 4 + 63) / 64 : 1; }
 
 static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, int npairs, const hh_pass_desc* passes,
                             const int32_t* so, double thr, bool smoothing) {
@@ -231,8 +230,8 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
     if (deforms[p]) {
       Wt += (nr * nc + 3) / 4 * 4;  // 16-byte aligned per pair: the deformation stores pixel quads
       Q += (nr + 2) * (nc + 2);
-      WC += (nc + 31) / 32 * nseg_host(nr + 2);  // column tiles x segments
-      WR += (nr + 2 + 31) / 32 * nseg_host(nc + 2);  // 32-row groups x segments
+      WC += (nc + 31) / 32 * hh::b_nseg(nr + 2);  // column tiles x segments
+      WR += (nr + 2 + 31) / 32 * hh::b_nseg(nc + 2);  // 32-row groups x segments
     }
     roff[p] = R;
     const Grid& gf = P.grids[p].back();

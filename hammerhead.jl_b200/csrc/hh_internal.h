@@ -9,6 +9,13 @@ struct BPair;
 
 constexpr int KMAX = 8;  // peaks tracked per window on the device (n_peaks <= 8)
 
+// B-spline prefilter: each line's two Thomas sweeps are cut into independent
+// segments of BS_SEG unknowns whose sweeps start BS_WARM unknowns early from a
+// zero state (k_deform.cu). Segments of a padded line of n elements (n - 4
+// unknowns); the batched plan counts its work items with it.
+constexpr int BS_SEG = 64, BS_WARM = 32;
+__host__ __device__ __forceinline__ int64_t b_nseg(int64_t n) { return n >= 5 ? (n - 4 + BS_SEG - 1) / BS_SEG : 1; }
+
 // Arguments of the fused correlation kernel (one pass, one image pair).
 struct CorrArgs {
   const float* A;            // deformed (or raw) frame A, column-major nr x nc

@@ -71,13 +71,15 @@ __global__ void bspline_factors_kernel(int64_t n, float* cp, float* inv) {
 // Both Thomas sweeps are contractions (|cp_k| -> 0.268), so each line is cut
 // into independent segments of BS_SEG unknowns whose sweeps start BS_WARM
 // unknowns early from a zero state; the neglected term is below
-// 0.268^32 ~ 5e-19 of the value. The CPU restatement uses the same
-// segmentation, so the coefficients agree bit for bit. The forward sweep is
+// 0.268^32 ~ 5e-19 of the value, far under float rounding. The CPU
+// restatement solves each line in one sweep; the deformed images are held to
+// 4 ulp of the image scale against it. The forward sweep is
 // d_k = (rhs_k - d_{k-1}/6) inv_k (unknown k at line element k + 2; rhs_0 and
 // rhs_{m-1} carry the known c1 and c_{n-2}), the backward sweep
 // x_k = d_k - cp_k x_{k+1}, followed by the "Line" boundary coefficients
-// c0 = 2c1 - c2 and c_{n-1} = 2c_{n-2} - c_{n-3}.
-constexpr int BS_SEG = 64, BS_WARM = 32;
+// c0 = 2c1 - c2 and c_{n-1} = 2c_{n-2} - c_{n-3}. BS_SEG, BS_WARM and the
+// segment count b_nseg are in hh_internal.h (the batched plan counts work
+// items with them).
 
 cudaError_t launch_bspline_factors(int64_t n, float* cp, float* inv, cudaStream_t s) {
   bspline_factors_kernel<<<1, 1, 0, s>>>(n, cp, inv);
@@ -220,14 +222,15 @@ static unsigned b_blocks(int64_t n, int cap_per_sm = 16) {
 // padded column, the copied rows 1 and n - 2 included, so no padded copy of
 // the image is made first. Work items: (column tile, segment) per pair,
 // counted from BPair::wcol.
-__host__ __device__ __forceinline__ int64_t b_nseg(int64_t n) { return n >= 5 ? (n - 4 + BS_SEG - 1) / BS_SEG : 1; }
 
 constexpr int BS_TILE = BS_WARM + BS_SEG;  // rows staged per column
 constexpr int BS_TLD = BS_TILE + 1;        // odd stride: conflict-free by lane and by row
 constexpr int BSC_WARPS = 4;
-// per warp: a tile (32 columns x 96 rows at stride 97, or 96 columns x 32
-// rows at stride 33) and the elimination factors of its 96 unknowns
-constexpr int BS_WTILE = 96 * 33 > 32 * BS_TLD ? 96 * 33 : 32 * BS_TLD;
+constexpr int BS_RPL = (BS_TILE + 31) / 32;  // staged rows per lane and column
+// per warp: a tile (32 columns x BS_TILE rows at stride BS_TLD, or BS_TILE
+// columns x 32 rows at stride 33) and the elimination factors of its
+// BS_TILE unknowns
+constexpr int BS_WTILE = BS_TILE * 33 > 32 * BS_TLD ? BS_TILE * 33 : 32 * BS_TLD;
 constexpr int BS_WSTRIDE = BS_WTILE + BS_TILE;
 constexpr size_t BSC_SMEM = (size_t)BSC_WARPS * BS_WSTRIDE * sizeof(float);
 
@@ -242,7 +245,7 @@ __device__ __forceinline__ void stage_factors(float* F, const float* f, int cnt,
   bs_cp_async_wait_all();
 }
 
-// Rows [0, cnt) (cnt <= 96) of `ncol` columns between global memory (column
+// Rows [0, cnt) (cnt <= BS_TILE) of `ncol` columns between global memory (column
 // c at g + c * gld) and a staged tile (column c at T + c * BS_TLD). The
 // lanes walk down the columns. Loads are asynchronous copies straight into
 // shared memory, all of the tile's issued before the first is waited for (in
@@ -259,25 +262,25 @@ __device__ __forceinline__ void bs_cp_async_wait_all() {
 __device__ __forceinline__ void tile_load(float* T, const float* g, int64_t gld, int ncol, int cnt, int lane) {
   for (int c = 0; c < ncol; ++c)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
+    for (int j = 0; j < BS_RPL; ++j) {
       const int r = lane + 32 * j;
       if (r < cnt) bs_cp_async4(T + c * BS_TLD + r, g + c * gld + r);
     }
 }
 __device__ __forceinline__ void tile_store(const float* T, float* g, int64_t gld, int ncol, int cnt, int lane) {
   for (int c0 = 0; c0 < ncol; c0 += 8) {
-    float v[8][3];
+    float v[8][BS_RPL];
 #pragma unroll
     for (int u = 0; u < 8; ++u)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
+      for (int j = 0; j < BS_RPL; ++j) {
         const int c = c0 + u, r = lane + 32 * j;
         v[u][j] = (c < ncol && r < cnt) ? T[c * BS_TLD + r] : 0.f;
       }
 #pragma unroll
     for (int u = 0; u < 8; ++u)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
+      for (int j = 0; j < BS_RPL; ++j) {
         const int c = c0 + u, r = lane + 32 * j;
         if (c < ncol && r < cnt) g[c * gld + r] = v[u][j];
       }
