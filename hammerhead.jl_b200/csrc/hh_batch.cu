@@ -426,8 +426,11 @@ static hh_status build_plan(hh_ctx* ctx, BPlan& P, const hh_batch_pair* pairs, i
     for (const auto& c : S.classes) {
       recw = std::max(recw, (size_t)c.njobs * hh::correlate_record_words(c.npeaks));
       if (!c.special) gw = std::max(gw, (size_t)(c.gen.gscr_slices * c.gen.gscr_stride));
-      if ((c.unc_fused || c.unc_post) && hh::uq_general(c.pd.window[0], c.pd.window[1]))
-        uw = std::max(uw, (size_t)(4 * ctx->num_sms) * hh::uq_general_stride(c.pd.window[0], c.pd.window[1]));
+      if ((c.unc_fused || c.unc_post) && hh::uq_general(c.pd.window[0], c.pd.window[1])) {
+        hh::UQArgs ua{};  // the launch's slices, as uq_setup sizes them
+        uq_setup(ctx, c.pd.window[0], c.pd.window[1], ua);
+        uw = std::max(uw, (size_t)ua.gscr_slices * (size_t)ua.gscr_stride);
+      }
     }
   HH_TRY(plan_alloc(ctx, P, recw, &P.rec));
   if (gw) HH_TRY(plan_alloc(ctx, P, gw, &P.gscr));
